@@ -1,0 +1,112 @@
+"""ctypes declarations of libclbool_b200.so (the C ABI in include/clbool_b200.h).
+
+The library is the product: there is no CPU fallback.  If the shared object
+is missing, importing this module raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libclbool_b200.so")
+
+u32p = C.POINTER(C.c_uint32)
+u64p = C.POINTER(C.c_uint64)
+vp = C.c_void_p
+
+
+class clb_dcsr(C.Structure):
+    _fields_ = [("nrows", C.c_uint64), ("ncols", C.c_uint64), ("nnz", C.c_uint64), ("nzr", C.c_uint64),
+                ("rpt", vp), ("rows", vp), ("cols", vp)]
+
+
+class clb_coo(C.Structure):
+    _fields_ = [("nrows", C.c_uint64), ("ncols", C.c_uint64), ("nnz", C.c_uint64), ("rows", vp), ("cols", vp)]
+
+
+class clb_csr(C.Structure):
+    _fields_ = [("nrows", C.c_uint64), ("ncols", C.c_uint64), ("nnz", C.c_uint64), ("rpt", vp), ("cols", vp)]
+
+
+class clb_spgemm_stats(C.Structure):
+    _fields_ = [("products", C.c_uint64), ("nnz", C.c_uint64), ("nzr", C.c_uint64),
+                ("rows_per_bin", C.c_uint64 * 16), ("fallback_rows", C.c_uint64), ("capacity", C.c_uint64),
+                ("kernel_launches", C.c_uint32), ("reserved", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {"products": self.products, "nnz": self.nnz, "nzr": self.nzr,
+                "rows_per_bin": list(self.rows_per_bin)[:10], "fallback_rows": self.fallback_rows,
+                "capacity": self.capacity, "kernel_launches": self.kernel_launches}
+
+
+P = C.POINTER
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "clb_status_string": (C.c_char_p, [C.c_int]),
+    "clb_last_error": (C.c_char_p, []),
+    "clb_version": (C.c_int, []),
+    "clb_controls_create": (C.c_int, [C.c_int, P(vp)]),
+    "clb_controls_destroy": (C.c_int, [vp]),
+    "clb_controls_set_stream": (C.c_int, [vp, vp]),
+    "clb_controls_get_stream": (vp, [vp]),
+    "clb_controls_set_allocator": (C.c_int, [vp, vp, vp, vp]),
+    "clb_controls_sync": (C.c_int, [vp]),
+    "clb_controls_device": (C.c_int, [vp]),
+    "clb_device_count": (C.c_int, [P(C.c_int)]),
+    "clb_device_info": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, P(C.c_int), P(C.c_uint64)]),
+    "clb_malloc": (C.c_int, [vp, C.c_size_t, P(vp)]),
+    "clb_free": (C.c_int, [vp, vp]),
+    "clb_memcpy_h2d": (C.c_int, [vp, vp, vp, C.c_size_t]),
+    "clb_memcpy_d2h": (C.c_int, [vp, vp, vp, C.c_size_t]),
+    "clb_memcpy_d2d": (C.c_int, [vp, vp, vp, C.c_size_t]),
+    "clb_host_alloc": (C.c_int, [C.c_size_t, P(vp)]),
+    "clb_host_free": (C.c_int, [vp]),
+    "clb_dcsr_release": (C.c_int, [vp, P(clb_dcsr)]),
+    "clb_coo_release": (C.c_int, [vp, P(clb_coo)]),
+    "clb_csr_release": (C.c_int, [vp, P(clb_csr)]),
+    "clb_prefix_sum_u32": (C.c_int, [vp, vp, C.c_uint64, P(C.c_uint64)]),
+    "clb_prefix_sum_u64": (C.c_int, [vp, vp, C.c_uint64, P(C.c_uint64)]),
+    "clb_fill_u32": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32]),
+    "clb_coo_to_dcsr": (C.c_int, [vp, P(clb_coo), P(clb_dcsr), C.c_int]),
+    "clb_dcsr_to_coo": (C.c_int, [vp, P(clb_dcsr), P(clb_coo), C.c_int]),
+    "clb_dcsr_to_csr": (C.c_int, [vp, P(clb_dcsr), P(clb_csr)]),
+    "clb_csr_to_dcsr": (C.c_int, [vp, P(clb_csr), P(clb_dcsr)]),
+    "clb_dcsr_spgemm_hash": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_stats)]),
+    "clb_dcsr_workload": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, P(C.c_uint64)]),
+}
+
+# Entry points added as the library grows; bound when present.
+_OPTIONAL = {
+    "clb_coo_reduce_duplicates": (C.c_int, [vp, P(clb_coo), P(clb_coo)]),
+    "clb_coo_sort": (C.c_int, [vp, vp, vp, C.c_uint64]),
+    "clb_dcsr_spgemm_esc": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_stats)]),
+    "clb_coo_add": (C.c_int, [vp, P(clb_coo), P(clb_coo), P(clb_coo)]),
+    "clb_csr_add": (C.c_int, [vp, P(clb_csr), P(clb_csr), P(clb_csr)]),
+    "clb_dcsr_kronecker": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr)]),
+    "clb_dcsr_transpose": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr)]),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libclbool_b200.so not built ({LIB_PATH}); run `python clbool_b200/build.py`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGS.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    for name, (res, args) in _OPTIONAL.items():
+        f = getattr(lib, name, None)
+        if f is not None:
+            f.restype = res
+            f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def declared_symbols() -> list[str]:
+    return sorted(list(_SIGS) + list(_OPTIONAL))

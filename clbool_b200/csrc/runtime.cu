@@ -1,0 +1,311 @@
+// runtime.cu -- controls, memory, copies and error reporting of the C ABI.
+//
+// Replaces the reference's Controls (src/core/controls.hpp:12-28: one
+// device, an in-order queue and an out-of-order queue) and
+// create_controls/show_devices (src/common/env.cpp:7-54) with one CUDA
+// device, one stream and a stream-ordered memory pool.  There is no JIT
+// kernel cache (src/core/kernel_cache.hpp): every kernel is compiled ahead
+// of time for sm_100a.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+
+namespace clb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int fail(int status, const std::string &msg) {
+    g_last_error = std::string(clb_status_string(status)) + ": " + msg;
+    return status;
+}
+
+void *dev_alloc(clb_controls *ctl, size_t bytes) {
+    if (bytes == 0) return nullptr;
+    if (ctl->alloc) return ctl->alloc(ctl->alloc_ctx, bytes, (void *)ctl->stream);
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, bytes, ctl->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void dev_free(clb_controls *ctl, void *p) {
+    if (!p) return;
+    if (ctl->release) {
+        ctl->release(ctl->alloc_ctx, p, (void *)ctl->stream);
+        return;
+    }
+    cudaFreeAsync(p, ctl->stream);
+}
+
+int read_scalars(clb_controls *ctl, const uint64_t *d_src, uint64_t *h_dst, int count) {
+    CLB_TRY_CUDA(cudaMemcpyAsync(ctl->h_scalars, d_src, sizeof(uint64_t) * count, cudaMemcpyDeviceToHost, ctl->stream),
+                 CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    memcpy(h_dst, ctl->h_scalars, sizeof(uint64_t) * count);
+    return CLB_SUCCESS;
+}
+
+int clear_status(clb_controls *ctl) {
+    CLB_TRY_CUDA(cudaMemsetAsync(ctl->d_status, 0, sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    return CLB_SUCCESS;
+}
+
+int check_status(clb_controls *ctl, const char *op) {
+    CLB_TRY_CUDA(cudaMemcpyAsync(ctl->h_scalars + 63, ctl->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 ctl->stream),
+                 CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    uint32_t s = (uint32_t)(ctl->h_scalars[63] & 0xFFFFFFFFu);
+    if (s != 0) {
+        char buf[160];
+        snprintf(buf, sizeof(buf), "%s: device status word 0x%x", op, s);
+        return fail(CLB_DEVICE_STATUS_ERROR, buf);
+    }
+    return CLB_SUCCESS;
+}
+
+}  // namespace clb
+
+using namespace clb;
+
+extern "C" {
+
+const char *clb_status_string(int s) {
+    switch (s) {
+        case CLB_SUCCESS: return "CLBOOL_SUCCESS";
+        case CLB_NO_SUCH_PROGRAM: return "CLBOOL_NO_SUCH_PROGRAM";
+        case CLB_CREATE_KERNEL_ERROR: return "CLBOOL_CREATE_KERNEL_ERROR";
+        case CLB_BUILD_PROGRAM_ERROR: return "CLBOOL_BUILD_PROGRAM_ERROR";
+        case CLB_INCOMPLETE_KERNEL: return "CLBOOL_INCOMPLETE_KERNEL";
+        case CLB_RUN_KERNEL_FAILURE: return "CLBOOL_RUN_KERNEL_FAILURE";
+        case CLB_EVENT_WAITING_ERROR: return "CLBOOL_EVENT_WAITING_ERROR";
+        case CLB_CREATE_BUFFER_ERROR: return "CLBOOL_CREATE_BUFFER_ERROR";
+        case CLB_COPY_BUFFER_ERROR: return "CLBOOL_COPY_BUFFER_ERROR";
+        case CLB_READ_BUFFER_ERROR: return "CLBOOL_READ_BUFFER_ERROR";
+        case CLB_WRITE_BUFFER_ERROR: return "CLBOOL_WRITE_BUFFER_ERROR";
+        case CLB_CREATE_CONTROLS_ERROR: return "CLBOOL_CREATE_CONTROLS_ERROR";
+        case CLB_INVALID_ARGUMENT: return "CLBOOL_INVALID_ARGUMENT";
+        case CLB_INVALID_VALUE: return "CLBOOL_INVALID_VALUE";
+        case CLB_INITIALIZATION_ERROR: return "CLBOOL_INITIALIZATION_ERROR";
+        case CLB_DEVICE_STATUS_ERROR: return "CLBOOL_DEVICE_STATUS_ERROR";
+        case CLB_NOT_SUPPORTED: return "CLBOOL_NOT_SUPPORTED";
+        default: return "CLBOOL_UNKNOWN_STATUS";
+    }
+}
+
+const char *clb_last_error(void) { return g_last_error.c_str(); }
+
+int clb_version(void) { return 100; }
+
+int clb_device_count(int *count) {
+    if (!count) return fail(CLB_INVALID_ARGUMENT, "count is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return CLB_SUCCESS;
+}
+
+int clb_device_info(int device, char *name, size_t name_len, int *sm_count, uint64_t *total_mem) {
+    int n = 0;
+    clb_device_count(&n);
+    if (device < 0 || device >= n)
+        return fail(CLB_CREATE_CONTROLS_ERROR, "no CUDA device with id " + std::to_string(device));
+    cudaDeviceProp p;
+    CLB_TRY_CUDA(cudaGetDeviceProperties(&p, device), CLB_CREATE_CONTROLS_ERROR);
+    if (name && name_len) {
+        strncpy(name, p.name, name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    if (sm_count) *sm_count = p.multiProcessorCount;
+    if (total_mem) *total_mem = p.totalGlobalMem;
+    return CLB_SUCCESS;
+}
+
+int clb_controls_create(int device, clb_controls **out) {
+    if (!out) return fail(CLB_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    clb_device_count(&n);
+    if (device < 0 || device >= n)
+        return fail(CLB_CREATE_CONTROLS_ERROR, "no CUDA device with id " + std::to_string(device));
+    int prev = -1;
+    cudaGetDevice(&prev);
+    CLB_TRY_CUDA(cudaSetDevice(device), CLB_CREATE_CONTROLS_ERROR);
+    clb_controls *ctl = new clb_controls();
+    ctl->device = device;
+    cudaDeviceProp p;
+    cudaError_t e = cudaGetDeviceProperties(&p, device);
+    if (e == cudaSuccess) {
+        ctl->sm_count = p.multiProcessorCount;
+        ctl->smem_optin = p.sharedMemPerBlockOptin;
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctl->stream, cudaStreamNonBlocking);
+    ctl->own_stream = true;
+    if (e == cudaSuccess) e = cudaMallocHost(&ctl->h_scalars, 64 * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&ctl->d_status, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(ctl->d_status, 0, sizeof(uint32_t));
+    if (e == cudaSuccess) {
+        // Keep freed pool memory cached: repeated calls reuse it instead of
+        // returning it to the driver at every synchronisation.
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        std::string msg = cudaGetErrorString(e);
+        clb_controls_destroy(ctl);
+        return fail(CLB_CREATE_CONTROLS_ERROR, msg);
+    }
+    *out = ctl;
+    return CLB_SUCCESS;
+}
+
+int clb_controls_destroy(clb_controls *ctl) {
+    if (!ctl) return CLB_SUCCESS;
+    DeviceGuard g(ctl);
+    if (ctl->stream) cudaStreamSynchronize(ctl->stream);
+    if (ctl->own_stream && ctl->stream) cudaStreamDestroy(ctl->stream);
+    if (ctl->h_scalars) cudaFreeHost(ctl->h_scalars);
+    if (ctl->d_status) cudaFree(ctl->d_status);
+    delete ctl;
+    return CLB_SUCCESS;
+}
+
+int clb_controls_set_stream(clb_controls *ctl, void *stream) {
+    if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
+    DeviceGuard g(ctl);
+    if (ctl->own_stream && ctl->stream) {
+        cudaStreamSynchronize(ctl->stream);
+        cudaStreamDestroy(ctl->stream);
+    }
+    if (stream) {
+        ctl->stream = (cudaStream_t)stream;
+        ctl->own_stream = false;
+    } else {
+        CLB_TRY_CUDA(cudaStreamCreateWithFlags(&ctl->stream, cudaStreamNonBlocking), CLB_CREATE_CONTROLS_ERROR);
+        ctl->own_stream = true;
+    }
+    return CLB_SUCCESS;
+}
+
+void *clb_controls_get_stream(clb_controls *ctl) { return ctl ? (void *)ctl->stream : nullptr; }
+
+int clb_controls_device(clb_controls *ctl) { return ctl ? ctl->device : -1; }
+
+int clb_controls_set_allocator(clb_controls *ctl, clb_alloc_fn alloc, clb_free_fn release, void *ctx) {
+    if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
+    if ((alloc == nullptr) != (release == nullptr))
+        return fail(CLB_INVALID_ARGUMENT, "allocator needs both alloc and release (or neither)");
+    ctl->alloc = alloc;
+    ctl->release = release;
+    ctl->alloc_ctx = ctx;
+    return CLB_SUCCESS;
+}
+
+int clb_controls_sync(clb_controls *ctl) {
+    if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    return CLB_SUCCESS;
+}
+
+int clb_malloc(clb_controls *ctl, size_t bytes, void **out) {
+    if (!ctl || !out) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    *out = nullptr;
+    if (bytes == 0) return fail(CLB_CREATE_BUFFER_ERROR, "zero-size buffer");
+    void *p = dev_alloc(ctl, bytes);
+    if (!p) return fail(CLB_CREATE_BUFFER_ERROR, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    *out = p;
+    return CLB_SUCCESS;
+}
+
+int clb_free(clb_controls *ctl, void *ptr) {
+    if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
+    if (!ptr) return CLB_SUCCESS;
+    DeviceGuard g(ctl);
+    dev_free(ctl, ptr);
+    return CLB_SUCCESS;
+}
+
+static int copy_sync(clb_controls *ctl, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, int err) {
+    if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
+    if (bytes == 0) return CLB_SUCCESS;
+    if (!dst || !src) return fail(CLB_INVALID_ARGUMENT, "NULL pointer");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, ctl->stream), err);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    return CLB_SUCCESS;
+}
+
+int clb_memcpy_h2d(clb_controls *ctl, void *dst, const void *src, size_t bytes) {
+    return copy_sync(ctl, dst, src, bytes, cudaMemcpyHostToDevice, CLB_WRITE_BUFFER_ERROR);
+}
+int clb_memcpy_d2h(clb_controls *ctl, void *dst, const void *src, size_t bytes) {
+    return copy_sync(ctl, dst, src, bytes, cudaMemcpyDeviceToHost, CLB_READ_BUFFER_ERROR);
+}
+int clb_memcpy_d2d(clb_controls *ctl, void *dst, const void *src, size_t bytes) {
+    return copy_sync(ctl, dst, src, bytes, cudaMemcpyDeviceToDevice, CLB_COPY_BUFFER_ERROR);
+}
+
+int clb_host_alloc(size_t bytes, void **out) {
+    if (!out) return fail(CLB_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (bytes == 0) return CLB_SUCCESS;
+    CLB_TRY_CUDA(cudaMallocHost(out, bytes), CLB_CREATE_BUFFER_ERROR);
+    return CLB_SUCCESS;
+}
+
+int clb_host_free(void *ptr) {
+    if (ptr) CLB_TRY_CUDA(cudaFreeHost(ptr), CLB_RUN_KERNEL_FAILURE);
+    return CLB_SUCCESS;
+}
+
+int clb_dcsr_release(clb_controls *ctl, clb_dcsr *m) {
+    if (!ctl || !m) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    dev_free(ctl, m->rpt);
+    dev_free(ctl, m->rows);
+    dev_free(ctl, m->cols);
+    m->rpt = nullptr;
+    m->rows = nullptr;
+    m->cols = nullptr;
+    m->nnz = m->nzr = 0;
+    return CLB_SUCCESS;
+}
+
+int clb_coo_release(clb_controls *ctl, clb_coo *m) {
+    if (!ctl || !m) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    dev_free(ctl, m->rows);
+    dev_free(ctl, m->cols);
+    m->rows = m->cols = nullptr;
+    m->nnz = 0;
+    return CLB_SUCCESS;
+}
+
+int clb_csr_release(clb_controls *ctl, clb_csr *m) {
+    if (!ctl || !m) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    dev_free(ctl, m->rpt);
+    dev_free(ctl, m->cols);
+    m->rpt = nullptr;
+    m->cols = nullptr;
+    m->nnz = 0;
+    return CLB_SUCCESS;
+}
+
+}  // extern "C"

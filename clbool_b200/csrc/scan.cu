@@ -1,0 +1,153 @@
+// scan.cu -- exclusive prefix sums (prefix_sum, src/common/cl_operations.cpp:4-88).
+//
+// The reference runs a recursive Blelloch scan with a host wait after every
+// level and a blocking read of the total.  Here a scan is three
+// stream-ordered kernels with no host synchronisation:
+//   1. tile_reduce: every 4096-element tile sums its inputs (64-bit);
+//   2. tiles_scan : one CTA scans the tile sums and writes the grand total;
+//   3. downsweep  : every tile rescans its inputs from its tile offset.
+// Each warp owns a contiguous 512-element segment and walks it in 32-wide
+// coalesced steps with a shuffle scan, so loads and stores are fully
+// coalesced and no shared-memory transpose is needed.
+#include "common.cuh"
+
+namespace clb {
+
+namespace {
+
+constexpr int SCAN_NT = 256;
+constexpr int SCAN_WARPS = SCAN_NT / 32;
+constexpr int SCAN_ITEMS = 16;                          // 32-wide steps per warp
+constexpr uint64_t SCAN_SEG = 32ull * SCAN_ITEMS;       // elements per warp
+constexpr uint64_t SCAN_TILE = SCAN_SEG * SCAN_WARPS;   // elements per CTA
+
+template <class TIn>
+__device__ __forceinline__ uint64_t warp_segment_sum(const TIn *in, uint64_t seg_beg, uint64_t n) {
+    uint64_t s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        uint64_t idx = seg_beg + (uint64_t)i * 32 + lane_id();
+        if (idx < n) s += (uint64_t)in[idx];
+    }
+    return warp_sum(s);
+}
+
+template <class TIn>
+__global__ void __launch_bounds__(SCAN_NT) tile_reduce_kernel(const TIn *__restrict__ in, uint64_t n,
+                                                              uint64_t *__restrict__ tile_sums) {
+    __shared__ uint64_t wsum[SCAN_WARPS];
+    uint64_t tile_beg = (uint64_t)blockIdx.x * SCAN_TILE;
+    uint64_t s = warp_segment_sum(in, tile_beg + warp_id() * SCAN_SEG, n);
+    if (lane_id() == 0) wsum[warp_id()] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t t = 0;
+#pragma unroll
+        for (int w = 0; w < SCAN_WARPS; ++w) t += wsum[w];
+        tile_sums[blockIdx.x] = t;
+    }
+}
+
+constexpr int TS_NT = 1024;
+
+__global__ void __launch_bounds__(TS_NT) tiles_scan_kernel(uint64_t *__restrict__ sums, uint64_t ntiles,
+                                                           uint64_t *__restrict__ d_total) {
+    __shared__ uint64_t scratch[33];
+    uint64_t carry = 0;
+    for (uint64_t base = 0; base < ntiles; base += TS_NT) {
+        uint64_t i = base + threadIdx.x;
+        uint64_t v = i < ntiles ? sums[i] : 0;
+        uint64_t tot;
+        uint64_t ex = block_exclusive_scan<uint64_t, TS_NT>(v, scratch, &tot);
+        if (i < ntiles) sums[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && d_total) *d_total = carry;
+}
+
+template <class TIn, class TOut>
+__global__ void __launch_bounds__(SCAN_NT) downsweep_kernel(const TIn *in, TOut *out, uint64_t n,
+                                                            const uint64_t *__restrict__ tile_offsets) {
+    __shared__ uint64_t wsum[SCAN_WARPS];
+    uint64_t tile_beg = (uint64_t)blockIdx.x * SCAN_TILE;
+    uint64_t seg_beg = tile_beg + warp_id() * SCAN_SEG;
+    uint64_t s = warp_segment_sum(in, seg_beg, n);
+    if (lane_id() == 0) wsum[warp_id()] = s;
+    __syncthreads();
+    uint64_t carry = tile_offsets[blockIdx.x];
+    for (unsigned w = 0; w < warp_id(); ++w) carry += wsum[w];
+    // The segment is read fully by warp_segment_sum before any write below,
+    // and no other warp touches it, so `out` may alias `in`.
+#pragma unroll 4
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        uint64_t idx = seg_beg + (uint64_t)i * 32 + lane_id();
+        uint64_t v = idx < n ? (uint64_t)in[idx] : 0;
+        uint64_t inc = warp_inclusive_scan(v);
+        if (idx < n) out[idx] = (TOut)(carry + inc - v);
+        carry += __shfl_sync(0xFFFFFFFFu, inc, 31);
+    }
+}
+
+template <class TIn, class TOut>
+int scan_impl(clb_controls *ctl, const TIn *in, TOut *out, uint64_t n, uint64_t *d_total) {
+    if (n == 0) {
+        if (d_total) CLB_TRY_CUDA(cudaMemsetAsync(d_total, 0, sizeof(uint64_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+        return CLB_SUCCESS;
+    }
+    uint64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (ntiles > 0x7FFFFFFFull) return fail(CLB_NOT_SUPPORTED, "scan too long");
+    Temp<uint64_t> sums;
+    CLB_RETURN_IF(sums.alloc(ctl, ntiles));
+    tile_reduce_kernel<TIn><<<(unsigned)ntiles, SCAN_NT, 0, ctl->stream>>>(in, n, sums.ptr);
+    tiles_scan_kernel<<<1, TS_NT, 0, ctl->stream>>>(sums.ptr, ntiles, d_total);
+    downsweep_kernel<TIn, TOut><<<(unsigned)ntiles, SCAN_NT, 0, ctl->stream>>>(in, out, n, sums.ptr);
+    ctl->launches += 3;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+}  // namespace
+
+int scan_u32_to_u64(clb_controls *ctl, const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *d_total) {
+    return scan_impl<uint32_t, uint64_t>(ctl, in, out, n, d_total);
+}
+
+int scan_u32_inplace(clb_controls *ctl, uint32_t *data, uint64_t n, uint64_t *d_total) {
+    return scan_impl<uint32_t, uint32_t>(ctl, data, data, n, d_total);
+}
+
+int scan_u64_inplace(clb_controls *ctl, uint64_t *data, uint64_t n, uint64_t *d_total) {
+    return scan_impl<uint64_t, uint64_t>(ctl, data, data, n, d_total);
+}
+
+}  // namespace clb
+
+using namespace clb;
+
+extern "C" {
+
+int clb_prefix_sum_u32(clb_controls *ctl, uint32_t *array, uint64_t n, uint64_t *total) {
+    if (!ctl || (n && !array)) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    Temp<uint64_t> t;
+    CLB_RETURN_IF(t.alloc(ctl, 1));
+    CLB_RETURN_IF(scan_u32_inplace(ctl, array, n, t.ptr));
+    uint64_t h = 0;
+    CLB_RETURN_IF(read_scalars(ctl, t.ptr, &h, 1));
+    if (total) *total = h;
+    return CLB_SUCCESS;
+}
+
+int clb_prefix_sum_u64(clb_controls *ctl, uint64_t *array, uint64_t n, uint64_t *total) {
+    if (!ctl || (n && !array)) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    Temp<uint64_t> t;
+    CLB_RETURN_IF(t.alloc(ctl, 1));
+    CLB_RETURN_IF(scan_u64_inplace(ctl, array, n, t.ptr));
+    uint64_t h = 0;
+    CLB_RETURN_IF(read_scalars(ctl, t.ptr, &h, 1));
+    if (total) *total = h;
+    return CLB_SUCCESS;
+}
+
+}  // extern "C"

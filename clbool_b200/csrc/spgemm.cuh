@@ -1,0 +1,27 @@
+// spgemm.cuh -- host-side entry points shared by the SpGEMM forms.
+#pragma once
+
+#include "spgemm_kernels.cuh"
+
+namespace clb {
+
+int validate_spgemm(const clb_dcsr &A, const clb_dcsr &B);
+// Builds B's dense row map when worthwhile and fills the row view.
+int prepare_b(clb_controls *ctl, const clb_dcsr &B, Temp<uint64_t> &dense, BRows &b);
+// work[i] = products of A row i; *d_total += their sum.
+int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t *work, uint64_t *d_total);
+// Histogram + scatter of the rows into accumulator bins.  The bound of
+// distinct columns is cap[i] when cap is non-null, else min(work[i], ncols).
+// flags[i] = 1 for rows with products (input of the C row-position scan).
+int launch_binning(clb_controls *ctl, const uint32_t *work, const uint32_t *cap, uint64_t n, uint64_t ncols,
+                   uint32_t *info, uint32_t *list, uint32_t *flags);
+// Runs every bin's accumulator kernel (symbolic or numeric).
+int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, const AView &a, const BRows &b,
+                        const RowOut &o, uint64_t ncols, uint64_t nrows_max);
+// C.rpt/C.rows from the row flags' exclusive scan (pos) and the row offsets.
+int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
+                    const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz);
+int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
+                         clb_spgemm_stats *stats);
+
+}  // namespace clb

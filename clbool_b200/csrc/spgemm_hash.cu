@@ -1,0 +1,218 @@
+// spgemm_hash.cu -- dcsr::matrix_multiplication_hash, exact two-pass form.
+//
+// Reference: src/dcsr/dcsr_matrix_multiplication_hash.cpp:51-119 (flow),
+// count_workload (dcsr_matrix_multiplication.cpp:388-404, count_workload.cl),
+// binning (..._hash.cpp:13-47, 301-345), count_nnz (:122-201), fill_nnz
+// (:203-299).  Differences of mechanism, not of result:
+//   * B's rows are found through a dense row map built once per call (two
+//     loads) instead of a binary search per A entry;
+//   * binning is a device histogram + scatter (no host loop, no host copy of
+//     the workload);
+//   * C's row list is known right after the workload pass (a row has output
+//     iff it has products), so no empty-row compaction pass runs at the end;
+//   * offsets are 64-bit.
+#include <cstring>
+#include <string>
+
+#include "spgemm.cuh"
+
+namespace clb {
+
+namespace {
+
+constexpr int WL_NT = 256;
+constexpr int WL_GROUP = 8;  // lanes per A row in the workload kernel
+
+__global__ void __launch_bounds__(WL_NT) workload_kernel(AView a, BRows b, uint32_t *__restrict__ work,
+                                                         unsigned long long *__restrict__ total) {
+    __shared__ unsigned long long ptot;
+    if (threadIdx.x == 0) ptot = 0;
+    __syncthreads();
+    const uint32_t gl = threadIdx.x & (WL_GROUP - 1);
+    const uint32_t gmask = 0xFFu << (lane_id() & 24u);
+    unsigned long long mine = 0;
+    for (uint64_t row = ((uint64_t)blockIdx.x * WL_NT + threadIdx.x) / WL_GROUP; row < a.nzr;
+         row += (uint64_t)gridDim.x * (WL_NT / WL_GROUP)) {
+        const uint64_t ja = a.rpt[row], je = a.rpt[row + 1];
+        uint32_t s = 0;
+        for (uint64_t j = ja + gl; j < je; j += WL_GROUP) {
+            uint64_t bb;
+            s += b_row(b, __ldg(a.cols + j), bb);
+        }
+#pragma unroll
+        for (int d = WL_GROUP / 2; d > 0; d >>= 1) s += __shfl_xor_sync(gmask, s, d);
+        if (gl == 0) {
+            work[row] = s;
+            mine += s;
+        }
+    }
+    if (mine) atomicAdd(&ptot, mine);
+    __syncthreads();
+    if (threadIdx.x == 0 && ptot) atomicAdd(total, ptot);
+}
+
+}  // namespace
+
+int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t *work, uint64_t *d_total) {
+    unsigned grid = persistent_grid(ctl, 8, ceil_div_u(a.nzr, WL_NT / WL_GROUP));
+    workload_kernel<<<grid, WL_NT, 0, ctl->stream>>>(a, b, work, (unsigned long long *)d_total);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+int prepare_b(clb_controls *ctl, const clb_dcsr &B, Temp<uint64_t> &dense, BRows &b) {
+    b.rpt = B.rpt;
+    b.rows = B.rows;
+    b.cols = B.cols;
+    b.nzr = B.nzr;
+    b.nrows = B.nrows;
+    b.dense = nullptr;
+    if (use_dense_map(B.nrows, B.nnz)) {
+        CLB_RETURN_IF(dense.alloc(ctl, B.nrows + 1));
+        CLB_RETURN_IF(dcsr_dense_rpt(ctl, &B, dense.ptr));
+        b.dense = dense.ptr;
+    }
+    return CLB_SUCCESS;
+}
+
+int validate_spgemm(const clb_dcsr &A, const clb_dcsr &B) {
+    if (A.ncols != B.nrows)
+        return fail(CLB_INVALID_ARGUMENT, "Invalid input matrix size! a : " + std::to_string(A.nrows) + " x " +
+                                              std::to_string(A.ncols) + ", b: " + std::to_string(B.nrows) + " x " +
+                                              std::to_string(B.ncols));
+    if (B.nnz >= (1ull << 32) || A.nzr >= (1ull << 32))
+        return fail(CLB_NOT_SUPPORTED, "right operand with 2^32 or more entries, or left with 2^32 stored rows");
+    if (B.ncols > 0xFFFFFFFFull) return fail(CLB_NOT_SUPPORTED, "more than 2^32-1 columns");
+    if ((A.nnz && (!A.rpt || !A.rows || !A.cols)) || (B.nnz && (!B.rpt || !B.rows || !B.cols)))
+        return fail(CLB_INVALID_ARGUMENT, "matrix with entries but NULL arrays");
+    return CLB_SUCCESS;
+}
+
+int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
+                         clb_spgemm_stats *stats) {
+    clb_dcsr C{};
+    C.nrows = A.nrows;
+    C.ncols = B.ncols;
+    clb_spgemm_stats st{};
+    ctl->launches = 0;
+    if (A.nnz == 0 || B.nnz == 0 || A.nzr == 0 || B.nzr == 0) {
+        *out = C;
+        if (stats) *stats = st;
+        return CLB_SUCCESS;
+    }
+    CLB_RETURN_IF(clear_status(ctl));
+    const AView a{A.rpt, A.rows, A.cols, A.nzr};
+    BRows b;
+    Temp<uint64_t> dense;
+    CLB_RETURN_IF(prepare_b(ctl, B, dense, b));
+
+    const uint64_t n = A.nzr;
+    // scalars: [0] products, [1] nnz(C), [2] nzr(C)
+    Temp<uint64_t> scal;
+    CLB_RETURN_IF(scal.alloc(ctl, 4));
+    CLB_TRY_CUDA(cudaMemsetAsync(scal.ptr, 0, 4 * sizeof(uint64_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    Temp<uint32_t> work, row_nnz, flags, list, info;
+    Temp<uint64_t> off;
+    CLB_RETURN_IF(work.alloc(ctl, n));
+    CLB_RETURN_IF(row_nnz.alloc(ctl, n));
+    CLB_RETURN_IF(flags.alloc(ctl, n));
+    CLB_RETURN_IF(list.alloc(ctl, n));
+    CLB_RETURN_IF(info.alloc(ctl, 2 * NUM_BINS));
+    CLB_RETURN_IF(off.alloc(ctl, n));
+
+    CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, scal.ptr + 0));
+    CLB_RETURN_IF(launch_binning(ctl, work.ptr, nullptr, n, B.ncols, info.ptr, list.ptr, flags.ptr));
+    CLB_TRY_CUDA(cudaMemsetAsync(row_nnz.ptr, 0, n * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+
+    BinLists bl{list.ptr, info.ptr};
+    RowOut sym{row_nnz.ptr, nullptr, nullptr, nullptr, nullptr, ctl->d_status};
+    CLB_RETURN_IF(launch_accumulators(ctl, false, bl, a, b, sym, B.ncols, n));
+
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, row_nnz.ptr, off.ptr, n, scal.ptr + 1));
+    CLB_RETURN_IF(scan_u32_inplace(ctl, flags.ptr, n, scal.ptr + 2));
+    uint64_t h[3];
+    CLB_RETURN_IF(read_scalars(ctl, scal.ptr, h, 3));
+    uint32_t hinfo[NUM_BINS];
+    CLB_TRY_CUDA(cudaMemcpy(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost), CLB_READ_BUFFER_ERROR);
+    st.products = h[0];
+    const uint64_t nnz = h[1], nzr = h[2];
+    st.nnz = nnz;
+    st.nzr = nzr;
+    for (int k = 0; k < NUM_BINS; ++k) st.rows_per_bin[k] = hinfo[k];
+    if (nnz == 0) {
+        CLB_RETURN_IF(check_status(ctl, "matrix_multiplication_hash"));
+        st.kernel_launches = ctl->launches;
+        *out = C;
+        if (stats) *stats = st;
+        return CLB_SUCCESS;
+    }
+
+    Temp<uint64_t> c_rpt;
+    Temp<uint32_t> c_rows, c_cols;
+    CLB_RETURN_IF(c_rpt.alloc(ctl, nzr + 1));
+    CLB_RETURN_IF(c_rows.alloc(ctl, nzr));
+    CLB_RETURN_IF(c_cols.alloc(ctl, nnz));
+    CLB_RETURN_IF(launch_assemble(ctl, work.ptr, flags.ptr, off.ptr, A.rows, n, c_rpt.ptr, c_rows.ptr, nzr, nnz));
+
+    RowOut num{nullptr, off.ptr, nullptr, nullptr, c_cols.ptr, ctl->d_status};
+    CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n));
+    CLB_RETURN_IF(check_status(ctl, "matrix_multiplication_hash"));
+
+    C.nnz = nnz;
+    C.nzr = nzr;
+    C.rpt = c_rpt.release_ownership();
+    C.rows = c_rows.release_ownership();
+    C.cols = c_cols.release_ownership();
+    *out = C;
+    st.kernel_launches = ctl->launches;
+    if (stats) *stats = st;
+    return CLB_SUCCESS;
+}
+
+}  // namespace clb
+
+using namespace clb;
+
+extern "C" {
+
+int clb_dcsr_spgemm_hash(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
+                         clb_spgemm_stats *stats) {
+    if (!ctl || !a || !b || !c) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    const clb_dcsr A = *a, B = *b;
+    CLB_RETURN_IF(validate_spgemm(A, B));
+    DeviceGuard g(ctl);
+    return spgemm_hash_two_pass(ctl, A, B, c, stats);
+}
+
+int clb_dcsr_workload(clb_controls *ctl, const clb_dcsr *a_, const clb_dcsr *b_, uint32_t *workload,
+                      uint64_t *total) {
+    if (!ctl || !a_ || !b_) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    const clb_dcsr A = *a_, B = *b_;
+    CLB_RETURN_IF(validate_spgemm(A, B));
+    DeviceGuard g(ctl);
+    if (A.nzr == 0) {
+        if (total) *total = 0;
+        return CLB_SUCCESS;
+    }
+    if (!workload) return fail(CLB_INVALID_ARGUMENT, "workload is NULL");
+    if (B.nnz == 0) {
+        CLB_TRY_CUDA(cudaMemsetAsync(workload, 0, A.nzr * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+        CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+        if (total) *total = 0;
+        return CLB_SUCCESS;
+    }
+    const AView a{A.rpt, A.rows, A.cols, A.nzr};
+    BRows b;
+    Temp<uint64_t> dense, tot;
+    CLB_RETURN_IF(prepare_b(ctl, B, dense, b));
+    CLB_RETURN_IF(tot.alloc(ctl, 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(tot.ptr, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_RETURN_IF(launch_workload(ctl, a, b, workload, tot.ptr));
+    uint64_t h = 0;
+    CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &h, 1));
+    if (total) *total = h;
+    return CLB_SUCCESS;
+}
+
+}  // extern "C"

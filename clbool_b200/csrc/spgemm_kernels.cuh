@@ -1,0 +1,415 @@
+// spgemm_kernels.cuh -- row accumulators of the boolean SpGEMM, shared by
+// the exact two-pass form and the learned single-pass form.
+//
+// Reference algorithm (src/dcsr/dcsr_matrix_multiplication_hash.cpp:51-119):
+// products per A row -> bins by size -> per-bin symbolic count -> scan ->
+// per-bin numeric fill.  The accumulators here are designed for sm_100a:
+//   * warp ESC (rows with <= 256 products): the warp copies the products into
+//     a private shared buffer, sorts them in registers with a bitonic network
+//     over shuffles, and drops duplicates with one neighbour shuffle;
+//   * CTA hash (<= 4096 distinct columns possible): open-addressing table in
+//     shared memory (Fibonacci hashing, linear probing, bounded), then a
+//     shared-memory bitonic sort of the compacted keys;
+//   * CTA bitmap (heavy rows): a 128 KB shared-memory bitmap over a column
+//     chunk; the population count is the symbolic result and a warp scan of
+//     per-word counts emits the columns already sorted (no sort pass).
+#pragma once
+
+#include "common.cuh"
+
+namespace clb {
+
+struct AView {
+    const uint64_t *rpt;
+    const uint32_t *rows;
+    const uint32_t *cols;
+    uint64_t nzr;
+};
+
+// Accumulator bins (bin 0 = rows without products, not listed).
+enum Bin : int {
+    BIN_NONE = 0,
+    BIN_W1 = 1,   // products <= 32
+    BIN_W2 = 2,   // <= 64
+    BIN_W4 = 3,   // <= 128
+    BIN_W8 = 4,   // <= 256
+    BIN_H1K = 5,  // distinct-column bound <= 512  -> table 1024
+    BIN_H2K = 6,  // <= 1024 -> 2048
+    BIN_H4K = 7,  // <= 2048 -> 4096
+    BIN_H8K = 8,  // <= 4096 -> 8192
+    BIN_BMP = 9,  // bitmap
+    NUM_BINS = 10
+};
+
+// Bin of a row from its product count and its distinct-column bound
+// (min(products, ncols), or a learned capacity).
+__host__ __device__ __forceinline__ int bin_of(uint64_t products, uint64_t distinct_bound) {
+    if (products == 0) return BIN_NONE;
+    if (products <= 32) return BIN_W1;
+    if (products <= 64) return BIN_W2;
+    if (products <= 128) return BIN_W4;
+    if (products <= 256) return BIN_W8;
+    if (distinct_bound <= 512) return BIN_H1K;
+    if (distinct_bound <= 1024) return BIN_H2K;
+    if (distinct_bound <= 2048) return BIN_H4K;
+    if (distinct_bound <= 4096) return BIN_H8K;
+    return BIN_BMP;
+}
+
+// Row lists of all bins packed in one array; info[b] = count of bin b,
+// info[NUM_BINS + b] = scatter cursor.  Offset of bin b = sum of counts below.
+struct BinLists {
+    const uint32_t *list;
+    const uint32_t *info;
+};
+
+__device__ __forceinline__ void bin_range(const BinLists &bl, int bin, uint32_t &beg, uint32_t &cnt) {
+    uint32_t o = 0;
+    for (int b = 1; b < bin; ++b) o += bl.info[b];
+    beg = o;
+    cnt = bl.info[bin];
+}
+
+// Output side of an accumulator.  Symbolic: row_nnz[i] = distinct columns.
+// Numeric: columns written at cols + row_off[i]; when row_cap is non-null
+// (learned form) a row whose count exceeds row_cap[i] is not written and is
+// flagged in overflow[i] instead.
+struct RowOut {
+    uint32_t *row_nnz;
+    const uint64_t *row_off;
+    const uint32_t *row_cap;
+    uint32_t *overflow;
+    uint32_t *cols;
+    uint32_t *status;
+};
+
+// ------------------------------------------------------------- warp ESC ----
+template <int E>
+__device__ __forceinline__ void warp_bitonic_sort(uint32_t (&v)[E]) {
+    constexpr int N = 32 * E;
+    const uint32_t lane = lane_id();
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= E) {
+                const int lx = j / E;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    uint32_t idx = lane * E + e;
+                    uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, v[e], lx);
+                    bool up = (idx & k) == 0;
+                    bool lower = (idx & j) == 0;
+                    v[e] = (up == lower) ? min(v[e], o) : max(v[e], o);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    if ((e & j) == 0) {
+                        const int e2 = e | j;
+                        uint32_t idx = lane * E + e;
+                        bool up = (idx & k) == 0;
+                        uint32_t x = v[e], y = v[e2];
+                        if ((x > y) == up) {
+                            v[e] = y;
+                            v[e2] = x;
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+constexpr int ESC_WARPS = 8;
+
+// One warp per row; the row's products (<= 32*E) are gathered into a
+// warp-private shared buffer, sorted in registers, deduplicated.
+template <int E, bool NUMERIC>
+__global__ void __launch_bounds__(ESC_WARPS * 32) warp_esc_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o) {
+    constexpr int N = 32 * E;
+    __shared__ uint32_t sbuf[ESC_WARPS][N];
+    uint32_t *buf = sbuf[warp_id()];
+    const uint32_t lane = lane_id();
+    uint32_t beg, cnt;
+    bin_range(bl, bin, beg, cnt);
+    for (uint32_t w = blockIdx.x * ESC_WARPS + warp_id(); w < cnt; w += gridDim.x * ESC_WARPS) {
+        const uint32_t i = bl.list[beg + w];
+        const uint64_t ja = a.rpt[i], je = a.rpt[i + 1];
+        uint32_t fill = 0;
+        for (uint64_t j0 = ja; j0 < je; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            uint64_t bb = 0;
+            uint32_t len = 0;
+            if (j < je) len = b_row(b, __ldg(a.cols + j), bb);
+            uint32_t inc = warp_inclusive_scan(len);
+            uint32_t off = fill + inc - len;
+            uint32_t mask = __ballot_sync(0xFFFFFFFFu, len > 0);
+            while (mask) {
+                const int src = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const uint64_t sb = __shfl_sync(0xFFFFFFFFu, bb, src);
+                const uint32_t sl = __shfl_sync(0xFFFFFFFFu, len, src);
+                const uint32_t so = __shfl_sync(0xFFFFFFFFu, off, src);
+                for (uint32_t t = lane; t < sl; t += 32) {
+                    if (so + t < (uint32_t)N) buf[so + t] = __ldg(b.cols + sb + t);
+                }
+            }
+            fill += __shfl_sync(0xFFFFFFFFu, inc, 31);
+        }
+        __syncwarp();
+        if (fill > (uint32_t)N) {  // binning guarantees fill <= N
+            if (lane == 0) raise_status(o.status, DEV_BOUNDS);
+            fill = N;
+        }
+        uint32_t v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            uint32_t idx = lane * E + e;
+            v[e] = idx < fill ? buf[idx] : EMPTY;
+        }
+        __syncwarp();
+        warp_bitonic_sort<E>(v);
+        const uint32_t prev_last = __shfl_up_sync(0xFFFFFFFFu, v[E - 1], 1);
+        uint32_t flags = 0, mine = 0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            bool first = (lane == 0 && e == 0);
+            uint32_t pv = (e == 0) ? prev_last : v[e > 0 ? e - 1 : 0];
+            bool f = v[e] != EMPTY && (first || v[e] != pv);
+            flags |= (f ? 1u : 0u) << e;
+            mine += f ? 1u : 0u;
+        }
+        if (!NUMERIC) {
+            uint32_t total = warp_sum(mine);
+            if (lane == 0) o.row_nnz[i] = total;
+        } else {
+            uint32_t inc = warp_inclusive_scan(mine);
+            uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
+            if (o.row_cap) {
+                if (total > o.row_cap[i]) {
+                    if (lane == 0) o.overflow[i] = 1;
+                    continue;
+                }
+                if (lane == 0) o.row_nnz[i] = total;
+            }
+            uint32_t *dst = o.cols + o.row_off[i] + (inc - mine);
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                if (flags & (1u << e)) *dst++ = v[e];
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------- CTA hash ----
+template <int T>
+__device__ __forceinline__ uint32_t hash_insert(uint32_t *table, uint32_t c, uint32_t *status) {
+    constexpr int LOG2T = (T == 1024) ? 10 : (T == 2048) ? 11 : (T == 4096) ? 12 : (T == 8192) ? 13 : 14;
+    uint32_t h = (c * 0x9E3779B1u) >> (32 - LOG2T);
+#pragma unroll 1
+    for (int probe = 0; probe < T; ++probe) {
+        uint32_t cur = *(volatile uint32_t *)(table + h);
+        if (cur == c) return 0;
+        if (cur == EMPTY) {
+            uint32_t prev = atomicCAS(table + h, EMPTY, c);
+            if (prev == EMPTY) return 1;
+            if (prev == c) return 0;
+        }
+        h = (h + 1) & (T - 1);
+    }
+    raise_status(status, DEV_PROBE_LIMIT);
+    return 0;
+}
+
+// Sort s[0, M) ascending, M a power of two; all NT threads participate.
+template <int NT>
+__device__ __forceinline__ void block_bitonic_sort(uint32_t *s, uint32_t M) {
+    for (uint32_t k = 2; k <= M; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < (M >> 1); t += NT) {
+                uint32_t lo = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                uint32_t hi = lo | j;
+                bool up = (lo & k) == 0;
+                uint32_t x = s[lo], y = s[hi];
+                if ((x > y) == up) {
+                    s[lo] = y;
+                    s[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Insert every product of A row i into an accumulator: warp per A entry,
+// lanes stride the B row, four independent loads in flight per lane.
+template <class F>
+__device__ __forceinline__ void for_each_product(const AView &a, const BRows &b, uint32_t i, int nwarps, F &&f) {
+    const uint32_t lane = lane_id();
+    const uint64_t ja = a.rpt[i], je = a.rpt[i + 1];
+    for (uint64_t j = ja + warp_id(); j < je; j += nwarps) {
+        uint64_t bb;
+        const uint32_t len = b_row(b, __ldg(a.cols + j), bb);
+        const uint32_t *src = b.cols + bb;
+        uint32_t t = lane;
+        for (; t + 96 < len; t += 128) {
+            uint32_t c0 = __ldg(src + t), c1 = __ldg(src + t + 32), c2 = __ldg(src + t + 64), c3 = __ldg(src + t + 96);
+            f(c0);
+            f(c1);
+            f(c2);
+            f(c3);
+        }
+        for (; t < len; t += 32) f(__ldg(src + t));
+    }
+}
+
+template <int T, int NT, bool NUMERIC>
+__global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o) {
+    constexpr int SPT = T / NT;  // slots per thread
+    __shared__ uint32_t table[T];
+    __shared__ uint32_t scratch[33];
+    uint32_t beg, cnt;
+    bin_range(bl, bin, beg, cnt);
+    for (uint32_t item = blockIdx.x; item < cnt; item += gridDim.x) {
+        const uint32_t i = bl.list[beg + item];
+        for (int s = threadIdx.x; s < T; s += NT) table[s] = EMPTY;
+        __syncthreads();
+        uint32_t mine = 0;
+        for_each_product(a, b, i, NT / 32, [&](uint32_t c) { mine += hash_insert<T>(table, c, o.status); });
+        __syncthreads();
+        if (!NUMERIC) {
+            uint32_t total = block_sum<uint32_t, NT>(mine, scratch);
+            if (threadIdx.x == 0) o.row_nnz[i] = total;
+            continue;
+        }
+        uint32_t keys[SPT];
+        uint32_t kc = 0;
+#pragma unroll
+        for (int s = 0; s < SPT; ++s) {
+            keys[s] = table[threadIdx.x * SPT + s];
+            kc += keys[s] != EMPTY ? 1u : 0u;
+        }
+        uint32_t nnz;
+        uint32_t w = block_exclusive_scan<uint32_t, NT>(kc, scratch, &nnz);
+        if (o.row_cap && nnz > o.row_cap[i]) {
+            if (threadIdx.x == 0) o.overflow[i] = 1;
+            continue;  // every thread takes this branch (nnz is block-uniform)
+        }
+#pragma unroll
+        for (int s = 0; s < SPT; ++s)
+            if (keys[s] != EMPTY) table[w++] = keys[s];
+        __syncthreads();
+        uint32_t M = 1;
+        while (M < nnz) M <<= 1;
+        for (uint32_t s = nnz + threadIdx.x; s < M; s += NT) table[s] = EMPTY;
+        __syncthreads();
+        block_bitonic_sort<NT>(table, M);
+        uint32_t *dst = o.cols + o.row_off[i];
+        for (uint32_t s = threadIdx.x; s < nnz; s += NT) dst[s] = table[s];
+        if (o.row_cap && threadIdx.x == 0) o.row_nnz[i] = nnz;
+        __syncthreads();
+    }
+}
+
+// ----------------------------------------------------------- CTA bitmap ----
+constexpr int BMP_NT = 1024;
+constexpr int BMP_NW = BMP_NT / 32;
+constexpr uint32_t BMP_MAX_WORDS = 32768;  // 128 KB: 2^20 columns per chunk
+
+// Words of the bitmap for `ncols` columns: a multiple of 32 * BMP_NW so the
+// warps split it evenly, at most BMP_MAX_WORDS.
+inline uint32_t bitmap_words(uint64_t ncols) {
+    uint64_t w = (ncols + 31) / 32;
+    uint64_t unit = 32ull * BMP_NW;
+    w = (w + unit - 1) / unit * unit;
+    if (w > BMP_MAX_WORDS) w = BMP_MAX_WORDS;
+    return (uint32_t)w;
+}
+
+template <bool NUMERIC>
+__global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o,
+                                                               uint64_t ncols, uint32_t W) {
+    extern __shared__ uint32_t bm[];
+    __shared__ uint32_t wtot[BMP_NW];
+    __shared__ uint32_t scratch[33];
+    uint32_t beg, cnt;
+    bin_range(bl, bin, beg, cnt);
+    for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) bm[w] = 0;
+    __syncthreads();
+    const uint32_t lane = lane_id(), wi = warp_id();
+    const uint32_t WPW = W / BMP_NW;  // words per warp in the emission pass
+    const uint64_t chunk_cols = (uint64_t)W * 32;
+    for (uint32_t item = blockIdx.x; item < cnt; item += gridDim.x) {
+        const uint32_t i = bl.list[beg + item];
+        uint64_t total = 0;
+        uint64_t out_base = NUMERIC ? o.row_off[i] : 0;
+        bool overflowed = false;
+        for (uint64_t c0 = 0; c0 < ncols; c0 += chunk_cols) {
+            for_each_product(a, b, i, BMP_NW, [&](uint32_t c) {
+                // unsigned wrap sends columns below c0 out of range too
+                uint64_t r = (uint64_t)c - c0;
+                if (r < chunk_cols) atomicOr(bm + (r >> 5), 1u << (r & 31));
+            });
+            __syncthreads();
+            if (!NUMERIC || overflowed) {
+                uint32_t mine = 0;
+                for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) {
+                    mine += __popc(bm[w]);
+                    bm[w] = 0;
+                }
+                total += block_sum<uint32_t, BMP_NT>(mine, scratch);
+                continue;
+            }
+            // Emission: each warp owns WPW consecutive words.
+            const uint32_t wbeg = wi * WPW;
+            uint32_t mine = 0;
+            for (uint32_t w = wbeg + lane; w < wbeg + WPW; w += 32) mine += __popc(bm[w]);
+            mine = warp_sum(mine);
+            if (lane == 0) wtot[wi] = mine;
+            __syncthreads();
+            uint64_t woff = 0, ctot = 0;
+            for (uint32_t q = 0; q < (uint32_t)BMP_NW; ++q) {
+                uint32_t v = wtot[q];
+                woff += q < wi ? v : 0;
+                ctot += v;
+            }
+            if (o.row_cap && total + ctot > o.row_cap[i]) {
+                // learned form: the row does not fit its slot; finish the
+                // count only (clears the bitmap) and flag it.
+                overflowed = true;
+                for (uint32_t w = wbeg + lane; w < wbeg + WPW; w += 32) bm[w] = 0;
+                total += ctot;
+                __syncthreads();
+                continue;
+            }
+            uint64_t run = out_base + total + woff;
+            for (uint32_t w = wbeg; w < wbeg + WPW; w += 32) {
+                uint32_t word = bm[w + lane];
+                bm[w + lane] = 0;
+                uint32_t pc = __popc(word);
+                uint32_t inc = warp_inclusive_scan(pc);
+                uint64_t pos = run + (inc - pc);
+                const uint32_t colbase = (uint32_t)(c0 + (uint64_t)(w + lane) * 32);
+                while (word) {
+                    const int bit = __ffs(word) - 1;
+                    word &= word - 1;
+                    o.cols[pos++] = colbase + (uint32_t)bit;
+                }
+                run += __shfl_sync(0xFFFFFFFFu, inc, 31);
+            }
+            total += ctot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            if (!NUMERIC) {
+                o.row_nnz[i] = (uint32_t)total;
+            } else if (o.row_cap) {
+                if (overflowed) o.overflow[i] = 1;
+                else o.row_nnz[i] = (uint32_t)total;
+            }
+        }
+    }
+}
+
+}  // namespace clb

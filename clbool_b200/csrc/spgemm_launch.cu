@@ -1,0 +1,169 @@
+// spgemm_launch.cu -- binning, C assembly and accumulator launches.
+#include <mutex>
+
+#include "spgemm.cuh"
+
+namespace clb {
+
+namespace {
+
+constexpr int BIN_NT = 256;
+
+__global__ void __launch_bounds__(BIN_NT) bin_count_kernel(const uint32_t *__restrict__ work,
+                                                           const uint32_t *__restrict__ cap, uint64_t n, uint64_t ncols,
+                                                           uint32_t *__restrict__ info, uint32_t *__restrict__ flags) {
+    __shared__ uint32_t hist[NUM_BINS];
+    if (threadIdx.x < NUM_BINS) hist[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint64_t i = (uint64_t)blockIdx.x * BIN_NT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * BIN_NT) {
+        uint32_t p = work[i];
+        uint64_t bound = cap ? (uint64_t)cap[i] : (p < ncols ? (uint64_t)p : ncols);
+        int bin = bin_of(p, bound);
+        atomicAdd(&hist[bin], 1u);
+        flags[i] = p > 0 ? 1u : 0u;
+    }
+    __syncthreads();
+    if (threadIdx.x < NUM_BINS && hist[threadIdx.x]) atomicAdd(&info[threadIdx.x], hist[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(BIN_NT) bin_scatter_kernel(const uint32_t *__restrict__ work,
+                                                             const uint32_t *__restrict__ cap, uint64_t n,
+                                                             uint64_t ncols, uint32_t *__restrict__ info,
+                                                             uint32_t *__restrict__ list) {
+    __shared__ uint32_t boff[NUM_BINS];
+    if (threadIdx.x == 0) {
+        uint32_t o = 0;
+        boff[0] = 0;
+        for (int b = 1; b < NUM_BINS; ++b) {
+            boff[b] = o;
+            o += info[b];
+        }
+    }
+    __syncthreads();
+    for (uint64_t i0 = (uint64_t)blockIdx.x * BIN_NT; i0 < n; i0 += (uint64_t)gridDim.x * BIN_NT) {
+        uint64_t i = i0 + threadIdx.x;
+        int bin = BIN_NONE;
+        if (i < n) {
+            uint32_t p = work[i];
+            uint64_t bound = cap ? (uint64_t)cap[i] : (p < ncols ? (uint64_t)p : ncols);
+            bin = bin_of(p, bound);
+        }
+        // warp-aggregated reservation per bin
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if ((int)lane_id() == leader && bin != BIN_NONE) base = atomicAdd(&info[NUM_BINS + bin], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+        if (bin != BIN_NONE) {
+            uint32_t rank = __popc(peers & ((1u << lane_id()) - 1u));
+            list[boff[bin] + base + rank] = (uint32_t)i;
+        }
+    }
+}
+
+__global__ void assemble_kernel(const uint32_t *__restrict__ work, const uint32_t *__restrict__ pos,
+                                const uint64_t *__restrict__ off, const uint32_t *__restrict__ a_rows, uint64_t n,
+                                uint64_t *__restrict__ c_rpt, uint32_t *__restrict__ c_rows, uint64_t nzr,
+                                uint64_t nnz) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (work[i] > 0) {
+            uint32_t p = pos[i];
+            c_rpt[p] = off[i];
+            c_rows[p] = a_rows[i];
+        }
+        if (i == 0) c_rpt[nzr] = nnz;
+    }
+}
+
+// Occupancy of each accumulator kernel, measured once per process.
+template <class K>
+int occupancy(K kernel, int nt, size_t dyn_smem) {
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, nt, dyn_smem) != cudaSuccess) {
+        cudaGetLastError();
+        blocks = 1;
+    }
+    return blocks > 0 ? blocks : 1;
+}
+
+template <int E, bool NUM>
+int launch_esc(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
+               uint64_t nmax) {
+    static int occ = occupancy(warp_esc_kernel<E, NUM>, ESC_WARPS * 32, 0);
+    unsigned grid = persistent_grid(ctl, occ, ceil_div_u(nmax, ESC_WARPS));
+    warp_esc_kernel<E, NUM><<<grid, ESC_WARPS * 32, 0, ctl->stream>>>(bl, bin, a, b, o);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+template <int T, int NT, bool NUM>
+int launch_hash(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
+                uint64_t nmax) {
+    static int occ = occupancy(hash_cta_kernel<T, NT, NUM>, NT, 0);
+    unsigned grid = persistent_grid(ctl, occ, nmax);
+    hash_cta_kernel<T, NT, NUM><<<grid, NT, 0, ctl->stream>>>(bl, bin, a, b, o);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+template <bool NUM>
+int launch_bitmap(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
+                  uint64_t ncols, uint64_t nmax) {
+    const uint32_t W = bitmap_words(ncols);
+    const size_t smem = (size_t)W * 4;
+    CLB_TRY_CUDA(cudaFuncSetAttribute(bitmap_cta_kernel<NUM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 CLB_RUN_KERNEL_FAILURE);
+    int occ = occupancy(bitmap_cta_kernel<NUM>, BMP_NT, smem);
+    unsigned grid = persistent_grid(ctl, occ, nmax);
+    bitmap_cta_kernel<NUM><<<grid, BMP_NT, smem, ctl->stream>>>(bl, bin, a, b, o, ncols, W);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+template <bool NUM>
+int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o, uint64_t ncols,
+               uint64_t nmax) {
+    // Heavy bins first so the long rows start early.
+    CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, BIN_BMP, a, b, o, ncols, nmax));
+    CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax)));
+    CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, nmax)));
+    CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, nmax)));
+    CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, nmax)));
+    CLB_RETURN_IF((launch_esc<8, NUM>(ctl, bl, BIN_W8, a, b, o, nmax)));
+    CLB_RETURN_IF((launch_esc<4, NUM>(ctl, bl, BIN_W4, a, b, o, nmax)));
+    CLB_RETURN_IF((launch_esc<2, NUM>(ctl, bl, BIN_W2, a, b, o, nmax)));
+    CLB_RETURN_IF((launch_esc<1, NUM>(ctl, bl, BIN_W1, a, b, o, nmax)));
+    return CLB_SUCCESS;
+}
+
+}  // namespace
+
+int launch_binning(clb_controls *ctl, const uint32_t *work, const uint32_t *cap, uint64_t n, uint64_t ncols,
+                   uint32_t *info, uint32_t *list, uint32_t *flags) {
+    CLB_TRY_CUDA(cudaMemsetAsync(info, 0, 2 * NUM_BINS * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    unsigned grid = persistent_grid(ctl, 8, ceil_div_u(n, BIN_NT));
+    bin_count_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, info, flags);
+    bin_scatter_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, info, list);
+    ctl->launches += 2;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, const AView &a, const BRows &b,
+                        const RowOut &o, uint64_t ncols, uint64_t nmax) {
+    return numeric ? launch_all<true>(ctl, bl, a, b, o, ncols, nmax) : launch_all<false>(ctl, bl, a, b, o, ncols, nmax);
+}
+
+int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
+                    const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz) {
+    unsigned grid = persistent_grid(ctl, 8, ceil_div_u(n, 256));
+    assemble_kernel<<<grid, 256, 0, ctl->stream>>>(work, pos, off, a_rows, n, c_rpt, c_rows, nzr, nnz);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+}  // namespace clb

@@ -1,0 +1,173 @@
+/*
+ * clbool_b200.h -- C ABI of libclbool_b200.so, the sm_100a (B200) back end
+ * of clBool's boolean sparse hot path.
+ *
+ * Plain pointers and sizes only.  All matrix arrays live in device memory of
+ * the controls' device.  Index arrays (rows, cols) are uint32; offsets (rpt)
+ * are uint64 so that products with more than 2^32 output entries stay
+ * representable (the reference stores them as uint32).
+ *
+ * Every entry point returns a clb_status (0 = success).  Operations are
+ * synchronous on return, like the reference's host functions, and run on the
+ * controls' stream.  Output arrays are allocated through the controls'
+ * allocator (stream-ordered cudaMallocAsync by default) and released with
+ * clb_free() or clb_*_release().  An empty matrix carries NULL arrays, as
+ * the reference's matrix_dcsr(nrows, ncols) carries no buffers
+ * (src/core/matrix_dcsr.hpp:44-48).  Output structs may alias input structs:
+ * inputs are read before the output struct is written.
+ */
+#ifndef CLBOOL_B200_H
+#define CLBOOL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CLB_API __attribute__((visibility("default")))
+#else
+#define CLB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1..14 are clbool::Status (src/core/error.hpp:130-151) in
+ * the reference's order, shifted by one so that 0 means success. */
+typedef enum clb_status {
+    CLB_SUCCESS = 0,
+    CLB_NO_SUCH_PROGRAM = 1,
+    CLB_CREATE_KERNEL_ERROR = 2,
+    CLB_BUILD_PROGRAM_ERROR = 3,
+    CLB_INCOMPLETE_KERNEL = 4,
+    CLB_RUN_KERNEL_FAILURE = 5,
+    CLB_EVENT_WAITING_ERROR = 6,
+    CLB_CREATE_BUFFER_ERROR = 7,
+    CLB_COPY_BUFFER_ERROR = 8,
+    CLB_READ_BUFFER_ERROR = 9,
+    CLB_WRITE_BUFFER_ERROR = 10,
+    CLB_CREATE_CONTROLS_ERROR = 11,
+    CLB_INVALID_ARGUMENT = 12,
+    CLB_INVALID_VALUE = 13,
+    CLB_INITIALIZATION_ERROR = 14,
+    /* Not in the reference: a kernel reported failure through the device
+     * status word (bounded wait gave up, accumulator overflow that has no
+     * fallback, bounds check). */
+    CLB_DEVICE_STATUS_ERROR = 64,
+    /* Not in the reference: a size limit of this implementation. */
+    CLB_NOT_SUPPORTED = 65
+} clb_status;
+
+/* DCSR (src/core/matrix_dcsr.hpp:11-84): only non-empty rows are stored. */
+typedef struct clb_dcsr {
+    uint64_t nrows, ncols, nnz, nzr;
+    uint64_t *rpt;  /* nzr + 1 */
+    uint32_t *rows; /* nzr, strictly increasing */
+    uint32_t *cols; /* nnz, strictly increasing inside a row */
+} clb_dcsr;
+
+/* COO (src/core/matrix_coo.hpp:12-83): lexicographically sorted pairs. */
+typedef struct clb_coo {
+    uint64_t nrows, ncols, nnz;
+    uint32_t *rows; /* nnz */
+    uint32_t *cols; /* nnz */
+} clb_coo;
+
+/* CSR (src/core/matrix_csr.hpp:7-42). */
+typedef struct clb_csr {
+    uint64_t nrows, ncols, nnz;
+    uint64_t *rpt;  /* nrows + 1 */
+    uint32_t *cols; /* nnz */
+} clb_csr;
+
+/* Per-call SpGEMM statistics (optional out-parameter). */
+typedef struct clb_spgemm_stats {
+    uint64_t products;        /* sum over A rows of the B-row lengths hit  */
+    uint64_t nnz, nzr;        /* of C                                       */
+    uint64_t rows_per_bin[16];/* A rows routed to each accumulator bin      */
+    uint64_t fallback_rows;   /* learned form: rows re-run by two passes    */
+    uint64_t capacity;        /* learned form: slots allocated for C        */
+    uint32_t kernel_launches; /* kernels this call launched                 */
+    uint32_t reserved;
+} clb_spgemm_stats;
+
+typedef struct clb_controls clb_controls;
+
+/* Caller-supplied device allocator: alloc returns NULL on failure. */
+typedef void *(*clb_alloc_fn)(void *ctx, size_t bytes, void *stream);
+typedef void (*clb_free_fn)(void *ctx, void *ptr, void *stream);
+
+/* ------------------------------------------------------------- runtime -- */
+/* Name of a status code; never NULL. */
+CLB_API const char *clb_status_string(int status);
+/* Message of the last failing call on this host thread ("" if none). */
+CLB_API const char *clb_last_error(void);
+/* Library version: major*10000 + minor*100 + patch. */
+CLB_API int clb_version(void);
+
+/* Replaces create_controls(platform_id, device_id)
+ * (src/common/env.cpp:7-36): one controls object per CUDA device. */
+CLB_API int clb_controls_create(int device, clb_controls **out);
+CLB_API int clb_controls_destroy(clb_controls *ctl);
+/* Run subsequent operations on `stream` (a cudaStream_t; NULL = own stream). */
+CLB_API int clb_controls_set_stream(clb_controls *ctl, void *stream);
+CLB_API void *clb_controls_get_stream(clb_controls *ctl);
+CLB_API int clb_controls_set_allocator(clb_controls *ctl, clb_alloc_fn alloc, clb_free_fn release, void *ctx);
+CLB_API int clb_controls_sync(clb_controls *ctl);
+CLB_API int clb_controls_device(clb_controls *ctl);
+
+/* Replaces show_devices() (src/common/env.cpp:38-54). */
+CLB_API int clb_device_count(int *count);
+CLB_API int clb_device_info(int device, char *name, size_t name_len, int *sm_count, uint64_t *total_mem);
+
+/* Device memory through the controls' allocator. */
+CLB_API int clb_malloc(clb_controls *ctl, size_t bytes, void **out);
+CLB_API int clb_free(clb_controls *ctl, void *ptr);
+/* Stream-ordered copies; synchronous on return. */
+CLB_API int clb_memcpy_h2d(clb_controls *ctl, void *dst, const void *src, size_t bytes);
+CLB_API int clb_memcpy_d2h(clb_controls *ctl, void *dst, const void *src, size_t bytes);
+CLB_API int clb_memcpy_d2d(clb_controls *ctl, void *dst, const void *src, size_t bytes);
+/* Pinned host memory for staging. */
+CLB_API int clb_host_alloc(size_t bytes, void **out);
+CLB_API int clb_host_free(void *ptr);
+
+CLB_API int clb_dcsr_release(clb_controls *ctl, clb_dcsr *m);
+CLB_API int clb_coo_release(clb_controls *ctl, clb_coo *m);
+CLB_API int clb_csr_release(clb_controls *ctl, clb_csr *m);
+
+/* ----------------------------------------------------------- primitives -- */
+/* prefix_sum (src/common/cl_operations.hpp:9-12, cl_operations.cpp:4-88):
+ * exclusive scan of `n` entries in place; *total = sum of the inputs. */
+CLB_API int clb_prefix_sum_u32(clb_controls *ctl, uint32_t *array, uint64_t n, uint64_t *total);
+CLB_API int clb_prefix_sum_u64(clb_controls *ctl, uint64_t *array, uint64_t n, uint64_t *total);
+
+/* fill_with (src/common/cl_operations.hpp:14, cl_operations.cpp:94-100). */
+CLB_API int clb_fill_u32(clb_controls *ctl, uint32_t *array, uint64_t n, uint32_t value);
+
+/* ---------------------------------------------------------- conversions -- */
+/* coo_to_dcsr_shallow (src/common/matrices_conversions.hpp:11):
+ * out->rpt/rows are new; out->cols aliases in->cols unless deep != 0. */
+CLB_API int clb_coo_to_dcsr(clb_controls *ctl, const clb_coo *in, clb_dcsr *out, int deep);
+/* dcsr_to_coo_shallow / dcsr_to_coo_deep (matrices_conversions.hpp:9-10). */
+CLB_API int clb_dcsr_to_coo(clb_controls *ctl, const clb_dcsr *in, clb_coo *out, int deep);
+/* dcsr_to_csr (matrices_conversions.hpp:26): out->cols aliases in->cols. */
+CLB_API int clb_dcsr_to_csr(clb_controls *ctl, const clb_dcsr *in, clb_csr *out);
+/* csr_to_dcsr (matrices_conversions.hpp:24): out->cols aliases in->cols. */
+CLB_API int clb_csr_to_dcsr(clb_controls *ctl, const clb_csr *in, clb_dcsr *out);
+
+/* ------------------------------------------------------------ operations -- */
+/* dcsr::matrix_multiplication_hash (src/dcsr/dcsr.hpp:33-36,
+ * dcsr_matrix_multiplication_hash.cpp:51-119): C = A*B over (or, and), the
+ * exact two-pass form (symbolic count, scan, numeric fill). */
+CLB_API int clb_dcsr_spgemm_hash(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
+                         clb_spgemm_stats *stats);
+
+/* Products per A row (count_workload, dcsr_matrix_multiplication.cpp:388-404):
+ * workload has a->nzr entries in device memory; *total = their sum. */
+CLB_API int clb_dcsr_workload(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, uint32_t *workload,
+                      uint64_t *total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CLBOOL_B200_H */
