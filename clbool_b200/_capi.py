@@ -29,6 +29,10 @@ class clb_csr(C.Structure):
     _fields_ = [("nrows", C.c_uint64), ("ncols", C.c_uint64), ("nnz", C.c_uint64), ("rpt", vp), ("cols", vp)]
 
 
+class clb_profile_entry(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("launches", C.c_uint32), ("reserved", C.c_uint32), ("ms", C.c_double)]
+
+
 class clb_spgemm_stats(C.Structure):
     _fields_ = [("products", C.c_uint64), ("nnz", C.c_uint64), ("nzr", C.c_uint64),
                 ("rows_per_bin", C.c_uint64 * 16), ("fallback_rows", C.c_uint64), ("capacity", C.c_uint64),
@@ -56,6 +60,10 @@ _SIGS = {
     "clb_controls_device": (C.c_int, [vp]),
     "clb_device_count": (C.c_int, [P(C.c_int)]),
     "clb_device_info": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, P(C.c_int), P(C.c_uint64)]),
+    "clb_profile_enable": (C.c_int, [vp, C.c_int]),
+    "clb_profile_read": (C.c_int, [vp, P(clb_profile_entry), C.c_int, P(C.c_int)]),
+    "clb_coo_sort": (C.c_int, [vp, vp, vp, C.c_uint64]),
+    "clb_coo_reduce_duplicates": (C.c_int, [vp, P(clb_coo), P(clb_coo)]),
     "clb_malloc": (C.c_int, [vp, C.c_size_t, P(vp)]),
     "clb_free": (C.c_int, [vp, vp]),
     "clb_memcpy_h2d": (C.c_int, [vp, vp, vp, C.c_size_t]),
@@ -79,8 +87,6 @@ _SIGS = {
 
 # Entry points added as the library grows; bound when present.
 _OPTIONAL = {
-    "clb_coo_reduce_duplicates": (C.c_int, [vp, P(clb_coo), P(clb_coo)]),
-    "clb_coo_sort": (C.c_int, [vp, vp, vp, C.c_uint64]),
     "clb_dcsr_spgemm_esc": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_stats)]),
     "clb_coo_add": (C.c_int, [vp, P(clb_coo), P(clb_coo), P(clb_coo)]),
     "clb_csr_add": (C.c_int, [vp, P(clb_csr), P(clb_csr), P(clb_csr)]),

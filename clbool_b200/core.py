@@ -66,6 +66,18 @@ class Controls:
     def set_stream(self, stream_ptr: int) -> None:
         check(lib.clb_controls_set_stream(self._h, C.c_void_p(stream_ptr or None)), "set_stream")
 
+    def profile(self, on: bool = True) -> None:
+        """Enable (or disable) per-kernel CUDA-event timing; clears records."""
+        check(lib.clb_profile_enable(self._h, 1 if on else 0), "profile_enable")
+
+    def profile_read(self) -> dict:
+        """{kernel name: (launches, total ms)} since the last read; clears."""
+        from ._capi import clb_profile_entry
+        buf = (clb_profile_entry * 64)()
+        n = C.c_int()
+        check(lib.clb_profile_read(self._h, buf, 64, C.byref(n)), "profile_read")
+        return {buf[i].name.decode(): (int(buf[i].launches), float(buf[i].ms)) for i in range(n.value)}
+
     @property
     def stream(self) -> int:
         return lib.clb_controls_get_stream(self._h) or 0

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 #include "clbool_b200.h"
 
@@ -54,6 +55,14 @@ struct clb_controls {
     clb_free_fn release = nullptr;
     void *alloc_ctx = nullptr;
     uint32_t launches = 0;          // kernels launched by the current call
+    // Opt-in kernel timing: one event pair per launch on `stream`.
+    struct ProfRec {
+        const char *name;
+        cudaEvent_t start, stop;
+    };
+    bool profiling = false;
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> event_pool;
 };
 
 namespace clb {
@@ -103,6 +112,16 @@ struct Temp {
         if (ptr && ctl) dev_free(ctl, ptr);
         ptr = nullptr;
     }
+};
+
+// Records a CUDA event pair around the launches issued in its scope when the
+// controls have profiling enabled (clb_profile_enable).
+struct ProfScope {
+    clb_controls *ctl;
+    const char *name;
+    cudaEvent_t start = nullptr;
+    ProfScope(clb_controls *c, const char *n);
+    ~ProfScope();
 };
 
 // Reads `count` 64-bit scalars from device memory (one sync).

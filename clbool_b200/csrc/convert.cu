@@ -15,12 +15,15 @@ namespace {
 
 constexpr int NT = 256;
 
-// out[r] = offset of the first stored row >= r; out[nrows] = nnz.
+// out[r] = offset of the first stored row >= r, for r in [0, nrows].  Stored
+// rows with an index >= nrows (out of the matrix) fall outside every dense
+// row, so they are never looked up -- as the reference's exact row search
+// (count_workload.cl:8-27) never matches them.
 __global__ void dense_rpt_kernel(const uint64_t *__restrict__ rpt, const uint32_t *__restrict__ rows, uint64_t nzr,
                                  uint64_t nrows, uint64_t *__restrict__ out) {
     for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= nrows;
          r += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t p = r < nrows ? lower_bound_dev<uint32_t, uint64_t>(rows, nzr, (uint32_t)r) : nzr;
+        uint64_t p = r <= 0xFFFFFFFFull ? lower_bound_dev<uint32_t, uint64_t>(rows, nzr, (uint32_t)r) : nzr;
         out[r] = rpt[p];
     }
 }
@@ -91,6 +94,7 @@ unsigned grid_for(const clb_controls *ctl, uint64_t n) {
 }  // namespace
 
 int dcsr_dense_rpt(clb_controls *ctl, const clb_dcsr *m, uint64_t *out) {
+    ProfScope ps(ctl, "dense_row_map");
     dense_rpt_kernel<<<grid_for(ctl, m->nrows + 1), NT, 0, ctl->stream>>>(m->rpt, m->rows, m->nzr, m->nrows, out);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
@@ -197,7 +201,11 @@ int clb_dcsr_to_csr(clb_controls *ctl, const clb_dcsr *in_, clb_csr *out) {
     Temp<uint64_t> rpt;
     CLB_RETURN_IF(rpt.alloc(ctl, in.nrows + 1));
     CLB_RETURN_IF(dcsr_dense_rpt(ctl, &in, rpt.ptr));
-    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    // The reference checks that the CSR keeps every entry
+    // (matrices_conversions.cpp:268): rows stored past nrows do not fit.
+    uint64_t last = 0;
+    CLB_RETURN_IF(read_scalars(ctl, rpt.ptr + in.nrows, &last, 1));
+    if (last != in.nnz) return fail(CLB_INVALID_VALUE, "nnz in dcsr and csr matrices should be equal!");
     r.nnz = in.nnz;
     r.rpt = rpt.release_ownership();
     r.cols = in.cols;

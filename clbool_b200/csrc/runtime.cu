@@ -70,6 +70,34 @@ int check_status(clb_controls *ctl, const char *op) {
     return CLB_SUCCESS;
 }
 
+static cudaEvent_t take_event(clb_controls *ctl) {
+    if (!ctl->event_pool.empty()) {
+        cudaEvent_t e = ctl->event_pool.back();
+        ctl->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+
+ProfScope::ProfScope(clb_controls *c, const char *n) : ctl(c), name(n) {
+    if (!ctl->profiling) return;
+    start = take_event(ctl);
+    if (start) cudaEventRecord(start, ctl->stream);
+}
+
+ProfScope::~ProfScope() {
+    if (!start) return;
+    cudaEvent_t stop = take_event(ctl);
+    if (!stop) return;
+    cudaEventRecord(stop, ctl->stream);
+    ctl->prof.push_back({name, start, stop});
+}
+
 }  // namespace clb
 
 using namespace clb;
@@ -177,6 +205,11 @@ int clb_controls_destroy(clb_controls *ctl) {
     if (!ctl) return CLB_SUCCESS;
     DeviceGuard g(ctl);
     if (ctl->stream) cudaStreamSynchronize(ctl->stream);
+    for (auto &r : ctl->prof) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    for (auto e : ctl->event_pool) cudaEventDestroy(e);
     if (ctl->own_stream && ctl->stream) cudaStreamDestroy(ctl->stream);
     if (ctl->h_scalars) cudaFreeHost(ctl->h_scalars);
     if (ctl->d_status) cudaFree(ctl->d_status);
@@ -219,6 +252,45 @@ int clb_controls_sync(clb_controls *ctl) {
     if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
     DeviceGuard g(ctl);
     CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    return CLB_SUCCESS;
+}
+
+int clb_profile_enable(clb_controls *ctl, int on) {
+    if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    for (auto &r : ctl->prof) {
+        ctl->event_pool.push_back(r.start);
+        ctl->event_pool.push_back(r.stop);
+    }
+    ctl->prof.clear();
+    ctl->profiling = on != 0;
+    return CLB_SUCCESS;
+}
+
+int clb_profile_read(clb_controls *ctl, clb_profile_entry *out, int capacity, int *count) {
+    if (!ctl || !count) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    int n = 0;
+    for (auto &r : ctl->prof) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.start, r.stop);
+        int k = 0;
+        while (k < n && strncmp(out[k].name, r.name, sizeof(out[k].name)) != 0) ++k;
+        if (k == n) {
+            if (n >= capacity || !out) continue;
+            memset(&out[n], 0, sizeof(out[n]));
+            strncpy(out[n].name, r.name, sizeof(out[n].name) - 1);
+            ++n;
+        }
+        out[k].launches += 1;
+        out[k].ms += ms;
+        ctl->event_pool.push_back(r.start);
+        ctl->event_pool.push_back(r.stop);
+    }
+    ctl->prof.clear();
+    *count = n;
     return CLB_SUCCESS;
 }
 

@@ -98,6 +98,7 @@ int scan_impl(clb_controls *ctl, const TIn *in, TOut *out, uint64_t n, uint64_t 
     if (ntiles > 0x7FFFFFFFull) return fail(CLB_NOT_SUPPORTED, "scan too long");
     Temp<uint64_t> sums;
     CLB_RETURN_IF(sums.alloc(ctl, ntiles));
+    ProfScope ps(ctl, "scan");
     tile_reduce_kernel<TIn><<<(unsigned)ntiles, SCAN_NT, 0, ctl->stream>>>(in, n, sums.ptr);
     tiles_scan_kernel<<<1, TS_NT, 0, ctl->stream>>>(sums.ptr, ntiles, d_total);
     downsweep_kernel<TIn, TOut><<<(unsigned)ntiles, SCAN_NT, 0, ctl->stream>>>(in, out, n, sums.ptr);

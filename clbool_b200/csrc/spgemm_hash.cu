@@ -55,6 +55,7 @@ __global__ void __launch_bounds__(WL_NT) workload_kernel(AView a, BRows b, uint3
 
 int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t *work, uint64_t *d_total) {
     unsigned grid = persistent_grid(ctl, 8, ceil_div_u(a.nzr, WL_NT / WL_GROUP));
+    ProfScope ps(ctl, "workload");
     workload_kernel<<<grid, WL_NT, 0, ctl->stream>>>(a, b, work, (unsigned long long *)d_total);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();

@@ -88,9 +88,10 @@ int occupancy(K kernel, int nt, size_t dyn_smem) {
 
 template <int E, bool NUM>
 int launch_esc(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
-               uint64_t nmax) {
+               uint64_t nmax, const char *name) {
     static int occ = occupancy(warp_esc_kernel<E, NUM>, ESC_WARPS * 32, 0);
     unsigned grid = persistent_grid(ctl, occ, ceil_div_u(nmax, ESC_WARPS));
+    ProfScope ps(ctl, name);
     warp_esc_kernel<E, NUM><<<grid, ESC_WARPS * 32, 0, ctl->stream>>>(bl, bin, a, b, o);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
@@ -99,9 +100,10 @@ int launch_esc(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, c
 
 template <int T, int NT, bool NUM>
 int launch_hash(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
-                uint64_t nmax) {
+                uint64_t nmax, const char *name) {
     static int occ = occupancy(hash_cta_kernel<T, NT, NUM>, NT, 0);
     unsigned grid = persistent_grid(ctl, occ, nmax);
+    ProfScope ps(ctl, name);
     hash_cta_kernel<T, NT, NUM><<<grid, NT, 0, ctl->stream>>>(bl, bin, a, b, o);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
@@ -110,13 +112,14 @@ int launch_hash(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, 
 
 template <bool NUM>
 int launch_bitmap(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
-                  uint64_t ncols, uint64_t nmax) {
+                  uint64_t ncols, uint64_t nmax, const char *name) {
     const uint32_t W = bitmap_words(ncols);
     const size_t smem = (size_t)W * 4;
     CLB_TRY_CUDA(cudaFuncSetAttribute(bitmap_cta_kernel<NUM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  CLB_RUN_KERNEL_FAILURE);
     int occ = occupancy(bitmap_cta_kernel<NUM>, BMP_NT, smem);
     unsigned grid = persistent_grid(ctl, occ, nmax);
+    ProfScope ps(ctl, name);
     bitmap_cta_kernel<NUM><<<grid, BMP_NT, smem, ctl->stream>>>(bl, bin, a, b, o, ncols, W);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
@@ -127,15 +130,15 @@ template <bool NUM>
 int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o, uint64_t ncols,
                uint64_t nmax) {
     // Heavy bins first so the long rows start early.
-    CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, BIN_BMP, a, b, o, ncols, nmax));
-    CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax)));
-    CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, nmax)));
-    CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, nmax)));
-    CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, nmax)));
-    CLB_RETURN_IF((launch_esc<8, NUM>(ctl, bl, BIN_W8, a, b, o, nmax)));
-    CLB_RETURN_IF((launch_esc<4, NUM>(ctl, bl, BIN_W4, a, b, o, nmax)));
-    CLB_RETURN_IF((launch_esc<2, NUM>(ctl, bl, BIN_W2, a, b, o, nmax)));
-    CLB_RETURN_IF((launch_esc<1, NUM>(ctl, bl, BIN_W1, a, b, o, nmax)));
+    CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, BIN_BMP, a, b, o, ncols, nmax, NUM ? "bitmap_numeric" : "bitmap_symbolic"));
+    CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax, NUM ? "hash8k_numeric" : "hash8k_symbolic")));
+    CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, nmax, NUM ? "hash4k_numeric" : "hash4k_symbolic")));
+    CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, nmax, NUM ? "hash2k_numeric" : "hash2k_symbolic")));
+    CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, nmax, NUM ? "hash1k_numeric" : "hash1k_symbolic")));
+    CLB_RETURN_IF((launch_esc<8, NUM>(ctl, bl, BIN_W8, a, b, o, nmax, NUM ? "esc256_numeric" : "esc256_symbolic")));
+    CLB_RETURN_IF((launch_esc<4, NUM>(ctl, bl, BIN_W4, a, b, o, nmax, NUM ? "esc128_numeric" : "esc128_symbolic")));
+    CLB_RETURN_IF((launch_esc<2, NUM>(ctl, bl, BIN_W2, a, b, o, nmax, NUM ? "esc64_numeric" : "esc64_symbolic")));
+    CLB_RETURN_IF((launch_esc<1, NUM>(ctl, bl, BIN_W1, a, b, o, nmax, NUM ? "esc32_numeric" : "esc32_symbolic")));
     return CLB_SUCCESS;
 }
 
@@ -145,6 +148,7 @@ int launch_binning(clb_controls *ctl, const uint32_t *work, const uint32_t *cap,
                    uint32_t *info, uint32_t *list, uint32_t *flags) {
     CLB_TRY_CUDA(cudaMemsetAsync(info, 0, 2 * NUM_BINS * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     unsigned grid = persistent_grid(ctl, 8, ceil_div_u(n, BIN_NT));
+    ProfScope ps(ctl, "binning");
     bin_count_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, info, flags);
     bin_scatter_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, info, list);
     ctl->launches += 2;
@@ -160,6 +164,7 @@ int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, con
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
                     const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz) {
     unsigned grid = persistent_grid(ctl, 8, ceil_div_u(n, 256));
+    ProfScope ps(ctl, "assemble");
     assemble_kernel<<<grid, 256, 0, ctl->stream>>>(work, pos, off, a_rows, n, c_rpt, c_rows, nzr, nnz);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();

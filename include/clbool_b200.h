@@ -120,6 +120,20 @@ CLB_API int clb_controls_device(clb_controls *ctl);
 CLB_API int clb_device_count(int *count);
 CLB_API int clb_device_info(int device, char *name, size_t name_len, int *sm_count, uint64_t *total_mem);
 
+/* Opt-in kernel timing: with profiling on, every kernel launch (or group of
+ * launches of one name) is bracketed by CUDA events on the controls' stream.
+ * clb_profile_read synchronises, aggregates the records by name and clears
+ * them.  Not in the reference (its timing is wall-clock logging,
+ * src/common/cl_includes.hpp:61-71). */
+typedef struct clb_profile_entry {
+    char name[48];
+    uint32_t launches;
+    uint32_t reserved;
+    double ms;
+} clb_profile_entry;
+CLB_API int clb_profile_enable(clb_controls *ctl, int on);
+CLB_API int clb_profile_read(clb_controls *ctl, clb_profile_entry *out, int capacity, int *count);
+
 /* Device memory through the controls' allocator. */
 CLB_API int clb_malloc(clb_controls *ctl, size_t bytes, void **out);
 CLB_API int clb_free(clb_controls *ctl, void *ptr);
@@ -143,6 +157,15 @@ CLB_API int clb_prefix_sum_u64(clb_controls *ctl, uint64_t *array, uint64_t n, u
 
 /* fill_with (src/common/cl_operations.hpp:14, cl_operations.cpp:94-100). */
 CLB_API int clb_fill_u32(clb_controls *ctl, uint32_t *array, uint64_t n, uint32_t value);
+
+/* coo::sort_arrays (src/coo/coo_initialization.hpp:9): sort (row, col)
+ * pairs lexicographically, in place. */
+CLB_API int clb_coo_sort(clb_controls *ctl, uint32_t *rows, uint32_t *cols, uint64_t n);
+
+/* matrix_coo(..., sorted, noDuplicates=false) dedupe
+ * (src/core/matrix_coo.cpp:117-170): `in` must be sorted; `out` gets new
+ * arrays without adjacent duplicates. */
+CLB_API int clb_coo_reduce_duplicates(clb_controls *ctl, const clb_coo *in, clb_coo *out);
 
 /* ---------------------------------------------------------- conversions -- */
 /* coo_to_dcsr_shallow (src/common/matrices_conversions.hpp:11):

@@ -352,7 +352,8 @@ int orc_spgemm(const orc_dcsr *a, const orc_dcsr *b, orc_dcsr *c) {
     if (b->nrows <= (1ull << 27)) {
         bmap = (int64_t *)malloc((b->nrows + 1) * sizeof(int64_t));
         for (uint64_t k = 0; k < b->nrows; ++k) bmap[k] = -1;
-        for (uint64_t p = 0; p < b->nzr; ++p) bmap[b->rows[p]] = (int64_t)p;
+        for (uint64_t p = 0; p < b->nzr; ++p)
+            if (b->rows[p] < b->nrows) bmap[b->rows[p]] = (int64_t)p;  /* rows past nrows never match */
     }
     uint64_t nwords = (b->ncols + 63) / 64;
     uint64_t *rownnz = (uint64_t *)malloc(a->nzr * sizeof(uint64_t));
@@ -423,7 +424,8 @@ int orc_spgemm_row_nnz(const orc_dcsr *a, const orc_dcsr *b, uint64_t *rownnz) {
     if (b->nrows <= (1ull << 27)) {
         bmap = (int64_t *)malloc((b->nrows + 1) * sizeof(int64_t));
         for (uint64_t k = 0; k < b->nrows; ++k) bmap[k] = -1;
-        for (uint64_t p = 0; p < b->nzr; ++p) bmap[b->rows[p]] = (int64_t)p;
+        for (uint64_t p = 0; p < b->nzr; ++p)
+            if (b->rows[p] < b->nrows) bmap[b->rows[p]] = (int64_t)p;  /* rows past nrows never match */
     }
     uint64_t nwords = (b->ncols + 63) / 64;
     #pragma omp parallel
