@@ -1,0 +1,472 @@
+"""Benchmark: boolean SpGEMM intermediate products/s on R-MAT scale-20 A*A.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--scale 20] [--form two_pass|learned]
+
+One step = one dcsr::matrix_multiplication_hash of the synthetic R-MAT
+scale-20 graph by itself (2^20 vertices, edge factor 16, a/b/c/d =
+.57/.19/.19/.05, duplicates removed, self-loops kept), producing C on the GPU.
+`value` is products/s with A resident in HBM; `e2e` is the same metric
+through the public API with host buffers (pinned H2D of A, D2H of all of C
+inside the timed region).  With N > 1 ranks (torchrun) every rank computes
+the C rows of its share of A's rows (balanced by products) against its own
+copy of A; no collective touches the data path.
+
+`--impl reference` times the reference's own CPU implementation
+(coo_utils::matrix_multiplication_cpu, compiled from the reference sources
+into oracle/_ref) on a bounded sample of A's rows with all host threads, and
+reports the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bool SpGEMM products/s: learned-sized vs two-pass, same GPU, bit-exact"
+UNIT = "products/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+# ------------------------------------------------------------------ helpers --
+def peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def rmat_a(scale: int):
+    from clbool_b200 import gen
+    r, c = gen.rmat(scale, seed=1)
+    rpt, rows, cols = gen.to_dcsr(r, c)
+    return 1 << scale, rpt, rows, cols
+
+
+def shard_rows(rpt_work: np.ndarray, world: int, rank: int) -> tuple[int, int]:
+    """Contiguous block of A's stored rows with about 1/world of the products."""
+    if world == 1:
+        return 0, rpt_work.size
+    cum = np.cumsum(rpt_work, dtype=np.float64)
+    tot = cum[-1] if cum.size else 0.0
+    lo = 0 if rank == 0 else int(np.searchsorted(cum, tot * rank / world, side="left")) + 1
+    hi = rpt_work.size if rank == world - 1 else int(np.searchsorted(cum, tot * (rank + 1) / world, side="left")) + 1
+    return min(lo, rpt_work.size), min(hi, rpt_work.size)
+
+
+def bin_of(p: np.ndarray, bound: np.ndarray) -> np.ndarray:
+    """The accumulator bin of every row (mirrors bin_of in spgemm_kernels.cuh)."""
+    b = np.full(p.shape, 11, np.int32)
+    b[p > (1 << 17)] = 10
+    b[p > (1 << 20)] = 9
+    for lim, k in ((4096, 8), (2048, 7), (1024, 6), (512, 5)):
+        b[bound <= lim] = k
+    for lim, k in ((256, 4), (128, 3), (64, 2), (32, 1)):
+        b[p <= lim] = k
+    b[p == 0] = 0
+    return b
+
+
+KERNEL_BIN = {"bitmap": (9, 10, 11), "hash8k": 8, "hash4k": 7, "hash2k": 6, "hash1k": 5, "esc256": 4, "esc128": 3,
+              "esc64": 2, "esc32": 1}
+
+
+def algorithmic_bytes(kernel: str, a_len: np.ndarray, work: np.ndarray, c_len: np.ndarray, ncols: int) -> int:
+    """Bytes the accumulator launch `kernel` must move for its rows, by the
+    per-row model: A row pointer pair + row id (12 B), per A entry its column
+    and B's row pointer pair (12 B), every product's B column (4 B), and for
+    the numeric pass C's columns (4 B each) plus C's row pointer and id (12 B);
+    the symbolic pass writes one 4-byte count per row instead."""
+    base = kernel.split("_")[0]
+    if base not in KERNEL_BIN:
+        return 0
+    bins = bin_of(work, np.minimum(work, ncols))
+    m = np.isin(bins, np.atleast_1d(KERNEL_BIN[base]))
+    rows = int(m.sum())
+    reads = 12 * rows + 12 * int(a_len[m].sum()) + 4 * int(work[m].sum())
+    if kernel.endswith("numeric"):
+        return reads + 4 * int(c_len[m].sum()) + 12 * rows
+    return reads + 4 * rows
+
+
+# --------------------------------------------------------------- our arm --
+def run_ours(args, rank: int, world: int, dist) -> dict | None:
+    import clbool_b200 as cb
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    ctl = cb.create_controls(0, dev)
+    n, rpt, rows, cols = rmat_a(args.scale)
+    nnz_a = cols.size
+    A_full = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(rpt, rows, cols), n)
+    work_buf, total_products = cb.dcsr.workload(ctl, A_full, A_full)
+    work = work_buf.to_host(rows.size).astype(np.int64)
+    lo, hi = shard_rows(work, world, rank)
+    srpt = (rpt[lo:hi + 1] - rpt[lo]).astype(np.uint64)
+    srows, scols = rows[lo:hi], cols[int(rpt[lo]):int(rpt[hi])]
+    A = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(srpt, srows, scols), n) if hi > lo else \
+        cb.matrix_dcsr.zeros(n, n)
+    my_products = int(work[lo:hi].sum())
+    a_len = np.diff(srpt.astype(np.int64))
+    mywork = work[lo:hi]
+
+    flush = cb.DeviceBuffer.empty(ctl, 256 << 20, np.uint8)
+
+    def l2_flush():
+        cb.lib.clb_fill_u32(ctl.handle, __import__("ctypes").c_void_p(flush.ptr), (256 << 20) // 4, 0)
+
+    def step(stats=None):
+        return cb.dcsr.matrix_multiplication_hash(ctl, None, A, A_full, stats=stats)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        c = step()
+        del c
+    ctl.sync()
+
+    # timed region: per-step CUDA events via the library's profile records,
+    # L2 flushed between steps outside the events.
+    import ctypes
+    ev_ms = []
+    prof_tot: dict = {}
+    launches = 0
+    st = {}
+    c_len = None
+    with ClockSampler(dev) as clk:
+        barrier()
+        ctl.sync()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            l2_flush()
+            ctl.profile(True)
+            st = {}
+            c = step(st)
+            prof = ctl.profile_read()
+            ctl.profile(False)
+            launches += st["kernel_launches"]
+            step_ms = sum(v[1] for v in prof.values())
+            ev_ms.append(step_ms)
+            for name, (cnt, ms) in prof.items():
+                a, b = prof_tot.get(name, (0, 0.0))
+                prof_tot[name] = (a + cnt, b + ms)
+            if k == args.steps - 1 and c.nnz():
+                crpt = c.rpt_gpu().to_host(c.nzr() + 1).astype(np.int64)
+                crow = c.rows_gpu().to_host(c.nzr())
+                c_len = np.zeros(srows.size, np.int64)
+                c_len[np.searchsorted(srows, crow)] = np.diff(crpt)
+            del c
+        ctl.sync()
+        barrier()
+        wall = time.perf_counter() - t0
+    clocks = clk.summary()
+    # device time: the events bracket the library's kernels; the profile's
+    # per-kernel spans tile each call, so their sum is the call's device time.
+    my_ms = sum(ev_ms)
+    if dist is not None:
+        import torch
+        t = torch.tensor([my_ms, float(my_products), float(st.get("nnz", 0))], dtype=torch.float64, device=f"cuda:{dev}")
+        mx = t.clone()
+        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        total_ms, products_all, nnz_all = float(mx[0]), float(t[1]), float(t[2])
+    else:
+        total_ms, products_all, nnz_all = my_ms, float(my_products), float(st.get("nnz", 0))
+    ms_per_step = total_ms / args.steps
+    value = products_all / (ms_per_step / 1e3)
+
+    # roofline of the dominant kernel (largest device time in the timed steps)
+    peak, peak_kind = peaks()
+    top = max(prof_tot.items(), key=lambda kv: kv[1][1])
+    top_name, (top_launches, top_ms) = top
+    alg = algorithmic_bytes(top_name, a_len, mywork, c_len if c_len is not None else np.zeros_like(mywork), n)
+    per_launch_ms = top_ms / max(top_launches, 1)
+    achieved = alg / (per_launch_ms / 1e3) / 1e9 if alg else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(f"{top_name}@rmat_s{args.scale}")
+        except Exception:
+            traffic = None
+
+    # end to end through the public API with host buffers
+    e2e = run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, my_products, dist, dev)
+
+    if rank != 0:
+        return None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic", "impl": "ours",
+        "config": {"workload": f"rmat_s{args.scale}_AxA_hash_{args.form}", "scale": args.scale, "edge_factor": 16,
+                   "abcd": [0.57, 0.19, 0.19, 0.05], "nnz_A": int(nnz_a), "products": int(products_all),
+                   "nnz_C": int(nnz_all), "form": args.form, "parallelism": f"rows{world}",
+                   "l2": "256 MiB device memset between steps, outside the step events; C (>30 GB) also exceeds L2"},
+        "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "alg_bytes_per_launch": alg, "launch_ms": per_launch_ms},
+        "kernels_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in sorted(prof_tot.items(),
+                                                                                 key=lambda kv: -kv[1][1])},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "wall_s": wall,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(n, rpt, rows, cols, work)
+    return line
+
+
+def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev) -> dict:
+    """products/s through the public API: pinned host A -> device, SpGEMM,
+    all of C -> pinned host, per step."""
+    import ctypes
+    lib = cb.lib
+
+    def pinned(nbytes):
+        p = ctypes.c_void_p()
+        cb.core.check(lib.clb_host_alloc(max(nbytes, 1), ctypes.byref(p)), "host_alloc")
+        return p
+
+    h_rpt, h_rows, h_cols = pinned(srpt.nbytes), pinned(srows.nbytes), pinned(scols.nbytes)
+    ctypes.memmove(h_rpt, srpt.ctypes.data, srpt.nbytes)
+    ctypes.memmove(h_rows, srows.ctypes.data, srows.nbytes)
+    ctypes.memmove(h_cols, scols.ctypes.data, scols.nbytes)
+    # size of C, to stage the read-back in pinned memory
+    c0 = cb.dcsr.matrix_multiplication_hash(ctl, None, cb.matrix_dcsr_from_cpu(
+        ctl, cb.matrix_dcsr_cpu(srpt, srows, scols), n), A_full)
+    c_bytes = (8 * (c0.nzr() + 1) + 4 * c0.nzr() + 4 * c0.nnz()) if c0.nnz() else 0
+    h_c = pinned(c_bytes)
+    del c0
+    steps = max(1, min(args.steps, 3))
+    times = []
+    for _ in range(steps):
+        if dist is not None:
+            dist.barrier()
+        ctl.sync()
+        t0 = time.perf_counter()
+        d_rpt = cb.DeviceBuffer.empty(ctl, srpt.size, np.uint64)
+        d_rows = cb.DeviceBuffer.empty(ctl, max(srows.size, 1), np.uint32)
+        d_cols = cb.DeviceBuffer.empty(ctl, max(scols.size, 1), np.uint32)
+        lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(d_rpt.ptr), h_rpt, srpt.nbytes)
+        lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(d_rows.ptr), h_rows, srows.nbytes)
+        lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(d_cols.ptr), h_cols, scols.nbytes)
+        A = cb.matrix_dcsr(d_rpt, d_rows, d_cols, n, n, scols.size, srows.size)
+        C = cb.dcsr.matrix_multiplication_hash(ctl, None, A, A_full)
+        if C.nnz():
+            off = 0
+            for buf, nb in ((C.rpt_gpu(), 8 * (C.nzr() + 1)), (C.rows_gpu(), 4 * C.nzr()), (C.cols_gpu(), 4 * C.nnz())):
+                lib.clb_memcpy_d2h(ctl.handle, ctypes.c_void_p(h_c.value + off), ctypes.c_void_p(buf.ptr), nb)
+                off += nb
+        del C, A, d_rpt, d_rows, d_cols
+        ctl.sync()
+        dt = time.perf_counter() - t0
+        if dist is not None:
+            import torch
+            t = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t[0])
+        times.append(dt)
+    lib.clb_host_free(h_rpt)
+    lib.clb_host_free(h_rows)
+    lib.clb_host_free(h_cols)
+    lib.clb_host_free(h_c)
+    tot_products = products
+    if dist is not None:
+        import torch
+        t = torch.tensor([float(products)], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t)
+        tot_products = float(t[0])
+    sec = statistics.median(times)
+    return {"value": tot_products / sec, "unit": UNIT, "h2d_bytes_per_step": int(srpt.nbytes + srows.nbytes + scols.nbytes),
+            "d2h_bytes_per_step": int(c_bytes), "s_per_step": sec, "steps": steps}
+
+
+# ------------------------------------------------------------ CPU baselines --
+def _row_sample(rows_n: int, frac: float, seed: int = 7) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(rows_n, size=max(1, int(rows_n * frac)), replace=False))
+
+
+def _sub_dcsr(rpt, rows, cols, pick):
+    lens = (rpt[pick + 1] - rpt[pick]).astype(np.int64)
+    srpt = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    idx = np.concatenate([np.arange(int(rpt[i]), int(rpt[i + 1])) for i in pick]) if pick.size else np.zeros(0, np.int64)
+    return srpt, rows[pick], cols[idx]
+
+
+def cpu_baseline(n, rpt, rows, cols, work) -> dict:
+    """The oracle's multithreaded CPU product on a seeded sample of A's rows."""
+    import oracle as O
+    threads = O.set_threads(os.cpu_count() or 1)
+    pick = _row_sample(rows.size, 0.25)
+    srpt, srows, scols = _sub_dcsr(rpt, rows, cols, pick)
+    A = O.Dcsr(n, n, srpt, srows, scols)
+    B = O.Dcsr(n, n, rpt, rows, cols)
+    t0 = time.perf_counter()
+    C = O.spgemm(A, B)
+    dt = time.perf_counter() - t0
+    p = int(work[pick].sum())
+    del C
+    return {"value": p / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"25% of A's stored rows (seed 7): {pick.size} rows, {p} products, {dt:.2f} s"}
+
+
+def run_reference(args) -> dict:
+    """The reference's own CPU product (matrix_multiplication_cpu) on bounded
+    samples of A's rows, one sample per host thread."""
+    import concurrent.futures as cf
+    import oracle as O
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "reference CPU library (oracle/_ref) was not built"}
+    R = O.Ref()
+    n, rpt, rows, cols = rmat_a(args.scale)
+    B = O.Dcsr(n, n, rpt, rows, cols)
+    work = np.diff(rpt.astype(np.int64))  # placeholder until products are known
+    Bd = O.Dcsr(n, n, rpt, rows, cols)
+    prod = O.workload(Bd, Bd).astype(np.int64)
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(11)
+    # The reference's product looks every A entry's column up by a linear
+    # std::find over B's stored rows (coo_utils.cpp:487), so its cost is
+    # ~ entries * nzr(B); size each thread's sample for a few seconds.
+    per_thread_rows = max(1, int(args.ref_rows))
+    samples = [np.sort(rng.choice(rows.size, size=per_thread_rows, replace=False)) for _ in range(threads)]
+
+    def one(pick):
+        srpt, srows, scols = _sub_dcsr(rpt, rows, cols, pick)
+        R.spgemm(O.Dcsr(n, n, srpt, srows, scols), B)
+        return int(prod[pick].sum())
+
+    def step():
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            p = sum(ex.map(one, samples))
+        return p, time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
+    ps, ts = 0, 0.0
+    for _ in range(args.steps):
+        p, t = step()
+        ps += p
+        ts += t
+    value = ps / ts
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ts / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"rmat_s{args.scale}_AxA_hash_{args.form}", "scale": args.scale},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{threads} threads x {per_thread_rows} random stored rows of A per step "
+                                       f"(coo_utils::matrix_multiplication_cpu)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# --------------------------------------------------------------------- main --
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--form", default="two_pass", choices=["two_pass", "learned"])
+    ap.add_argument("--ref-rows", type=int, default=24)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = dist_mod
+    try:
+        line = run_ours(args, rank, world, dist)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

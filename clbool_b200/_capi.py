@@ -40,7 +40,7 @@ class clb_spgemm_stats(C.Structure):
 
     def as_dict(self) -> dict:
         return {"products": self.products, "nnz": self.nnz, "nzr": self.nzr,
-                "rows_per_bin": list(self.rows_per_bin)[:10], "fallback_rows": self.fallback_rows,
+                "rows_per_bin": list(self.rows_per_bin)[:12], "fallback_rows": self.fallback_rows,
                 "capacity": self.capacity, "kernel_launches": self.kernel_launches}
 
 

@@ -37,8 +37,12 @@ enum Bin : int {
     BIN_H2K = 6,  // <= 1024 -> 2048
     BIN_H4K = 7,  // <= 2048 -> 4096
     BIN_H8K = 8,  // <= 4096 -> 8192
-    BIN_BMP = 9,  // bitmap
-    NUM_BINS = 10
+    // Bitmap rows, heaviest first: the three bins are contiguous in the row
+    // list and one dynamically scheduled launch walks them in order.
+    BIN_BMP_XL = 9,   // products > 2^20
+    BIN_BMP_L = 10,   // products > 2^17
+    BIN_BMP = 11,     // the rest
+    NUM_BINS = 12
 };
 
 // Bin of a row from its product count and its distinct-column bound
@@ -53,6 +57,8 @@ __host__ __device__ __forceinline__ int bin_of(uint64_t products, uint64_t disti
     if (distinct_bound <= 1024) return BIN_H2K;
     if (distinct_bound <= 2048) return BIN_H4K;
     if (distinct_bound <= 4096) return BIN_H8K;
+    if (products > (1u << 20)) return BIN_BMP_XL;
+    if (products > (1u << 17)) return BIN_BMP_L;
     return BIN_BMP;
 }
 
@@ -242,42 +248,111 @@ __device__ __forceinline__ void block_bitonic_sort(uint32_t *s, uint32_t M) {
     }
 }
 
-// Insert every product of A row i into an accumulator: warp per A entry,
-// lanes stride the B row, four independent loads in flight per lane.
-template <class F>
-__device__ __forceinline__ void for_each_product(const AView &a, const BRows &b, uint32_t i, int nwarps, F &&f) {
-    const uint32_t lane = lane_id();
+// Products of A row i, balanced over a whole CTA.  A entries are staged in
+// chunks of ECH: B-row starts and the exclusive prefix of B-row lengths go to
+// shared memory; then every warp takes 32*U consecutive products of the
+// flattened chunk, each lane walking its own entry cursor forward (one
+// binary search per warp chunk).  Consecutive lanes read consecutive columns
+// of one B row (coalesced) and each lane has U loads in flight before f runs.
+// f(col, valid) is called warp-uniformly (all 32 lanes, valid or not).
+template <int NT, int ECH, int U, class F>
+__device__ __forceinline__ void balanced_products(const AView &a, const BRows &b, uint32_t i, uint32_t *s_pre,
+                                                  uint32_t *s_beg, uint32_t *scratch, F &&f) {
+    constexpr int EPT = ECH / NT;
+    constexpr int NW = NT / 32;
+    constexpr uint32_t WCH = 32u * U;
+    const uint32_t lane = lane_id(), w = warp_id();
     const uint64_t ja = a.rpt[i], je = a.rpt[i + 1];
-    for (uint64_t j = ja + warp_id(); j < je; j += nwarps) {
-        uint64_t bb;
-        const uint32_t len = b_row(b, __ldg(a.cols + j), bb);
-        const uint32_t *src = b.cols + bb;
-        uint32_t t = lane;
-        for (; t + 96 < len; t += 128) {
-            uint32_t c0 = __ldg(src + t), c1 = __ldg(src + t + 32), c2 = __ldg(src + t + 64), c3 = __ldg(src + t + 96);
-            f(c0);
-            f(c1);
-            f(c2);
-            f(c3);
+    for (uint64_t c0 = ja; c0 < je; c0 += ECH) {
+        const uint32_t n = (uint32_t)min((uint64_t)ECH, je - c0);
+        for (uint32_t e = threadIdx.x; e < n; e += NT) {
+            uint64_t bb;
+            const uint32_t len = b_row(b, __ldg(a.cols + c0 + e), bb);
+            s_beg[e] = (uint32_t)bb;
+            s_pre[e] = len;
         }
-        for (; t < len; t += 32) f(__ldg(src + t));
+        __syncthreads();
+        uint32_t v[EPT];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const uint32_t e = threadIdx.x * EPT + k;
+            v[k] = e < n ? s_pre[e] : 0u;
+            sum += v[k];
+        }
+        uint32_t total;
+        uint32_t run = block_exclusive_scan<uint32_t, NT>(sum, scratch, &total);
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const uint32_t e = threadIdx.x * EPT + k;
+            if (e < n) s_pre[e] = run;
+            run += v[k];
+        }
+        if (threadIdx.x == 0) s_pre[n] = total;
+        __syncthreads();
+        for (uint32_t base = w * WCH; base < total; base += NW * WCH) {
+            const uint32_t p = base + lane;
+            uint32_t e;
+            {   // largest e in [0, n) with s_pre[e] <= p
+                uint32_t lo = 0, hi = n - 1;
+                const uint32_t key = p < total ? p : total - 1;
+                while (lo < hi) {
+                    const uint32_t m = (lo + hi + 1) >> 1;
+                    if (s_pre[m] <= key) lo = m; else hi = m - 1;
+                }
+                e = lo;
+            }
+            uint32_t col[U];
+            bool val[U];
+#pragma unroll
+            for (int s = 0; s < U; ++s) {
+                const uint32_t q = p + (uint32_t)s * 32u;
+                val[s] = q < total;
+                col[s] = 0;
+                if (val[s]) {
+                    while (s_pre[e + 1] <= q) ++e;
+                    col[s] = __ldg(b.cols + s_beg[e] + (q - s_pre[e]));
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < U; ++s) f(col[s], val[s]);
+        }
+        __syncthreads();
     }
 }
 
+// Next work item of a dynamically scheduled persistent CTA.
+__device__ __forceinline__ uint32_t next_item(uint32_t *counter, uint32_t *s_slot) {
+    if (threadIdx.x == 0) *s_slot = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t it = *s_slot;
+    __syncthreads();
+    return it;
+}
+
+constexpr int HASH_ECH = 1024;
+
 template <int T, int NT, bool NUMERIC>
-__global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o) {
+__global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o,
+                                                      uint32_t *counter) {
     constexpr int SPT = T / NT;  // slots per thread
     __shared__ uint32_t table[T];
+    __shared__ uint32_t s_pre[HASH_ECH + 1];
+    __shared__ uint32_t s_beg[HASH_ECH];
     __shared__ uint32_t scratch[33];
+    __shared__ uint32_t s_slot;
     uint32_t beg, cnt;
     bin_range(bl, bin, beg, cnt);
-    for (uint32_t item = blockIdx.x; item < cnt; item += gridDim.x) {
+    for (;;) {
+        const uint32_t item = next_item(counter, &s_slot);
+        if (item >= cnt) break;
         const uint32_t i = bl.list[beg + item];
         for (int s = threadIdx.x; s < T; s += NT) table[s] = EMPTY;
         __syncthreads();
         uint32_t mine = 0;
-        for_each_product(a, b, i, NT / 32, [&](uint32_t c) { mine += hash_insert<T>(table, c, o.status); });
-        __syncthreads();
+        balanced_products<NT, HASH_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
+            if (valid) mine += hash_insert<T>(table, c, o.status);
+        });
         if (!NUMERIC) {
             uint32_t total = block_sum<uint32_t, NT>(mine, scratch);
             if (threadIdx.x == 0) o.row_nnz[i] = total;
@@ -315,6 +390,7 @@ __global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AVie
 // ----------------------------------------------------------- CTA bitmap ----
 constexpr int BMP_NT = 1024;
 constexpr int BMP_NW = BMP_NT / 32;
+constexpr int BMP_ECH = 2048;
 constexpr uint32_t BMP_MAX_WORDS = 32768;  // 128 KB: 2^20 columns per chunk
 
 // Words of the bitmap for `ncols` columns: a multiple of 32 * BMP_NW so the
@@ -327,31 +403,74 @@ inline uint32_t bitmap_words(uint64_t ncols) {
     return (uint32_t)w;
 }
 
+// Dynamic shared memory of the bitmap kernel: W words + the entry stage.
+inline size_t bitmap_smem_bytes(uint32_t W) { return ((size_t)W + 2 * BMP_ECH + 1) * 4; }
+
+// Position of the n-th (0-based) set bit of w; w has more than n set bits.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t w, uint32_t n) {
+    uint32_t pos = 0, c;
+    c = __popc(w & 0xFFFFu);
+    if (n >= c) { n -= c; w >>= 16; pos += 16; }
+    c = __popc(w & 0xFFu);
+    if (n >= c) { n -= c; w >>= 8; pos += 8; }
+    c = __popc(w & 0xFu);
+    if (n >= c) { n -= c; w >>= 4; pos += 4; }
+    c = __popc(w & 0x3u);
+    if (n >= c) { n -= c; w >>= 2; pos += 2; }
+    c = w & 1u;
+    if (n >= c) pos += 1;
+    return pos;
+}
+
+// Rows of bins [bin_lo, bin_hi] (contiguous in the list, heaviest first),
+// one row per CTA at a time, taken from `counter`.
 template <bool NUMERIC>
-__global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o,
-                                                               uint64_t ncols, uint32_t W) {
-    extern __shared__ uint32_t bm[];
+__global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int bin_lo, int bin_hi, AView a, BRows b,
+                                                               RowOut o, uint64_t ncols, uint32_t W,
+                                                               uint32_t *counter) {
+    extern __shared__ uint32_t smem[];
+    uint32_t *bm = smem;
+    uint32_t *s_pre = smem + W;
+    uint32_t *s_beg = s_pre + BMP_ECH + 1;
     __shared__ uint32_t wtot[BMP_NW];
     __shared__ uint32_t scratch[33];
-    uint32_t beg, cnt;
-    bin_range(bl, bin, beg, cnt);
+    __shared__ uint32_t s_slot;
+    uint32_t beg, cnt = 0, tmp;
+    bin_range(bl, bin_lo, beg, tmp);
+    for (int q = bin_lo; q <= bin_hi; ++q) cnt += bl.info[q];
     for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) bm[w] = 0;
     __syncthreads();
     const uint32_t lane = lane_id(), wi = warp_id();
     const uint32_t WPW = W / BMP_NW;  // words per warp in the emission pass
     const uint64_t chunk_cols = (uint64_t)W * 32;
-    for (uint32_t item = blockIdx.x; item < cnt; item += gridDim.x) {
+    for (;;) {
+        const uint32_t item = next_item(counter, &s_slot);
+        if (item >= cnt) break;
         const uint32_t i = bl.list[beg + item];
         uint64_t total = 0;
-        uint64_t out_base = NUMERIC ? o.row_off[i] : 0;
+        const uint64_t out_base = NUMERIC ? o.row_off[i] : 0;
         bool overflowed = false;
         for (uint64_t c0 = 0; c0 < ncols; c0 += chunk_cols) {
-            for_each_product(a, b, i, BMP_NW, [&](uint32_t c) {
+            balanced_products<BMP_NT, BMP_ECH, 8>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
                 // unsigned wrap sends columns below c0 out of range too
-                uint64_t r = (uint64_t)c - c0;
-                if (r < chunk_cols) atomicOr(bm + (r >> 5), 1u << (r & 31));
+                const uint64_t r = (uint64_t)c - c0;
+                const bool in = valid && r < chunk_cols;
+                const uint32_t wd = in ? (uint32_t)(r >> 5) : 0xFFFFFFFFu;
+                uint32_t bit = in ? (1u << (r & 31)) : 0u;
+                // Lanes of one B row hold ascending columns: merge the bits of
+                // a run of lanes that target the same word, one atomic per run.
+                const uint32_t upw = __shfl_up_sync(0xFFFFFFFFu, wd, 1);
+                const bool head = lane == 0 || upw != wd;
+                if (__any_sync(0xFFFFFFFFu, in && !head)) {
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const uint32_t ob = __shfl_down_sync(0xFFFFFFFFu, bit, d);
+                        const uint32_t ow = __shfl_down_sync(0xFFFFFFFFu, wd, d);
+                        if (lane + d < 32 && ow == wd) bit |= ob;
+                    }
+                }
+                if (in && head) atomicOr(bm + wd, bit);
             });
-            __syncthreads();
             if (!NUMERIC || overflowed) {
                 uint32_t mine = 0;
                 for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) {
@@ -370,7 +489,7 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
             __syncthreads();
             uint64_t woff = 0, ctot = 0;
             for (uint32_t q = 0; q < (uint32_t)BMP_NW; ++q) {
-                uint32_t v = wtot[q];
+                const uint32_t v = wtot[q];
                 woff += q < wi ? v : 0;
                 ctot += v;
             }
@@ -385,18 +504,30 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
             }
             uint64_t run = out_base + total + woff;
             for (uint32_t w = wbeg; w < wbeg + WPW; w += 32) {
-                uint32_t word = bm[w + lane];
+                const uint32_t word = bm[w + lane];
                 bm[w + lane] = 0;
-                uint32_t pc = __popc(word);
-                uint32_t inc = warp_inclusive_scan(pc);
-                uint64_t pos = run + (inc - pc);
-                const uint32_t colbase = (uint32_t)(c0 + (uint64_t)(w + lane) * 32);
-                while (word) {
-                    const int bit = __ffs(word) - 1;
-                    word &= word - 1;
-                    o.cols[pos++] = colbase + (uint32_t)bit;
+                const uint32_t pc = __popc(word);
+                const uint32_t inc = warp_inclusive_scan(pc);
+                const uint32_t T = __shfl_sync(0xFFFFFFFFu, inc, 31);
+                // Output k of this 32-word step goes to lane k % 32 (coalesced
+                // stores): find the source lane L (first with inc[L] > k) and
+                // the (k - exclusive[L])-th set bit of its word.
+                for (uint32_t k0 = 0; k0 < T; k0 += 32) {
+                    const uint32_t k = k0 + lane;
+                    uint32_t L = 0;
+#pragma unroll
+                    for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
+                        const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, L + sft - 1);
+                        if (v <= k) L += sft;
+                    }
+                    const uint32_t wL = __shfl_sync(0xFFFFFFFFu, word, L);
+                    const uint32_t exL = __shfl_sync(0xFFFFFFFFu, inc - pc, L);
+                    if (k < T) {
+                        const uint32_t colbase = (uint32_t)(c0 + (uint64_t)(w + L) * 32);
+                        o.cols[run + k] = colbase + nth_set_bit(wL, k - exL);
+                    }
                 }
-                run += __shfl_sync(0xFFFFFFFFu, inc, 31);
+                run += T;
             }
             total += ctot;
             __syncthreads();

@@ -100,27 +100,27 @@ int launch_esc(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, c
 
 template <int T, int NT, bool NUM>
 int launch_hash(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
-                uint64_t nmax, const char *name) {
+                uint64_t nmax, uint32_t *counter, const char *name) {
     static int occ = occupancy(hash_cta_kernel<T, NT, NUM>, NT, 0);
     unsigned grid = persistent_grid(ctl, occ, nmax);
     ProfScope ps(ctl, name);
-    hash_cta_kernel<T, NT, NUM><<<grid, NT, 0, ctl->stream>>>(bl, bin, a, b, o);
+    hash_cta_kernel<T, NT, NUM><<<grid, NT, 0, ctl->stream>>>(bl, bin, a, b, o, counter);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
 }
 
 template <bool NUM>
-int launch_bitmap(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
-                  uint64_t ncols, uint64_t nmax, const char *name) {
+int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
+                  uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name) {
     const uint32_t W = bitmap_words(ncols);
-    const size_t smem = (size_t)W * 4;
+    const size_t smem = bitmap_smem_bytes(W);
     CLB_TRY_CUDA(cudaFuncSetAttribute(bitmap_cta_kernel<NUM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  CLB_RUN_KERNEL_FAILURE);
     int occ = occupancy(bitmap_cta_kernel<NUM>, BMP_NT, smem);
     unsigned grid = persistent_grid(ctl, occ, nmax);
     ProfScope ps(ctl, name);
-    bitmap_cta_kernel<NUM><<<grid, BMP_NT, smem, ctl->stream>>>(bl, bin, a, b, o, ncols, W);
+    bitmap_cta_kernel<NUM><<<grid, BMP_NT, smem, ctl->stream>>>(bl, BIN_BMP_XL, BIN_BMP, a, b, o, ncols, W, counter);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
@@ -129,12 +129,21 @@ int launch_bitmap(clb_controls *ctl, const BinLists &bl, int bin, const AView &a
 template <bool NUM>
 int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o, uint64_t ncols,
                uint64_t nmax) {
+    // work counters of the dynamically scheduled launches
+    Temp<uint32_t> ctr;
+    CLB_RETURN_IF(ctr.alloc(ctl, 8));
+    CLB_TRY_CUDA(cudaMemsetAsync(ctr.ptr, 0, 8 * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     // Heavy bins first so the long rows start early.
-    CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, BIN_BMP, a, b, o, ncols, nmax, NUM ? "bitmap_numeric" : "bitmap_symbolic"));
-    CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax, NUM ? "hash8k_numeric" : "hash8k_symbolic")));
-    CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, nmax, NUM ? "hash4k_numeric" : "hash4k_symbolic")));
-    CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, nmax, NUM ? "hash2k_numeric" : "hash2k_symbolic")));
-    CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, nmax, NUM ? "hash1k_numeric" : "hash1k_symbolic")));
+    CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, a, b, o, ncols, nmax, ctr.ptr + 0,
+                                     NUM ? "bitmap_numeric" : "bitmap_symbolic"));
+    CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax, ctr.ptr + 1,
+                                               NUM ? "hash8k_numeric" : "hash8k_symbolic")));
+    CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, nmax, ctr.ptr + 2,
+                                               NUM ? "hash4k_numeric" : "hash4k_symbolic")));
+    CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, nmax, ctr.ptr + 3,
+                                               NUM ? "hash2k_numeric" : "hash2k_symbolic")));
+    CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, nmax, ctr.ptr + 4,
+                                               NUM ? "hash1k_numeric" : "hash1k_symbolic")));
     CLB_RETURN_IF((launch_esc<8, NUM>(ctl, bl, BIN_W8, a, b, o, nmax, NUM ? "esc256_numeric" : "esc256_symbolic")));
     CLB_RETURN_IF((launch_esc<4, NUM>(ctl, bl, BIN_W4, a, b, o, nmax, NUM ? "esc128_numeric" : "esc128_symbolic")));
     CLB_RETURN_IF((launch_esc<2, NUM>(ctl, bl, BIN_W2, a, b, o, nmax, NUM ? "esc64_numeric" : "esc64_symbolic")));

@@ -185,6 +185,21 @@ CLB_API int clb_csr_to_dcsr(clb_controls *ctl, const clb_csr *in, clb_dcsr *out)
 CLB_API int clb_dcsr_spgemm_hash(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
                          clb_spgemm_stats *stats);
 
+/* coo::matrix_addition (src/coo/coo.hpp:9-14, coo_matrix_addition.cpp:32-73):
+ * C = A | B of sorted unique COOs; same shapes or CLB_INVALID_ARGUMENT. */
+CLB_API int clb_coo_add(clb_controls *ctl, const clb_coo *a, const clb_coo *b, clb_coo *c);
+
+/* csr::matrix_addition (src/csr/csr.hpp:12, csr_addition.cpp:26-168). */
+CLB_API int clb_csr_add(clb_controls *ctl, const clb_csr *a, const clb_csr *b, clb_csr *c);
+
+/* dcsr::kronecker_product (src/dcsr/dcsr.hpp:38-41,
+ * dcsr_kronecker_product.cpp:5-64): C row (ia, ib) = A.rows[ia]*B.nrows +
+ * B.rows[ib], columns A.cols[ja]*B.ncols + B.cols[jb]. */
+CLB_API int clb_dcsr_kronecker(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c);
+
+/* dcsr::transpose (src/dcsr/dcsr.hpp:17-19, dcsr_transpose.cpp:5-16). */
+CLB_API int clb_dcsr_transpose(clb_controls *ctl, const clb_dcsr *in, clb_dcsr *out);
+
 /* Products per A row (count_workload, dcsr_matrix_multiplication.cpp:388-404):
  * workload has a->nzr entries in device memory; *total = their sum. */
 CLB_API int clb_dcsr_workload(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, uint32_t *workload,

@@ -1,0 +1,124 @@
+"""coo::matrix_addition, csr::matrix_addition, dcsr::kronecker_product and
+dcsr::transpose on the GPU vs the oracle and the golden digests recorded from
+the reference's CPU functions (test/test_operations.cpp:14-277)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from util import coo_digest, csr_digest, dcsr_digest, from_device, golden, pairs_dcsr, to_device
+
+pytestmark = pytest.mark.gpu
+G = golden()
+
+
+def _coo_dev(ctl, rows, cols, n):
+    import clbool_b200 as cb
+    return cb.matrix_coo.from_host(ctl, rows, cols, n, n)
+
+
+def _csr_dev(ctl, rows, cols, n):
+    import clbool_b200 as cb
+    return cb.csr_from_cpu(ctl, cb.csr_cpu_from_pairs(rows, cols, n, n))
+
+
+def test_addition_coo_golden(controls):
+    import clbool_b200 as cb
+    for case in G["addition_coo"]:
+        s, ka, kb = case["size"], case["k_a"], case["k_b"]
+        ar, ac = O.generate_coo_pairs(s * ka, s)
+        br, bc = O.generate_coo_pairs(s * kb, s)
+        c = cb.matrix_coo()
+        cb.coo.matrix_addition(controls, c, _coo_dev(controls, ar, ac, s), _coo_dev(controls, br, bc, s))
+        h = cb.matrix_coo_from_gpu(controls, c)
+        assert coo_digest(h.rows, h.cols) == case["sum"], case
+
+
+def test_addition_coo_small_grid(controls):
+    """addition_coo_small: sizes 0..2000 step 15 x k_a, k_b in 0..9 (subsampled)."""
+    import clbool_b200 as cb
+    for s in range(0, 2000, 15 * 9):
+        for ka in range(0, 10, 3):
+            for kb in range(0, 10, 4):
+                a = O.Coo(s, s, *O.generate_coo_pairs(s * ka, s))
+                b = O.Coo(s, s, *O.generate_coo_pairs(s * kb, s))
+                c = cb.coo.matrix_addition(controls, None, _coo_dev(controls, a.rows, a.cols, s),
+                                           _coo_dev(controls, b.rows, b.cols, s))
+                want = O.coo_add(a, b)
+                h = cb.matrix_coo_from_gpu(controls, c)
+                assert np.array_equal(h.rows, want.rows) and np.array_equal(h.cols, want.cols), (s, ka, kb)
+
+
+def test_addition_csr_golden(controls):
+    import clbool_b200 as cb
+    for case in G["addition_csr"]:
+        s, ka, kb = case["size"], case["k_a"], case["k_b"]
+        ar, ac = O.generate_coo_pairs(s * ka, s)
+        br, bc = O.generate_coo_pairs(s * kb, s)
+        c = cb.matrix_csr()
+        cb.csr.matrix_addition(controls, c, _csr_dev(controls, ar, ac, s), _csr_dev(controls, br, bc, s))
+        h = cb.matrix_csr_from_gpu(controls, c)
+        if case["sum"]["nnz"] == 0:
+            assert c.nnz() == 0
+            continue
+        assert csr_digest(O.Csr(s, s, h.rpt, h.cols)) == case["sum"], case
+
+
+def test_addition_csr_skewed(controls):
+    """Long rows beside short ones (tiles inside one row and tiles spanning
+    thousands of rows), empty rows, and a row that only one side has."""
+    import clbool_b200 as cb
+    from clbool_b200 import gen
+    r, c = gen.rmat(14, seed=5)
+    n = 1 << 14
+    a = O.Coo(n, n, r, c)
+    aa = O.spgemm(O.coo_to_dcsr(a), O.coo_to_dcsr(a))
+    csr_c = O.dcsr_to_csr(aa)
+    csr_a = O.coo_to_csr(a)
+    A = cb.csr_from_cpu(controls, cb.matrix_csr_cpu(csr_c.rpt, csr_c.cols, n, n))
+    B = cb.csr_from_cpu(controls, cb.matrix_csr_cpu(csr_a.rpt, csr_a.cols, n, n))
+    out = cb.csr.matrix_addition(controls, None, A, B)
+    h = cb.matrix_csr_from_gpu(controls, out)
+    want = O.csr_add(csr_c, csr_a)
+    assert np.array_equal(h.rpt, want.rpt) and np.array_equal(h.cols, want.cols)
+
+
+def test_addition_empty_and_shape(controls):
+    import clbool_b200 as cb
+    a = _coo_dev(controls, *O.generate_coo_pairs(500, 100), 100)
+    e = cb.matrix_coo.zeros(100, 100)
+    c = cb.coo.matrix_addition(controls, None, a, e)
+    assert c.nnz() == a.nnz() and c.rows_gpu() is not a.rows_gpu()  # a copy
+    assert cb.coo.matrix_addition(controls, None, e, e).nnz() == 0
+    with pytest.raises(cb.ClBoolException) as ex:
+        cb.coo.matrix_addition(controls, None, a, cb.matrix_coo.zeros(100, 101))
+    assert ex.value.status_name == "CLBOOL_INVALID_ARGUMENT"
+
+
+def test_kronecker_golden(controls):
+    import clbool_b200 as cb
+    for case in G["kronecker_dcsr"]:
+        r, c = O.generate_coo_pairs(case["nnz"], case["size"])
+        a = O.coo_to_dcsr(O.Coo(case["size"], case["size"], r, c))
+        k = cb.dcsr.kronecker_product(controls, None, to_device(controls, a), to_device(controls, a))
+        got = O.dcsr_to_coo(from_device(controls, k))
+        assert coo_digest(got.rows, got.cols) == case["kron"]
+
+
+@pytest.mark.parametrize("na,nb", [(300, 40), (1000, 3000), (1, 5000)])
+def test_kronecker_vs_oracle(controls, na, nb):
+    import clbool_b200 as cb
+    a = O.coo_to_dcsr(O.Coo(60, 70, *O.generate_coo_pairs(na, 60)))
+    b = O.coo_to_dcsr(O.Coo(500, 400, *O.generate_coo_pairs(nb, 400)))
+    a = a._replace(ncols=70)
+    b = b._replace(nrows=500)
+    k = cb.dcsr.kronecker_product(controls, None, to_device(controls, a), to_device(controls, b))
+    assert dcsr_digest(from_device(controls, k)) == dcsr_digest(O.kronecker(a, b))
+
+
+@pytest.mark.parametrize("size,k", [(0, 0), (5, 3), (95, 19), (900, 25), (9400, 60)])
+def test_transpose(controls, size, k):
+    """transpose_* suites (test_operations.cpp:14-37)."""
+    import clbool_b200 as cb
+    a = pairs_dcsr(size, k)
+    t = cb.dcsr.transpose(controls, None, to_device(controls, a))
+    assert dcsr_digest(from_device(controls, t)) == dcsr_digest(O.transpose(a))

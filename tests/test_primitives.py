@@ -29,8 +29,7 @@ def test_prefix_sum_sizes_u64(controls, n):
     v = rng.integers(0, 1 << 40, size=n, dtype=np.uint64)
     buf = cb.DeviceBuffer.from_host(controls, v, np.uint64)
     total = cb.prefix_sum(controls, buf, n)
-    want, wt = O.prefix_sum_u32(np.zeros(0)) if False else (None, None)
-    ref = np.concatenate([[0], np.cumsum(v)[:-1]]).astype(np.uint64)
+    ref = np.concatenate([np.zeros(1, np.uint64), np.cumsum(v, dtype=np.uint64)[:-1]])
     assert total == int(v.sum(dtype=np.uint64))
     assert np.array_equal(buf.to_host(), ref)
 
