@@ -302,17 +302,24 @@ __device__ __forceinline__ void balanced_products(const AView &a, const BRows &b
                 }
                 e = lo;
             }
+            // The current entry's end and the offset that maps a product
+            // index to its position in B.cols (mod 2^32: positions < 2^32).
+            uint32_t end = s_pre[e + 1];
+            uint32_t off = s_beg[e] - s_pre[e];
             uint32_t col[U];
             bool val[U];
 #pragma unroll
             for (int s = 0; s < U; ++s) {
                 const uint32_t q = p + (uint32_t)s * 32u;
                 val[s] = q < total;
-                col[s] = 0;
-                if (val[s]) {
-                    while (s_pre[e + 1] <= q) ++e;
-                    col[s] = __ldg(b.cols + s_beg[e] + (q - s_pre[e]));
+                if (val[s] && q >= end) {
+                    do {
+                        ++e;
+                        end = s_pre[e + 1];
+                    } while (q >= end);
+                    off = s_beg[e] - s_pre[e];
                 }
+                col[s] = val[s] ? __ldg(b.cols + (q + off)) : 0u;
             }
 #pragma unroll
             for (int s = 0; s < U; ++s) f(col[s], val[s]);
@@ -392,46 +399,53 @@ constexpr int BMP_NT = 1024;
 constexpr int BMP_NW = BMP_NT / 32;
 constexpr int BMP_ECH = 2048;
 constexpr uint32_t BMP_MAX_WORDS = 32768;  // 128 KB: 2^20 columns per chunk
+constexpr uint32_t BMP_UNIT = 4u * 32u * BMP_NW;  // words per emission sweep (4 per lane)
 
-// Words of the bitmap for `ncols` columns: a multiple of 32 * BMP_NW so the
-// warps split it evenly, at most BMP_MAX_WORDS.
+// Words of the bitmap for `ncols` columns: a multiple of BMP_UNIT so the
+// warps split it evenly in 4-word lane steps, at most BMP_MAX_WORDS.
 inline uint32_t bitmap_words(uint64_t ncols) {
     uint64_t w = (ncols + 31) / 32;
-    uint64_t unit = 32ull * BMP_NW;
-    w = (w + unit - 1) / unit * unit;
+    w = (w + BMP_UNIT - 1) / BMP_UNIT * BMP_UNIT;
     if (w > BMP_MAX_WORDS) w = BMP_MAX_WORDS;
     return (uint32_t)w;
 }
 
 // Dynamic shared memory of the bitmap kernel: W words + the entry stage.
-inline size_t bitmap_smem_bytes(uint32_t W) { return ((size_t)W + 2 * BMP_ECH + 1) * 4; }
+inline size_t bitmap_smem_bytes(uint32_t W) { return ((size_t)W + 2 * BMP_ECH + 4) * 4; }
 
-// Position of the n-th (0-based) set bit of w; w has more than n set bits.
-__device__ __forceinline__ uint32_t nth_set_bit(uint32_t w, uint32_t n) {
-    uint32_t pos = 0, c;
-    c = __popc(w & 0xFFFFu);
-    if (n >= c) { n -= c; w >>= 16; pos += 16; }
-    c = __popc(w & 0xFFu);
-    if (n >= c) { n -= c; w >>= 8; pos += 8; }
-    c = __popc(w & 0xFu);
-    if (n >= c) { n -= c; w >>= 4; pos += 4; }
-    c = __popc(w & 0x3u);
-    if (n >= c) { n -= c; w >>= 2; pos += 2; }
-    c = w & 1u;
-    if (n >= c) pos += 1;
-    return pos;
+// One warp-uniform step of bitmap insertion: lane sets bit `r` (if `in`).
+// Lanes reading one B row hold ascending columns, so lanes that hit the same
+// word form contiguous runs; when any run is longer than one lane, every run
+// ORs its bits with one redux and only the run head issues the atomic.
+__device__ __forceinline__ void bitmap_set(uint32_t *bm, uint32_t r, bool in) {
+    const uint32_t lane = lane_id();
+    const uint32_t wd = in ? (r >> 5) : 0xFFFFFFFFu;
+    uint32_t bit = in ? (1u << (r & 31)) : 0u;
+    const uint32_t upw = __shfl_up_sync(0xFFFFFFFFu, wd, 1);
+    const bool head = lane == 0 || upw != wd;
+    const uint32_t heads = __ballot_sync(0xFFFFFFFFu, head);
+    if (heads != 0xFFFFFFFFu) {
+        const uint32_t le = 0xFFFFFFFFu >> (31 - lane);            // lanes <= lane
+        const uint32_t h = 31 - __clz(heads & le);                // my run's head
+        const uint32_t gt = heads & ~le;                          // heads above lane
+        const uint32_t hi_mask = gt ? ((1u << (__ffs(gt) - 1)) - 1u) : 0xFFFFFFFFu;
+        const uint32_t mask = hi_mask & ~((1u << h) - 1u);
+        bit = __reduce_or_sync(mask, bit);
+    }
+    if (in && head) atomicOr(bm + wd, bit);
 }
 
 // Rows of bins [bin_lo, bin_hi] (contiguous in the list, heaviest first),
-// one row per CTA at a time, taken from `counter`.
-template <bool NUMERIC>
+// one row per CTA at a time, taken from `counter`.  MULTI: the columns do
+// not fit one bitmap chunk, so every chunk re-walks the row's products.
+template <bool NUMERIC, bool MULTI>
 __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int bin_lo, int bin_hi, AView a, BRows b,
                                                                RowOut o, uint64_t ncols, uint32_t W,
                                                                uint32_t *counter) {
-    extern __shared__ uint32_t smem[];
+    extern __shared__ __align__(16) uint32_t smem[];
     uint32_t *bm = smem;
     uint32_t *s_pre = smem + W;
-    uint32_t *s_beg = s_pre + BMP_ECH + 1;
+    uint32_t *s_beg = s_pre + BMP_ECH + 4;
     __shared__ uint32_t wtot[BMP_NW];
     __shared__ uint32_t scratch[33];
     __shared__ uint32_t s_slot;
@@ -443,6 +457,7 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
     const uint32_t lane = lane_id(), wi = warp_id();
     const uint32_t WPW = W / BMP_NW;  // words per warp in the emission pass
     const uint64_t chunk_cols = (uint64_t)W * 32;
+    uint4 *bm4 = reinterpret_cast<uint4 *>(bm);
     for (;;) {
         const uint32_t item = next_item(counter, &s_slot);
         if (item >= cnt) break;
@@ -450,40 +465,38 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
         uint64_t total = 0;
         const uint64_t out_base = NUMERIC ? o.row_off[i] : 0;
         bool overflowed = false;
-        for (uint64_t c0 = 0; c0 < ncols; c0 += chunk_cols) {
-            balanced_products<BMP_NT, BMP_ECH, 8>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
-                // unsigned wrap sends columns below c0 out of range too
-                const uint64_t r = (uint64_t)c - c0;
-                const bool in = valid && r < chunk_cols;
-                const uint32_t wd = in ? (uint32_t)(r >> 5) : 0xFFFFFFFFu;
-                uint32_t bit = in ? (1u << (r & 31)) : 0u;
-                // Lanes of one B row hold ascending columns: merge the bits of
-                // a run of lanes that target the same word, one atomic per run.
-                const uint32_t upw = __shfl_up_sync(0xFFFFFFFFu, wd, 1);
-                const bool head = lane == 0 || upw != wd;
-                if (__any_sync(0xFFFFFFFFu, in && !head)) {
-#pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        const uint32_t ob = __shfl_down_sync(0xFFFFFFFFu, bit, d);
-                        const uint32_t ow = __shfl_down_sync(0xFFFFFFFFu, wd, d);
-                        if (lane + d < 32 && ow == wd) bit |= ob;
-                    }
-                }
-                if (in && head) atomicOr(bm + wd, bit);
-            });
+        for (uint64_t c0 = 0; c0 < (MULTI ? ncols : 1); c0 += chunk_cols) {
+            if (MULTI) {
+                balanced_products<BMP_NT, BMP_ECH, 8>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
+                    // unsigned wrap sends columns below c0 out of range too
+                    const uint64_t r = (uint64_t)c - c0;
+                    const bool in = valid && r < chunk_cols;
+                    bitmap_set(bm, (uint32_t)r, in);
+                });
+            } else {
+                balanced_products<BMP_NT, BMP_ECH, 8>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
+                    bitmap_set(bm, c, valid && c < (uint32_t)chunk_cols);
+                });
+            }
             if (!NUMERIC || overflowed) {
                 uint32_t mine = 0;
-                for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) {
-                    mine += __popc(bm[w]);
-                    bm[w] = 0;
+                for (uint32_t w4 = threadIdx.x; w4 < W / 4; w4 += BMP_NT) {
+                    const uint4 x = bm4[w4];
+                    mine += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+                    bm4[w4] = make_uint4(0, 0, 0, 0);
                 }
                 total += block_sum<uint32_t, BMP_NT>(mine, scratch);
                 continue;
             }
-            // Emission: each warp owns WPW consecutive words.
+            // Emission: each warp owns WPW consecutive words, 4 per lane per
+            // step; a lane writes its words' columns in order at its scanned
+            // offset (consecutive lanes -> consecutive outputs when sparse).
             const uint32_t wbeg = wi * WPW;
             uint32_t mine = 0;
-            for (uint32_t w = wbeg + lane; w < wbeg + WPW; w += 32) mine += __popc(bm[w]);
+            for (uint32_t w = wbeg + 4 * lane; w < wbeg + WPW; w += 128) {
+                const uint4 x = bm4[w >> 2];
+                mine += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+            }
             mine = warp_sum(mine);
             if (lane == 0) wtot[wi] = mine;
             __syncthreads();
@@ -494,40 +507,32 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
                 ctot += v;
             }
             if (o.row_cap && total + ctot > o.row_cap[i]) {
-                // learned form: the row does not fit its slot; finish the
-                // count only (clears the bitmap) and flag it.
+                // learned form: the row does not fit its slot; clear the
+                // bitmap and flag the row.
                 overflowed = true;
-                for (uint32_t w = wbeg + lane; w < wbeg + WPW; w += 32) bm[w] = 0;
+                for (uint32_t w = wbeg + 4 * lane; w < wbeg + WPW; w += 128) bm4[w >> 2] = make_uint4(0, 0, 0, 0);
                 total += ctot;
                 __syncthreads();
                 continue;
             }
             uint64_t run = out_base + total + woff;
-            for (uint32_t w = wbeg; w < wbeg + WPW; w += 32) {
-                const uint32_t word = bm[w + lane];
-                bm[w + lane] = 0;
-                const uint32_t pc = __popc(word);
+            for (uint32_t w = wbeg; w < wbeg + WPW; w += 128) {
+                const uint32_t wl = w + 4 * lane;
+                const uint4 x = bm4[wl >> 2];
+                bm4[wl >> 2] = make_uint4(0, 0, 0, 0);
+                const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
                 const uint32_t inc = warp_inclusive_scan(pc);
-                const uint32_t T = __shfl_sync(0xFFFFFFFFu, inc, 31);
-                // Output k of this 32-word step goes to lane k % 32 (coalesced
-                // stores): find the source lane L (first with inc[L] > k) and
-                // the (k - exclusive[L])-th set bit of its word.
-                for (uint32_t k0 = 0; k0 < T; k0 += 32) {
-                    const uint32_t k = k0 + lane;
-                    uint32_t L = 0;
-#pragma unroll
-                    for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
-                        const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, L + sft - 1);
-                        if (v <= k) L += sft;
-                    }
-                    const uint32_t wL = __shfl_sync(0xFFFFFFFFu, word, L);
-                    const uint32_t exL = __shfl_sync(0xFFFFFFFFu, inc - pc, L);
-                    if (k < T) {
-                        const uint32_t colbase = (uint32_t)(c0 + (uint64_t)(w + L) * 32);
-                        o.cols[run + k] = colbase + nth_set_bit(wL, k - exL);
-                    }
-                }
-                run += T;
+                uint32_t *dst = o.cols + run + (inc - pc);
+                const uint32_t cb = (uint32_t)(c0 + (uint64_t)wl * 32);
+                uint32_t word = x.x;
+                while (word) { *dst++ = cb + (uint32_t)(__ffs(word) - 1); word &= word - 1; }
+                word = x.y;
+                while (word) { *dst++ = cb + 32u + (uint32_t)(__ffs(word) - 1); word &= word - 1; }
+                word = x.z;
+                while (word) { *dst++ = cb + 64u + (uint32_t)(__ffs(word) - 1); word &= word - 1; }
+                word = x.w;
+                while (word) { *dst++ = cb + 96u + (uint32_t)(__ffs(word) - 1); word &= word - 1; }
+                run += __shfl_sync(0xFFFFFFFFu, inc, 31);
             }
             total += ctot;
             __syncthreads();

@@ -110,20 +110,29 @@ int launch_hash(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, 
     return CLB_SUCCESS;
 }
 
-template <bool NUM>
-int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
-                  uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name) {
+template <bool NUM, bool MULTI>
+int launch_bitmap_t(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
+                    uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name) {
     const uint32_t W = bitmap_words(ncols);
     const size_t smem = bitmap_smem_bytes(W);
-    CLB_TRY_CUDA(cudaFuncSetAttribute(bitmap_cta_kernel<NUM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+    auto kern = bitmap_cta_kernel<NUM, MULTI>;
+    CLB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  CLB_RUN_KERNEL_FAILURE);
-    int occ = occupancy(bitmap_cta_kernel<NUM>, BMP_NT, smem);
+    int occ = occupancy(kern, BMP_NT, smem);
     unsigned grid = persistent_grid(ctl, occ, nmax);
     ProfScope ps(ctl, name);
-    bitmap_cta_kernel<NUM><<<grid, BMP_NT, smem, ctl->stream>>>(bl, BIN_BMP_XL, BIN_BMP, a, b, o, ncols, W, counter);
+    kern<<<grid, BMP_NT, smem, ctl->stream>>>(bl, BIN_BMP_XL, BIN_BMP, a, b, o, ncols, W, counter);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
+}
+
+template <bool NUM>
+int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
+                  uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name) {
+    const bool multi = ncols > (uint64_t)bitmap_words(ncols) * 32;
+    return multi ? launch_bitmap_t<NUM, true>(ctl, bl, a, b, o, ncols, nmax, counter, name)
+                 : launch_bitmap_t<NUM, false>(ctl, bl, a, b, o, ncols, nmax, counter, name);
 }
 
 template <bool NUM>

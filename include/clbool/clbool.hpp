@@ -1,0 +1,402 @@
+// clbool.hpp -- C++ host layer of the B200 back end, mirroring the
+// reference's public surface (include/clbool.hpp) over the C ABI in
+// clbool_b200.h.  Header-only; link against libclbool_b200.so.
+//
+//   Controls, create_controls, show_devices   src/core/controls.hpp, src/common/env.hpp
+//   Status, Exception                          src/core/error.hpp:130-213
+//   matrix_dcsr / matrix_coo / matrix_csr      src/core/matrix_{dcsr,coo,csr}.hpp
+//   matrix_*_cpu                               src/core/cpu_matrices.hpp
+//   dcsr::, coo::, csr:: operations            src/dcsr/dcsr.hpp, src/coo/coo.hpp, src/csr/csr.hpp
+//   conversions                                src/common/matrices_conversions.hpp
+//   prefix_sum, fill_with                      src/common/cl_operations.hpp
+//
+// Device arrays are held by shared_ptr, so copies of matrices are shallow
+// (the reference's cl::Buffer is reference counted the same way) and
+// conversions documented as "shallow for cols" share the column array.
+// Row pointers are uint64 on the device (the reference uses uint32).
+#pragma once
+
+#include <clbool_b200.h>
+
+#include <cstdint>
+#include <iostream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace clbool {
+
+enum Status {
+    CLBOOL_NO_SUCH_PROGRAM,
+    CLBOOL_CREATE_KERNEL_ERROR,
+    CLBOOL_BUILD_PROGRAM_ERROR,
+    CLBOOL_INCOMPLETE_KERNEL,
+    CLBOOL_RUN_KERNEL_FAILURE,
+    CLBOOL_EVENT_WAITING_ERROR,
+    CLBOOL_CREATE_BUFFER_ERROR,
+    CLBOOL_COPY_BUFFER_ERROR,
+    CLBOOL_READ_BUFFER_ERROR,
+    CLBOOL_WRITE_BUFFER_ERROR,
+    CLBOOL_CREATE_CONTROLS_ERROR,
+    CLBOOL_INVALID_ARGUMENT,
+    CLBOOL_INVALID_VALUE,
+    CLBOOL_INITIALIZATION_ERROR,
+    CLBOOL_DEVICE_STATUS_ERROR,
+    CLBOOL_NOT_SUPPORTED
+};
+
+class Exception : public std::exception {
+    std::string message_;
+    Status status_;
+
+public:
+    Exception(std::string message, Status status) : message_(std::move(message)), status_(status) {}
+    const char *what() const noexcept override { return message_.c_str(); }
+    Status status() const { return status_; }
+    std::string get_message() const { return message_; }
+};
+
+namespace details {
+inline Status to_status(int code) {
+    if (code >= 1 && code <= 14) return static_cast<Status>(code - 1);
+    if (code == CLB_DEVICE_STATUS_ERROR) return CLBOOL_DEVICE_STATUS_ERROR;
+    if (code == CLB_NOT_SUPPORTED) return CLBOOL_NOT_SUPPORTED;
+    return CLBOOL_RUN_KERNEL_FAILURE;
+}
+inline void check(int code) {
+    if (code != CLB_SUCCESS) {
+        std::string msg = std::string("[") + clb_status_string(code) + "] " + clb_last_error();
+        throw Exception(msg, to_status(code));
+    }
+}
+}  // namespace details
+
+// ------------------------------------------------------------------ controls
+struct Controls {
+    std::shared_ptr<clb_controls> handle;
+    int device = 0;
+
+    explicit Controls(int device_id = 0) : device(device_id) {
+        clb_controls *h = nullptr;
+        details::check(clb_controls_create(device_id, &h));
+        handle = std::shared_ptr<clb_controls>(h, [](clb_controls *p) { clb_controls_destroy(p); });
+    }
+    clb_controls *get() const { return handle.get(); }
+    void sync() const { details::check(clb_controls_sync(get())); }
+};
+
+inline Controls create_controls(uint32_t platform_id = 0, uint32_t device_id = 0) {
+    if (platform_id != 0) throw Exception("no platform with id " + std::to_string(platform_id),
+                                          CLBOOL_CREATE_CONTROLS_ERROR);
+    return Controls(static_cast<int>(device_id));
+}
+
+inline void show_devices() {
+    int n = 0;
+    details::check(clb_device_count(&n));
+    for (int d = 0; d < n; ++d) {
+        char name[256];
+        int sms = 0;
+        uint64_t mem = 0;
+        details::check(clb_device_info(d, name, sizeof(name), &sms, &mem));
+        std::cout << "device id: " << d << "  " << name << "  SMs=" << sms << "  mem=" << (mem >> 20) << " MiB\n";
+    }
+}
+
+// ------------------------------------------------------------ device memory
+class Buffer {
+    std::shared_ptr<void> ptr_;
+    size_t bytes_ = 0;
+
+public:
+    Buffer() = default;
+    // Takes ownership of a library allocation.
+    Buffer(const Controls &c, void *p, size_t bytes) : bytes_(bytes) {
+        auto h = c.handle;
+        ptr_ = std::shared_ptr<void>(p, [h](void *q) {
+            if (q) clb_free(h.get(), q);
+        });
+    }
+    static Buffer create(const Controls &c, size_t bytes) {
+        void *p = nullptr;
+        details::check(clb_malloc(c.get(), bytes, &p));
+        return Buffer(c, p, bytes);
+    }
+    template <class T>
+    static Buffer upload(const Controls &c, const T *src, size_t n) {
+        if (n == 0) return Buffer();
+        Buffer b = create(c, n * sizeof(T));
+        details::check(clb_memcpy_h2d(c.get(), b.get(), src, n * sizeof(T)));
+        return b;
+    }
+    template <class T>
+    std::vector<T> download(const Controls &c, size_t n) const {
+        std::vector<T> out(n);
+        if (n) details::check(clb_memcpy_d2h(c.get(), out.data(), get(), n * sizeof(T)));
+        return out;
+    }
+    void *get() const { return ptr_.get(); }
+    size_t bytes() const { return bytes_; }
+    explicit operator bool() const { return ptr_ != nullptr; }
+};
+
+// -------------------------------------------------------------- host types
+using cpu_buffer = std::vector<uint32_t>;
+using coordinates = std::pair<uint32_t, uint32_t>;
+using matrix_coo_cpu_pairs = std::vector<coordinates>;
+
+struct matrix_dcsr_cpu {
+    std::vector<uint64_t> rpt;
+    cpu_buffer rows, cols;
+};
+struct matrix_coo_cpu {
+    cpu_buffer rows, cols;
+};
+struct matrix_csr_cpu {
+    std::vector<uint64_t> rpt;
+    cpu_buffer cols;
+    uint64_t nrows = 0, ncols = 0;
+};
+
+// ------------------------------------------------------------ device types
+namespace details {
+class matrix_base {
+protected:
+    uint64_t _nrows = 0, _ncols = 0, _nnz = 0;
+
+public:
+    using index_type = uint32_t;
+    matrix_base() = default;
+    matrix_base(uint64_t r, uint64_t c, uint64_t n) : _nrows(r), _ncols(c), _nnz(n) {}
+    uint64_t nrows() const { return _nrows; }
+    uint64_t ncols() const { return _ncols; }
+    uint64_t nnz() const { return _nnz; }
+    bool empty() const { return _nnz == 0; }
+};
+}  // namespace details
+
+class matrix_dcsr : public details::matrix_base {
+    Buffer _rpt, _rows, _cols;
+    uint64_t _nzr = 0;
+
+public:
+    matrix_dcsr() = default;
+    matrix_dcsr(uint64_t nrows, uint64_t ncols) : matrix_base(nrows, ncols, 0) {}
+    matrix_dcsr(Buffer rpt, Buffer rows, Buffer cols, uint64_t nrows, uint64_t ncols, uint64_t nnz, uint64_t nzr)
+        : matrix_base(nrows, ncols, nnz), _rpt(std::move(rpt)), _rows(std::move(rows)), _cols(std::move(cols)),
+          _nzr(nzr) {}
+    uint64_t nzr() const { return _nzr; }
+    const Buffer &rpt_gpu() const { return _rpt; }
+    const Buffer &rows_gpu() const { return _rows; }
+    const Buffer &cols_gpu() const { return _cols; }
+    clb_dcsr view() const {
+        return clb_dcsr{_nrows, _ncols, _nnz, _nzr, (uint64_t *)_rpt.get(), (uint32_t *)_rows.get(),
+                        (uint32_t *)_cols.get()};
+    }
+    // Wrap a clb_dcsr returned by the library; `cols_shared` keeps a column
+    // array that the result shares with an input.
+    static matrix_dcsr adopt(const Controls &c, const clb_dcsr &s, const Buffer *cols_shared = nullptr) {
+        if (s.nnz == 0) return matrix_dcsr(s.nrows, s.ncols);
+        Buffer cols = (cols_shared && cols_shared->get() == s.cols) ? *cols_shared : Buffer(c, s.cols, s.nnz * 4);
+        return matrix_dcsr(Buffer(c, s.rpt, (s.nzr + 1) * 8), Buffer(c, s.rows, s.nzr * 4), cols, s.nrows, s.ncols,
+                           s.nnz, s.nzr);
+    }
+};
+
+class matrix_csr : public details::matrix_base {
+    Buffer _rpt, _cols;
+
+public:
+    matrix_csr() = default;
+    matrix_csr(uint64_t nrows, uint64_t ncols) : matrix_base(nrows, ncols, 0) {}
+    matrix_csr(Buffer rpt, Buffer cols, uint64_t nrows, uint64_t ncols, uint64_t nnz)
+        : matrix_base(nrows, ncols, nnz), _rpt(std::move(rpt)), _cols(std::move(cols)) {}
+    const Buffer &rpt_gpu() const { return _rpt; }
+    const Buffer &cols_gpu() const { return _cols; }
+    clb_csr view() const { return clb_csr{_nrows, _ncols, _nnz, (uint64_t *)_rpt.get(), (uint32_t *)_cols.get()}; }
+    static matrix_csr adopt(const Controls &c, const clb_csr &s, const Buffer *cols_shared = nullptr) {
+        if (s.nnz == 0) return matrix_csr(s.nrows, s.ncols);
+        Buffer cols = (cols_shared && cols_shared->get() == s.cols) ? *cols_shared : Buffer(c, s.cols, s.nnz * 4);
+        return matrix_csr(Buffer(c, s.rpt, (s.nrows + 1) * 8), cols, s.nrows, s.ncols, s.nnz);
+    }
+};
+
+class matrix_coo : public details::matrix_base {
+    Buffer _rows, _cols;
+
+public:
+    matrix_coo() = default;
+    matrix_coo(uint64_t nrows, uint64_t ncols) : matrix_base(nrows, ncols, 0) {}
+    matrix_coo(Buffer rows, Buffer cols, uint64_t nrows, uint64_t ncols, uint64_t nnz)
+        : matrix_base(nrows, ncols, nnz), _rows(std::move(rows)), _cols(std::move(cols)) {}
+    // matrix_coo(controls, rows, cols, nrows, ncols, nnz, sorted, noDuplicates)
+    // (src/core/matrix_coo.cpp:17-47).
+    matrix_coo(const Controls &c, const uint32_t *rows, const uint32_t *cols, uint64_t nrows, uint64_t ncols,
+               uint64_t nnz, bool sorted = true, bool noDuplicates = true)
+        : matrix_base(nrows, ncols, nnz) {
+        if (nnz == 0) return;
+        _rows = Buffer::upload(c, rows, nnz);
+        _cols = Buffer::upload(c, cols, nnz);
+        if (!sorted) details::check(clb_coo_sort(c.get(), (uint32_t *)_rows.get(), (uint32_t *)_cols.get(), nnz));
+        if (!noDuplicates) {
+            clb_coo in = view(), out{};
+            details::check(clb_coo_reduce_duplicates(c.get(), &in, &out));
+            *this = adopt(c, out);
+        }
+    }
+    const Buffer &rows_gpu() const { return _rows; }
+    const Buffer &cols_gpu() const { return _cols; }
+    clb_coo view() const { return clb_coo{_nrows, _ncols, _nnz, (uint32_t *)_rows.get(), (uint32_t *)_cols.get()}; }
+    static matrix_coo adopt(const Controls &c, const clb_coo &s, const Buffer *rows_shared = nullptr,
+                            const Buffer *cols_shared = nullptr) {
+        if (s.nnz == 0) return matrix_coo(s.nrows, s.ncols);
+        Buffer rows = (rows_shared && rows_shared->get() == s.rows) ? *rows_shared : Buffer(c, s.rows, s.nnz * 4);
+        Buffer cols = (cols_shared && cols_shared->get() == s.cols) ? *cols_shared : Buffer(c, s.cols, s.nnz * 4);
+        return matrix_coo(rows, cols, s.nrows, s.ncols, s.nnz);
+    }
+};
+
+// ---------------------------------------------------------------- primitives
+inline uint64_t prefix_sum(Controls &c, Buffer &array, uint64_t &total_sum, uint64_t array_size) {
+    uint64_t t = 0;
+    details::check(clb_prefix_sum_u32(c.get(), (uint32_t *)array.get(), array_size, &t));
+    total_sum = t;
+    return t;
+}
+
+inline void fill_with(Controls &c, Buffer &array, uint64_t size, uint32_t value) {
+    details::check(clb_fill_u32(c.get(), (uint32_t *)array.get(), size, value));
+}
+inline void fill_with_zeroes(Controls &c, Buffer &array, uint64_t size) { fill_with(c, array, size, 0); }
+
+// --------------------------------------------------------------- conversions
+inline matrix_dcsr coo_to_dcsr_shallow(Controls &c, const matrix_coo &a) {
+    if (a.empty()) return matrix_dcsr(a.nrows(), a.ncols());
+    clb_coo in = a.view();
+    clb_dcsr out{};
+    details::check(clb_coo_to_dcsr(c.get(), &in, &out, 0));
+    return matrix_dcsr::adopt(c, out, &a.cols_gpu());
+}
+
+inline matrix_coo dcsr_to_coo_shallow(Controls &c, const matrix_dcsr &a) {
+    if (a.empty()) return matrix_coo(a.nrows(), a.ncols());
+    clb_dcsr in = a.view();
+    clb_coo out{};
+    details::check(clb_dcsr_to_coo(c.get(), &in, &out, 0));
+    return matrix_coo::adopt(c, out, nullptr, &a.cols_gpu());
+}
+
+inline matrix_coo dcsr_to_coo_deep(Controls &c, const matrix_dcsr &a) {
+    if (a.empty()) return matrix_coo(a.nrows(), a.ncols());
+    clb_dcsr in = a.view();
+    clb_coo out{};
+    details::check(clb_dcsr_to_coo(c.get(), &in, &out, 1));
+    return matrix_coo::adopt(c, out);
+}
+
+// shallow for cols!
+inline matrix_csr dcsr_to_csr(Controls &c, const matrix_dcsr &m) {
+    if (m.empty()) return matrix_csr(m.nrows(), m.ncols());
+    clb_dcsr in = m.view();
+    clb_csr out{};
+    details::check(clb_dcsr_to_csr(c.get(), &in, &out));
+    return matrix_csr::adopt(c, out, &m.cols_gpu());
+}
+
+// shallow for cols!
+inline matrix_dcsr csr_to_dcsr(Controls &c, const matrix_csr &m) {
+    if (m.empty()) return matrix_dcsr(m.nrows(), m.ncols());
+    clb_csr in = m.view();
+    clb_dcsr out{};
+    details::check(clb_csr_to_dcsr(c.get(), &in, &out));
+    return matrix_dcsr::adopt(c, out, &m.cols_gpu());
+}
+
+inline matrix_dcsr matrix_dcsr_from_cpu(Controls &c, const matrix_dcsr_cpu &m, uint64_t size) {
+    if (m.cols.empty()) return matrix_dcsr(size, size);
+    return matrix_dcsr(Buffer::upload(c, m.rpt.data(), m.rpt.size()), Buffer::upload(c, m.rows.data(), m.rows.size()),
+                       Buffer::upload(c, m.cols.data(), m.cols.size()), size, size, m.cols.size(), m.rows.size());
+}
+
+inline matrix_dcsr_cpu matrix_dcsr_from_gpu(Controls &c, const matrix_dcsr &m) {
+    if (m.empty()) return {};
+    return {m.rpt_gpu().download<uint64_t>(c, m.nzr() + 1), m.rows_gpu().download<uint32_t>(c, m.nzr()),
+            m.cols_gpu().download<uint32_t>(c, m.nnz())};
+}
+
+inline matrix_coo_cpu matrix_coo_from_gpu(Controls &c, const matrix_coo &m) {
+    if (m.empty()) return {};
+    return {m.rows_gpu().download<uint32_t>(c, m.nnz()), m.cols_gpu().download<uint32_t>(c, m.nnz())};
+}
+
+inline matrix_csr_cpu matrix_csr_from_gpu(Controls &c, const matrix_csr &m) {
+    if (m.empty()) return {{}, {}, m.nrows(), m.ncols()};
+    return {m.rpt_gpu().download<uint64_t>(c, m.nrows() + 1), m.cols_gpu().download<uint32_t>(c, m.nnz()), m.nrows(),
+            m.ncols()};
+}
+
+inline matrix_csr_cpu csr_cpu_from_pairs(const matrix_coo_cpu_pairs &mat, uint64_t m, uint64_t n) {
+    matrix_csr_cpu out;
+    out.nrows = m;
+    out.ncols = n;
+    out.rpt.assign(m + 1, 0);
+    out.cols.resize(mat.size());
+    for (size_t j = 0; j < mat.size(); ++j) {
+        out.rpt[mat[j].first + 1]++;
+        out.cols[j] = mat[j].second;
+    }
+    for (uint64_t i = 0; i < m; ++i) out.rpt[i + 1] += out.rpt[i];
+    return out;
+}
+
+inline matrix_csr csr_from_cpu(Controls &c, const matrix_csr_cpu &m) {
+    if (m.cols.empty()) return matrix_csr(m.nrows, m.ncols);
+    return matrix_csr(Buffer::upload(c, m.rpt.data(), m.rpt.size()), Buffer::upload(c, m.cols.data(), m.cols.size()),
+                      m.nrows, m.ncols, m.cols.size());
+}
+
+// ---------------------------------------------------------------- operations
+namespace dcsr {
+inline void matrix_multiplication_hash(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &a,
+                                       const matrix_dcsr &b, clb_spgemm_stats *stats = nullptr) {
+    clb_dcsr va = a.view(), vb = b.view(), out{};
+    details::check(clb_dcsr_spgemm_hash(c.get(), &va, &vb, &out, stats));
+    matrix_out = matrix_dcsr::adopt(c, out);
+}
+
+inline void kronecker_product(Controls &c, matrix_dcsr &matrix_c, const matrix_dcsr &matrix_a,
+                              const matrix_dcsr &matrix_b) {
+    clb_dcsr va = matrix_a.view(), vb = matrix_b.view(), out{};
+    details::check(clb_dcsr_kronecker(c.get(), &va, &vb, &out));
+    matrix_c = matrix_dcsr::adopt(c, out);
+}
+
+inline void transpose(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &matrix_in) {
+    clb_dcsr v = matrix_in.view(), out{};
+    details::check(clb_dcsr_transpose(c.get(), &v, &out));
+    matrix_out = matrix_dcsr::adopt(c, out);
+}
+}  // namespace dcsr
+
+namespace coo {
+inline void matrix_addition(Controls &c, matrix_coo &matrix_out, const matrix_coo &a, const matrix_coo &b) {
+    clb_coo va = a.view(), vb = b.view(), out{};
+    details::check(clb_coo_add(c.get(), &va, &vb, &out));
+    matrix_out = matrix_coo::adopt(c, out);
+}
+
+inline void sort_arrays(Controls &c, Buffer &rows_gpu, Buffer &cols_gpu, uint64_t n) {
+    details::check(clb_coo_sort(c.get(), (uint32_t *)rows_gpu.get(), (uint32_t *)cols_gpu.get(), n));
+}
+}  // namespace coo
+
+namespace csr {
+inline void matrix_addition(Controls &c, matrix_csr &out, const matrix_csr &a, const matrix_csr &b) {
+    clb_csr va = a.view(), vb = b.view(), o{};
+    details::check(clb_csr_add(c.get(), &va, &vb, &o));
+    out = matrix_csr::adopt(c, o);
+}
+}  // namespace csr
+
+}  // namespace clbool
