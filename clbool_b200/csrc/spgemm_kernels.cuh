@@ -290,17 +290,22 @@ __device__ __forceinline__ void balanced_products(const AView &a, const BRows &b
         }
         if (threadIdx.x == 0) s_pre[n] = total;
         __syncthreads();
+        uint32_t e = 0;  // lane's entry cursor, carried from chunk to chunk
         for (uint32_t base = w * WCH; base < total; base += NW * WCH) {
             const uint32_t p = base + lane;
-            uint32_t e;
-            {   // largest e in [0, n) with s_pre[e] <= p
-                uint32_t lo = 0, hi = n - 1;
+            {   // largest e in [e, n) with s_pre[e] <= p: short linear walk,
+                // binary search when the cursor is more than 8 entries behind
                 const uint32_t key = p < total ? p : total - 1;
-                while (lo < hi) {
-                    const uint32_t m = (lo + hi + 1) >> 1;
-                    if (s_pre[m] <= key) lo = m; else hi = m - 1;
+                if (e + 8 < n && s_pre[e + 8] <= key) {
+                    uint32_t lo = e + 8, hi = n - 1;
+                    while (lo < hi) {
+                        const uint32_t m = (lo + hi + 1) >> 1;
+                        if (s_pre[m] <= key) lo = m; else hi = m - 1;
+                    }
+                    e = lo;
+                } else {
+                    while (s_pre[e + 1] <= key) ++e;
                 }
-                e = lo;
             }
             // The current entry's end and the offset that maps a product
             // index to its position in B.cols (mod 2^32: positions < 2^32).
@@ -411,12 +416,32 @@ inline uint32_t bitmap_words(uint64_t ncols) {
 }
 
 // Dynamic shared memory of the bitmap kernel: W words + the entry stage.
-inline size_t bitmap_smem_bytes(uint32_t W) { return ((size_t)W + 2 * BMP_ECH + 4) * 4; }
+inline size_t bitmap_smem_bytes(uint32_t W) { return ((size_t)W + 2 * BMP_ECH + 4 + BMP_NT + 4) * 4; }
+
+// Position of the n-th (0-based) set bit of w; w has more than n set bits.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t w, uint32_t n) {
+    uint32_t pos = 0, c;
+    c = __popc(w & 0xFFFFu);
+    if (n >= c) { n -= c; w >>= 16; pos += 16; }
+    c = __popc(w & 0xFFu);
+    if (n >= c) { n -= c; w >>= 8; pos += 8; }
+    c = __popc(w & 0xFu);
+    if (n >= c) { n -= c; w >>= 4; pos += 4; }
+    c = __popc(w & 0x3u);
+    if (n >= c) { n -= c; w >>= 2; pos += 2; }
+    c = w & 1u;
+    if (n >= c) pos += 1;
+    return pos;
+}
 
 // One warp-uniform step of bitmap insertion: lane sets bit `r` (if `in`).
 // Lanes reading one B row hold ascending columns, so lanes that hit the same
-// word form contiguous runs; when any run is longer than one lane, every run
-// ORs its bits with one redux and only the run head issues the atomic.
+// word form contiguous runs (heads = first lane of each run).  All branches
+// below are warp-uniform:
+//   * every lane its own run  -> one atomic per lane;
+//   * at most 4 distinct words (dense hub rows) -> a full-warp OR reduction
+//     per word and one atomic per word;
+//   * otherwise a shuffle segmented OR and one atomic per run.
 __device__ __forceinline__ void bitmap_set(uint32_t *bm, uint32_t r, bool in) {
     const uint32_t lane = lane_id();
     const uint32_t wd = in ? (r >> 5) : 0xFFFFFFFFu;
@@ -424,13 +449,26 @@ __device__ __forceinline__ void bitmap_set(uint32_t *bm, uint32_t r, bool in) {
     const uint32_t upw = __shfl_up_sync(0xFFFFFFFFu, wd, 1);
     const bool head = lane == 0 || upw != wd;
     const uint32_t heads = __ballot_sync(0xFFFFFFFFu, head);
-    if (heads != 0xFFFFFFFFu) {
-        const uint32_t le = 0xFFFFFFFFu >> (31 - lane);            // lanes <= lane
-        const uint32_t h = 31 - __clz(heads & le);                // my run's head
-        const uint32_t gt = heads & ~le;                          // heads above lane
-        const uint32_t hi_mask = gt ? ((1u << (__ffs(gt) - 1)) - 1u) : 0xFFFFFFFFu;
-        const uint32_t mask = hi_mask & ~((1u << h) - 1u);
-        bit = __reduce_or_sync(mask, bit);
+    if (heads == 0xFFFFFFFFu) {
+        if (in) atomicOr(bm + wd, bit);
+        return;
+    }
+    if (__popc(heads) <= 4) {
+        uint32_t hm = heads;
+        while (hm) {
+            const int h = __ffs(hm) - 1;
+            hm &= hm - 1;
+            const uint32_t ww = __shfl_sync(0xFFFFFFFFu, wd, h);
+            const uint32_t x = __reduce_or_sync(0xFFFFFFFFu, wd == ww ? bit : 0u);
+            if ((int)lane == h && ww != 0xFFFFFFFFu) atomicOr(bm + ww, x);
+        }
+        return;
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t ob = __shfl_down_sync(0xFFFFFFFFu, bit, d);
+        const uint32_t ow = __shfl_down_sync(0xFFFFFFFFu, wd, d);
+        if (lane + d < 32 && ow == wd) bit |= ob;
     }
     if (in && head) atomicOr(bm + wd, bit);
 }
@@ -446,16 +484,15 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
     uint32_t *bm = smem;
     uint32_t *s_pre = smem + W;
     uint32_t *s_beg = s_pre + BMP_ECH + 4;
-    __shared__ uint32_t wtot[BMP_NW];
+    uint32_t *soff = s_beg + BMP_ECH;  // step output offsets (<= BMP_NT + 1)
     __shared__ uint32_t scratch[33];
-    __shared__ uint32_t s_slot;
+    __shared__ uint32_t s_slot, s_next;
     uint32_t beg, cnt = 0, tmp;
     bin_range(bl, bin_lo, beg, tmp);
     for (int q = bin_lo; q <= bin_hi; ++q) cnt += bl.info[q];
     for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) bm[w] = 0;
     __syncthreads();
     const uint32_t lane = lane_id(), wi = warp_id();
-    const uint32_t WPW = W / BMP_NW;  // words per warp in the emission pass
     const uint64_t chunk_cols = (uint64_t)W * 32;
     uint4 *bm4 = reinterpret_cast<uint4 *>(bm);
     for (;;) {
@@ -467,15 +504,15 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
         bool overflowed = false;
         for (uint64_t c0 = 0; c0 < (MULTI ? ncols : 1); c0 += chunk_cols) {
             if (MULTI) {
-                balanced_products<BMP_NT, BMP_ECH, 8>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
+                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
                     // unsigned wrap sends columns below c0 out of range too
                     const uint64_t r = (uint64_t)c - c0;
                     const bool in = valid && r < chunk_cols;
                     bitmap_set(bm, (uint32_t)r, in);
                 });
             } else {
-                balanced_products<BMP_NT, BMP_ECH, 8>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
-                    bitmap_set(bm, c, valid && c < (uint32_t)chunk_cols);
+                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
+                    if (valid && c < (uint32_t)chunk_cols) atomicOr(bm + (c >> 5), 1u << (c & 31));
                 });
             }
             if (!NUMERIC || overflowed) {
@@ -488,51 +525,71 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
                 total += block_sum<uint32_t, BMP_NT>(mine, scratch);
                 continue;
             }
-            // Emission: each warp owns WPW consecutive words, 4 per lane per
-            // step; a lane writes its words' columns in order at its scanned
-            // offset (consecutive lanes -> consecutive outputs when sparse).
-            const uint32_t wbeg = wi * WPW;
-            uint32_t mine = 0;
-            for (uint32_t w = wbeg + 4 * lane; w < wbeg + WPW; w += 128) {
-                const uint4 x = bm4[w >> 2];
-                mine += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+            // Emission, balanced by output: thread t counts 32-word step t,
+            // a block scan gives every step's output offset, and warp w takes
+            // the steps whose first output lies in the w-th 1/32 of the row's
+            // outputs (R-MAT columns are skewed: equal word ranges would give
+            // one warp most of the output).  Empty steps are skipped.
+            const uint32_t nsteps = W >> 5;
+            uint32_t scnt = 0;
+            if (threadIdx.x < nsteps) {
+                const uint4 *p4 = bm4 + threadIdx.x * 8;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const uint4 x = p4[k];
+                    scnt += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+                }
             }
-            mine = warp_sum(mine);
-            if (lane == 0) wtot[wi] = mine;
+            uint32_t ctot;
+            const uint32_t ex = block_exclusive_scan<uint32_t, BMP_NT>(scnt, scratch, &ctot);
+            if (threadIdx.x < nsteps) soff[threadIdx.x] = ex;
+            if (threadIdx.x == 0) {
+                soff[nsteps] = ctot;
+                s_next = 0;
+            }
             __syncthreads();
-            uint64_t woff = 0, ctot = 0;
-            for (uint32_t q = 0; q < (uint32_t)BMP_NW; ++q) {
-                const uint32_t v = wtot[q];
-                woff += q < wi ? v : 0;
-                ctot += v;
-            }
             if (o.row_cap && total + ctot > o.row_cap[i]) {
                 // learned form: the row does not fit its slot; clear the
                 // bitmap and flag the row.
                 overflowed = true;
-                for (uint32_t w = wbeg + 4 * lane; w < wbeg + WPW; w += 128) bm4[w >> 2] = make_uint4(0, 0, 0, 0);
+                for (uint32_t w4 = threadIdx.x; w4 < W / 4; w4 += BMP_NT) bm4[w4] = make_uint4(0, 0, 0, 0);
                 total += ctot;
                 __syncthreads();
                 continue;
             }
-            uint64_t run = out_base + total + woff;
-            for (uint32_t w = wbeg; w < wbeg + WPW; w += 128) {
-                const uint32_t wl = w + 4 * lane;
-                const uint4 x = bm4[wl >> 2];
-                bm4[wl >> 2] = make_uint4(0, 0, 0, 0);
-                const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+            uint32_t *const out = o.cols + out_base + total;
+            // Steps are taken dynamically (two per grab): the cost of a step
+            // follows its non-empty words, which no static split predicts.
+            for (;;) {
+                uint32_t g = 0;
+                if (lane == 0) g = atomicAdd(&s_next, 2u);
+                g = __shfl_sync(0xFFFFFFFFu, g, 0);
+                if (g >= nsteps) break;
+                for (uint32_t st = g; st < g + 2 && st < nsteps; ++st) {
+                const uint32_t pos = soff[st];
+                const uint32_t T = soff[st + 1] - pos;
+                if (T == 0) continue;  // empty step (warp-uniform)
+                const uint32_t word = bm[st * 32 + lane];
+                if (word) bm[st * 32 + lane] = 0;
+                // Output k of the step is written by lane k % 32 (coalesced):
+                // its source word is the first lane whose inclusive count
+                // exceeds k, its column the matching set bit of that word.
+                const uint32_t pc = __popc(word);
                 const uint32_t inc = warp_inclusive_scan(pc);
-                uint32_t *dst = o.cols + run + (inc - pc);
-                const uint32_t cb = (uint32_t)(c0 + (uint64_t)wl * 32);
-                uint32_t word = x.x;
-                while (word) { *dst++ = cb + (uint32_t)(__ffs(word) - 1); word &= word - 1; }
-                word = x.y;
-                while (word) { *dst++ = cb + 32u + (uint32_t)(__ffs(word) - 1); word &= word - 1; }
-                word = x.z;
-                while (word) { *dst++ = cb + 64u + (uint32_t)(__ffs(word) - 1); word &= word - 1; }
-                word = x.w;
-                while (word) { *dst++ = cb + 96u + (uint32_t)(__ffs(word) - 1); word &= word - 1; }
-                run += __shfl_sync(0xFFFFFFFFu, inc, 31);
+                const uint32_t cb = (uint32_t)(c0 + (uint64_t)st * 1024u);
+                for (uint32_t k0 = 0; k0 < T; k0 += 32) {
+                    const uint32_t k = k0 + lane;
+                    uint32_t L = 0;
+#pragma unroll
+                    for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
+                        const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, L + sft - 1);
+                        if (v <= k) L += sft;
+                    }
+                    const uint32_t wL = __shfl_sync(0xFFFFFFFFu, word, L);
+                    const uint32_t exL = __shfl_sync(0xFFFFFFFFu, inc - pc, L);
+                    if (k < T) out[pos + k] = cb + L * 32u + nth_set_bit(wL, k - exL);
+                }
+                }
             }
             total += ctot;
             __syncthreads();
