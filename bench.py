@@ -368,7 +368,7 @@ def cpu_baseline(n, rpt, rows, cols, work) -> dict:
     """The oracle's multithreaded CPU product on a seeded sample of A's rows."""
     import oracle as O
     threads = O.set_threads(os.cpu_count() or 1)
-    pick = _row_sample(rows.size, 0.25)
+    pick = _row_sample(rows.size, 0.10)
     srpt, srows, scols = _sub_dcsr(rpt, rows, cols, pick)
     A = O.Dcsr(n, n, srpt, srows, scols)
     B = O.Dcsr(n, n, rpt, rows, cols)
@@ -378,7 +378,7 @@ def cpu_baseline(n, rpt, rows, cols, work) -> dict:
     p = int(work[pick].sum())
     del C
     return {"value": p / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"25% of A's stored rows (seed 7): {pick.size} rows, {p} products, {dt:.2f} s"}
+            "sample": f"10% of A's stored rows (seed 7): {pick.size} rows, {p} products, {dt:.2f} s"}
 
 
 def run_reference(args) -> dict:
@@ -440,7 +440,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=20)
     ap.add_argument("--form", default="two_pass", choices=["two_pass", "learned"])
-    ap.add_argument("--ref-rows", type=int, default=24)
+    ap.add_argument("--ref-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
