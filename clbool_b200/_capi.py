@@ -77,6 +77,7 @@ _SIGS = {
     "clb_prefix_sum_u32": (C.c_int, [vp, vp, C.c_uint64, P(C.c_uint64)]),
     "clb_prefix_sum_u64": (C.c_int, [vp, vp, C.c_uint64, P(C.c_uint64)]),
     "clb_fill_u32": (C.c_int, [vp, vp, C.c_uint64, C.c_uint32]),
+    "clb_prefix_sum_u32_noalloc": (C.c_int, [vp, C.c_uint64, vp, vp]),
     "clb_coo_to_dcsr": (C.c_int, [vp, P(clb_coo), P(clb_dcsr), C.c_int]),
     "clb_dcsr_to_coo": (C.c_int, [vp, P(clb_dcsr), P(clb_coo), C.c_int]),
     "clb_dcsr_to_csr": (C.c_int, [vp, P(clb_dcsr), P(clb_csr)]),

@@ -9,6 +9,9 @@
 // Each warp owns a contiguous 512-element segment and walks it in 32-wide
 // coalesced steps with a shuffle scan, so loads and stores are fully
 // coalesced and no shared-memory transpose is needed.
+#include <mutex>
+#include <string>
+
 #include "common.cuh"
 
 namespace clb {
@@ -121,11 +124,74 @@ int scan_u64_inplace(clb_controls *ctl, uint64_t *data, uint64_t n, uint64_t *d_
     return scan_impl<uint64_t, uint64_t>(ctl, data, data, n, d_total);
 }
 
+// ------------------------------------------------ allocation-free variant --
+// Some callers cannot allocate device memory at the point where they need a
+// scan: a runtime that has reserved all of the GPU's memory for its own pool,
+// or a latency-critical loop that must not pay for cudaMalloc's implicit
+// synchronisation.  For them, the scan's only scratch (one 64-bit partial
+// sum per 4096-element tile) lives in this fixed array that the library
+// image brings with it.  Every GPU that loads the library holds the array
+// (512 KiB) until the process exits.
+constexpr uint64_t NOALLOC_MAX_TILES = 65536;  // n <= 65536 * 4096 = 2^28 entries
+static __device__ __align__(256) uint64_t g_scan_scratch[NOALLOC_MAX_TILES];
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_scratch_mutex;
+uint64_t *g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_scan_scratch on `device`, resolved once per device
+// with that device current.  In host code the array's name is only a host
+// stand-in, never a device address, so kernels must get this pointer.
+int scratch_address(int device, uint64_t **out) {
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES)
+        return fail(CLB_NOT_SUPPORTED, "device ordinal beyond the static scratch table");
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_scan_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(CLB_INITIALIZATION_ERROR,
+                        std::string("cudaGetSymbolAddress of the scan scratch: ") + cudaGetErrorString(e));
+        g_scratch_addr[device] = static_cast<uint64_t *>(p);
+    }
+    *out = g_scratch_addr[device];
+    return CLB_SUCCESS;
+}
+
+}  // namespace
+
 }  // namespace clb
 
 using namespace clb;
 
 extern "C" {
+
+int clb_prefix_sum_u32_noalloc(uint32_t *array, uint64_t n, uint64_t *d_total, void *stream) {
+    if (n && !array) return fail(CLB_INVALID_ARGUMENT, "array is NULL");
+    if (n > NOALLOC_MAX_TILES * SCAN_TILE)
+        return fail(CLB_INVALID_ARGUMENT, "prefix sum of " + std::to_string(n) +
+                                              " entries exceeds the static scratch limit of 2^28 entries");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        if (d_total) CLB_TRY_CUDA(cudaMemsetAsync(d_total, 0, sizeof(uint64_t), s), CLB_RUN_KERNEL_FAILURE);
+        return CLB_SUCCESS;
+    }
+    int device = 0;
+    CLB_TRY_CUDA(cudaGetDevice(&device), CLB_RUN_KERNEL_FAILURE);
+    uint64_t *sums = nullptr;
+    CLB_RETURN_IF(scratch_address(device, &sums));
+    // The tile sums are written in full by the first kernel before anything
+    // reads them, so the array's leftovers from an earlier call need no
+    // clearing.
+    const uint64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    tile_reduce_kernel<uint32_t><<<(unsigned)ntiles, SCAN_NT, 0, s>>>(array, n, sums);
+    tiles_scan_kernel<<<1, TS_NT, 0, s>>>(sums, ntiles, d_total);
+    downsweep_kernel<uint32_t, uint32_t><<<(unsigned)ntiles, SCAN_NT, 0, s>>>(array, array, n, sums);
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
 
 int clb_prefix_sum_u32(clb_controls *ctl, uint32_t *array, uint64_t n, uint64_t *total) {
     if (!ctl || (n && !array)) return fail(CLB_INVALID_ARGUMENT, "NULL argument");

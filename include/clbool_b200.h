@@ -155,6 +155,22 @@ CLB_API int clb_csr_release(clb_controls *ctl, clb_csr *m);
 CLB_API int clb_prefix_sum_u32(clb_controls *ctl, uint32_t *array, uint64_t n, uint64_t *total);
 CLB_API int clb_prefix_sum_u64(clb_controls *ctl, uint64_t *array, uint64_t n, uint64_t *total);
 
+/* No counterpart in the reference.  The same exclusive scan of `n` uint32
+ * entries in place, for callers that cannot allocate device memory when they
+ * need it (for instance a runtime that has reserved all of the GPU's memory
+ * for its own pool, or a hot loop that must not pay for cudaMalloc's implicit
+ * synchronisation).  It allocates nothing: its scratch is a fixed 512 KiB
+ * array inside the library, so n is limited to 2^28 entries (larger n is
+ * rejected with CLB_INVALID_ARGUMENT).  It takes no controls object, launches
+ * on `stream` (a cudaStream_t of the current device; NULL = legacy default
+ * stream), does not synchronise, and writes the sum of the inputs to the
+ * device pointer `d_total` when it is not NULL.  The first call on a device
+ * looks up the scratch array's device address for that device; make that
+ * first call before any stream capture.  Every call shares the one array, so
+ * calls whose work overlaps on the GPU (different streams, or different host
+ * threads on one device) race: serialise them. */
+CLB_API int clb_prefix_sum_u32_noalloc(uint32_t *array, uint64_t n, uint64_t *d_total, void *stream);
+
 /* fill_with (src/common/cl_operations.hpp:14, cl_operations.cpp:94-100). */
 CLB_API int clb_fill_u32(clb_controls *ctl, uint32_t *array, uint64_t n, uint32_t value);
 
