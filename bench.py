@@ -135,29 +135,107 @@ def bin_of(p: np.ndarray, bound: np.ndarray) -> np.ndarray:
     return b
 
 
-KERNEL_BIN = {"bitmap": (9, 10, 11), "hash8k": 8, "hash4k": 7, "hash2k": 6, "hash1k": 5, "esc256": 4, "esc128": 3,
+KERNEL_BIN = {"bitmap": (9, 10, 11), "hash8k": 8, "hash4k": 7, "hash2k": 6, "hash1k": 5, "cta_esc4096": 8,
+              "cta_esc2048": 7, "cta_esc1024": 6, "cta_esc512": 5, "esc256": 4, "esc128": 3,
               "esc64": 2, "esc32": 1}
 
 
-def algorithmic_bytes(kernel: str, a_len: np.ndarray, work: np.ndarray, c_len: np.ndarray, ncols: int) -> int:
+def algorithmic_bytes(kernel: str, a_len: np.ndarray, work: np.ndarray, c_len: np.ndarray, ncols: int,
+                      bound: np.ndarray | None = None) -> int:
     """Bytes the accumulator launch `kernel` must move for its rows, by the
     per-row model: A row pointer pair + row id (12 B), per A entry its column
     and B's row pointer pair (12 B), every product's B column (4 B), and for
     the numeric pass C's columns (4 B each) plus C's row pointer and id (12 B);
     the symbolic pass writes one 4-byte count per row instead."""
-    base = kernel.split("_")[0]
+    symbolic = kernel.endswith("_symbolic")
+    base = kernel.rsplit("_", 1)[0] if symbolic or kernel.endswith("_numeric") else kernel
     if base not in KERNEL_BIN:
         return 0
-    bins = bin_of(work, np.minimum(work, ncols))
+    bins = bin_of(work, np.minimum(work, ncols) if bound is None else bound)
     m = np.isin(bins, np.atleast_1d(KERNEL_BIN[base]))
     rows = int(m.sum())
     reads = 12 * rows + 12 * int(a_len[m].sum()) + 4 * int(work[m].sum())
-    if kernel.endswith("numeric"):
+    if not symbolic:
         return reads + 4 * int(c_len[m].sum()) + 12 * rows
     return reads + 4 * rows
 
 
 # --------------------------------------------------------------- our arm --
+def make_mxm(form: str, ctl, cb, sizer_path: str):
+    """The public call one step makes: (A, B, stats) -> C."""
+    if form == "learned":
+        from clbool_b200 import sizing
+        sizer = sizing.RowSizer.load(ctl, sizer_path)
+        return lambda A, B, stats=None: sizing.matrix_multiplication_learned(ctl, None, A, B, sizer, stats=stats)
+    if form == "esc":
+        return lambda A, B, stats=None: cb.dcsr.matrix_multiplication(ctl, None, A, B, stats=stats)
+    return lambda A, B, stats=None: cb.dcsr.matrix_multiplication_hash(ctl, None, A, B, stats=stats)
+
+
+def timed_steps(ctl, mxm, A, B, steps: int, l2_flush, barrier, srows, dev, want_c_len: bool):
+    """K steps, each bracketed by a CUDA event pair on the library's stream
+    (the whole call, host-side gaps included); the library's per-launch
+    profile records (also CUDA events on that stream) attribute the time to
+    kernels.  L2 is flushed between steps, outside the events."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctl.stream, device=f"cuda:{dev}")
+    ev_ms, kern_ms, prof_tot, launches, st, c_len = [], [], {}, 0, {}, None
+    with ClockSampler(dev) as clk:
+        barrier()
+        ctl.sync()
+        t0 = time.perf_counter()
+        for k in range(steps):
+            l2_flush()
+            ctl.profile(True)
+            st = {}
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            c = mxm(A, B, st)
+            e1.record(stream)
+            e1.synchronize()
+            prof = ctl.profile_read()
+            ctl.profile(False)
+            launches += st["kernel_launches"]
+            ev_ms.append(e0.elapsed_time(e1))
+            kern_ms.append(sum(v[1] for v in prof.values()))
+            for name, (cnt, ms) in prof.items():
+                a, b = prof_tot.get(name, (0, 0.0))
+                prof_tot[name] = (a + cnt, b + ms)
+            if want_c_len and k == steps - 1 and c.nnz():
+                crpt = c.rpt_gpu().to_host(c.nzr() + 1).astype(np.int64)
+                crow = c.rows_gpu().to_host(c.nzr())
+                c_len = np.zeros(srows.size, np.int64)
+                c_len[np.searchsorted(srows, crow)] = np.diff(crpt)
+            del c
+        ctl.sync()
+        barrier()
+        wall = time.perf_counter() - t0
+    return {"ev_ms": ev_ms, "kern_ms": kern_ms, "prof": prof_tot, "launches": launches, "stats": st,
+            "c_len": c_len, "wall": wall, "clocks": clk.summary()}
+
+
+def reduce_over_ranks(dist, dev, my_ms: float, my_products: int, my_nnz: int):
+    if dist is None:
+        return my_ms, float(my_products), float(my_nnz)
+    import torch
+    t = torch.tensor([my_ms, float(my_products), float(my_nnz)], dtype=torch.float64, device=f"cuda:{dev}")
+    mx = t.clone()
+    dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
+    dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(t[1]), float(t[2])
+
+
+def learned_bounds(ctl, cb, A, B, sizer_path: str, work: np.ndarray, ncols: int) -> np.ndarray:
+    """The capacities the learned form gives A's rows (host restatement of its
+    capacity rule), to attribute rows to accumulator bins."""
+    from clbool_b200 import sizing
+    from clbool_b200.train_sizer import capacities
+    sizer = sizing.RowSizer.load(ctl, sizer_path)
+    feat, _ = sizing.row_features(ctl, A, B)
+    pred = sizer.predict(feat, A.nzr()).to_host(A.nzr())
+    return capacities(pred, work, ncols, sizing.DEFAULT_MARGIN_LOG2, sizing.DEFAULT_SLACK)
+
+
 def run_ours(args, rank: int, world: int, dist) -> dict | None:
     import clbool_b200 as cb
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -181,74 +259,48 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     def l2_flush():
         cb.lib.clb_fill_u32(ctl.handle, __import__("ctypes").c_void_p(flush.ptr), (256 << 20) // 4, 0)
 
-    def step(stats=None):
-        return cb.dcsr.matrix_multiplication_hash(ctl, None, A, A_full, stats=stats)
-
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    # warm-up
+    mxm = make_mxm(args.form, ctl, cb, args.sizer)
     for _ in range(args.warmup):
-        c = step()
+        c = mxm(A, A_full)
         del c
     ctl.sync()
-
-    # timed region: per-step CUDA events via the library's profile records,
-    # L2 flushed between steps outside the events.
-    import ctypes
-    ev_ms = []
-    prof_tot: dict = {}
-    launches = 0
-    st = {}
-    c_len = None
-    with ClockSampler(dev) as clk:
-        barrier()
-        ctl.sync()
-        t0 = time.perf_counter()
-        for k in range(args.steps):
-            l2_flush()
-            ctl.profile(True)
-            st = {}
-            c = step(st)
-            prof = ctl.profile_read()
-            ctl.profile(False)
-            launches += st["kernel_launches"]
-            step_ms = sum(v[1] for v in prof.values())
-            ev_ms.append(step_ms)
-            for name, (cnt, ms) in prof.items():
-                a, b = prof_tot.get(name, (0, 0.0))
-                prof_tot[name] = (a + cnt, b + ms)
-            if k == args.steps - 1 and c.nnz():
-                crpt = c.rpt_gpu().to_host(c.nzr() + 1).astype(np.int64)
-                crow = c.rows_gpu().to_host(c.nzr())
-                c_len = np.zeros(srows.size, np.int64)
-                c_len[np.searchsorted(srows, crow)] = np.diff(crpt)
-            del c
-        ctl.sync()
-        barrier()
-        wall = time.perf_counter() - t0
-    clocks = clk.summary()
-    # device time: the events bracket the library's kernels; the profile's
-    # per-kernel spans tile each call, so their sum is the call's device time.
-    my_ms = sum(ev_ms)
-    if dist is not None:
-        import torch
-        t = torch.tensor([my_ms, float(my_products), float(st.get("nnz", 0))], dtype=torch.float64, device=f"cuda:{dev}")
-        mx = t.clone()
-        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        total_ms, products_all, nnz_all = float(mx[0]), float(t[1]), float(t[2])
-    else:
-        total_ms, products_all, nnz_all = my_ms, float(my_products), float(st.get("nnz", 0))
+    run = timed_steps(ctl, mxm, A, A_full, args.steps, l2_flush, barrier, srows, dev, True)
+    st = run["stats"]
+    total_ms, products_all, nnz_all = reduce_over_ranks(dist, dev, sum(run["ev_ms"]), my_products, st.get("nnz", 0))
     ms_per_step = total_ms / args.steps
     value = products_all / (ms_per_step / 1e3)
 
+    # the same workload through the exact two-pass form, for the comparison
+    compare = None
+    if args.form != "two_pass" and not args.no_compare:
+        mxm2 = make_mxm("two_pass", ctl, cb, args.sizer)
+        for _ in range(max(1, args.warmup // 2)):
+            c = mxm2(A, A_full)
+            del c
+        ctl.sync()
+        run2 = timed_steps(ctl, mxm2, A, A_full, args.steps, l2_flush, barrier, srows, dev, False)
+        t2, _, _ = reduce_over_ranks(dist, dev, sum(run2["ev_ms"]), my_products, 0)
+        v2 = products_all / (t2 / args.steps / 1e3)
+        compare = {"form": "two_pass", "value": v2, "ms_per_step": t2 / args.steps,
+                   f"{args.form}_over_two_pass": value / v2,
+                   "kernels_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in
+                                           sorted(run2["prof"].items(), key=lambda kv: -kv[1][1])}}
+
     # roofline of the dominant kernel (largest device time in the timed steps)
     peak, peak_kind = peaks()
-    top = max(prof_tot.items(), key=lambda kv: kv[1][1])
-    top_name, (top_launches, top_ms) = top
-    alg = algorithmic_bytes(top_name, a_len, mywork, c_len if c_len is not None else np.zeros_like(mywork), n)
+    prof_tot = run["prof"]
+    top_name, (top_launches, top_ms) = max(prof_tot.items(), key=lambda kv: kv[1][1])
+    bound = None
+    if args.form == "learned":
+        bound = learned_bounds(ctl, cb, A, A_full, args.sizer, mywork, n)
+    elif args.form == "esc":
+        bound = mywork
+    c_len = run["c_len"]
+    alg = algorithmic_bytes(top_name, a_len, mywork, c_len if c_len is not None else np.zeros_like(mywork), n, bound)
     per_launch_ms = top_ms / max(top_launches, 1)
     achieved = alg / (per_launch_ms / 1e3) / 1e9 if alg else None
     traffic = None
@@ -260,7 +312,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
             traffic = None
 
     # end to end through the public API with host buffers
-    e2e = run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, my_products, dist, dev)
+    e2e = run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, my_products, dist, dev, mxm)
 
     if rank != 0:
         return None
@@ -269,7 +321,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic", "impl": "ours",
-        "config": {"workload": f"rmat_s{args.scale}_AxA_hash_{args.form}", "scale": args.scale, "edge_factor": 16,
+        "config": {"workload": f"rmat_s{args.scale}_AxA_{args.form}", "scale": args.scale, "edge_factor": 16,
                    "abcd": [0.57, 0.19, 0.19, 0.05], "nnz_A": int(nnz_a), "products": int(products_all),
                    "nnz_C": int(nnz_all), "form": args.form, "parallelism": f"rows{world}",
                    "l2": "256 MiB device memset between steps, outside the step events; C (>30 GB) also exceeds L2"},
@@ -279,14 +331,19 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                      "alg_bytes_per_launch": alg, "launch_ms": per_launch_ms},
         "kernels_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in sorted(prof_tot.items(),
                                                                                  key=lambda kv: -kv[1][1])},
-        "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "wall_s": wall,
+        "kernel_ms_per_step_sum": sum(run["kern_ms"]) / args.steps,
+        "e2e": e2e, "gpu_launches": run["launches"], "clocks": run["clocks"], "wall_s": run["wall"],
     }
+    if args.form != "two_pass":
+        line["form_stats"] = {k: st.get(k) for k in ("capacity", "fallback_rows", "nzr", "nnz")}
+    if compare is not None:
+        line["compare"] = compare
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(n, rpt, rows, cols, work)
     return line
 
 
-def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev) -> dict:
+def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev, mxm) -> dict:
     """products/s through the public API: pinned host A -> device, SpGEMM,
     all of C -> pinned host, per step."""
     import ctypes
@@ -302,8 +359,7 @@ def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev) -
     ctypes.memmove(h_rows, srows.ctypes.data, srows.nbytes)
     ctypes.memmove(h_cols, scols.ctypes.data, scols.nbytes)
     # size of C, to stage the read-back in pinned memory
-    c0 = cb.dcsr.matrix_multiplication_hash(ctl, None, cb.matrix_dcsr_from_cpu(
-        ctl, cb.matrix_dcsr_cpu(srpt, srows, scols), n), A_full)
+    c0 = mxm(cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(srpt, srows, scols), n), A_full)
     c_bytes = (8 * (c0.nzr() + 1) + 4 * c0.nzr() + 4 * c0.nnz()) if c0.nnz() else 0
     h_c = pinned(c_bytes)
     del c0
@@ -321,7 +377,7 @@ def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev) -
         lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(d_rows.ptr), h_rows, srows.nbytes)
         lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(d_cols.ptr), h_cols, scols.nbytes)
         A = cb.matrix_dcsr(d_rpt, d_rows, d_cols, n, n, scols.size, srows.size)
-        C = cb.dcsr.matrix_multiplication_hash(ctl, None, A, A_full)
+        C = mxm(A, A_full)
         if C.nnz():
             off = 0
             for buf, nb in ((C.rpt_gpu(), 8 * (C.nzr() + 1)), (C.rows_gpu(), 4 * C.nzr()), (C.cols_gpu(), 4 * C.nnz())):
@@ -424,7 +480,7 @@ def run_reference(args) -> dict:
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ts / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"rmat_s{args.scale}_AxA_hash_{args.form}", "scale": args.scale},
+            "config": {"workload": f"rmat_s{args.scale}_AxA_{args.form}", "scale": args.scale},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{threads} threads x {per_thread_rows} random stored rows of A per step "
                                        f"(coo_utils::matrix_multiplication_cpu)"},
@@ -439,10 +495,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=20)
-    ap.add_argument("--form", default="two_pass", choices=["two_pass", "learned"])
+    ap.add_argument("--form", default=None, choices=["two_pass", "learned", "esc"],
+                    help="default: learned when the packaged predictor checkpoint exists, else two_pass")
+    ap.add_argument("--sizer", default=os.path.join(ROOT, "clbool_b200", "sizer_rmat.npz"),
+                    help="predictor checkpoint of the learned form")
+    ap.add_argument("--no-compare", action="store_true", help="skip timing the two-pass form beside it")
     ap.add_argument("--ref-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.form is None:
+        args.form = "learned" if os.path.exists(args.sizer) else "two_pass"
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -84,17 +84,26 @@ _SIGS = {
     "clb_csr_to_dcsr": (C.c_int, [vp, P(clb_csr), P(clb_dcsr)]),
     "clb_dcsr_spgemm_hash": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_stats)]),
     "clb_dcsr_workload": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, P(C.c_uint64)]),
-}
-
-# Entry points added as the library grows; bound when present.
-_OPTIONAL = {
     "clb_dcsr_spgemm_esc": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_stats)]),
     "clb_coo_add": (C.c_int, [vp, P(clb_coo), P(clb_coo), P(clb_coo)]),
     "clb_csr_add": (C.c_int, [vp, P(clb_csr), P(clb_csr), P(clb_csr)]),
     "clb_dcsr_kronecker": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr)]),
     "clb_dcsr_transpose": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr)]),
+    # learned sizing
+    "clb_sizer_num_params": (C.c_int, []),
+    "clb_sizer_create": (C.c_int, [vp, C.c_uint64, P(vp)]),
+    "clb_sizer_destroy": (C.c_int, [vp]),
+    "clb_sizer_get_params": (C.c_int, [vp, vp, C.c_size_t]),
+    "clb_sizer_set_params": (C.c_int, [vp, vp, C.c_size_t]),
+    "clb_dcsr_row_features": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, vp]),
+    "clb_dcsr_row_nnz": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp]),
+    "clb_sizer_predict": (C.c_int, [vp, vp, C.c_uint64, vp]),
+    "clb_sizer_gradients": (C.c_int, [vp, vp, vp, C.c_uint64, vp, P(C.c_float)]),
+    "clb_sizer_train": (C.c_int, [vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64,
+                                  P(C.c_float)]),
+    "clb_dcsr_spgemm_learned": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, C.c_float, C.c_float, P(clb_dcsr),
+                                          P(clb_spgemm_stats)]),
 }
-
 
 def _load():
     if not os.path.exists(LIB_PATH):
@@ -104,11 +113,6 @@ def _load():
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
-    for name, (res, args) in _OPTIONAL.items():
-        f = getattr(lib, name, None)
-        if f is not None:
-            f.restype = res
-            f.argtypes = args
     return lib
 
 
@@ -116,4 +120,4 @@ lib = _load()
 
 
 def declared_symbols() -> list[str]:
-    return sorted(list(_SIGS) + list(_OPTIONAL))
+    return sorted(_SIGS)

@@ -97,6 +97,9 @@ int main() {
         matrix_dcsr C;
         dcsr::matrix_multiplication_hash(controls, C, A, B);
         EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, C)) == product(pa, pb));
+        matrix_dcsr C2;
+        dcsr::matrix_multiplication(controls, C2, A, B);
+        EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, C2)) == product(pa, pb));
 
         std::vector<uint32_t> ar, ac, br, bc;
         for (auto &p : pa) { ar.push_back(p.first); ac.push_back(p.second); }

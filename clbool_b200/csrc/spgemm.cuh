@@ -21,6 +21,14 @@ int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, con
 // C.rpt/C.rows from the row flags' exclusive scan (pos) and the row offsets.
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
                     const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz);
+// Numeric accumulators without (hash_bins = false) the hash bins.
+int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
+                               const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins);
+// Single-pass forms (spgemm_single.cu): capacity slots, one numeric pass,
+// exact fallback for rows that outgrew their capacity, compaction.
+int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
+                       const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
+                       clb_spgemm_stats *st);
 int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
                          clb_spgemm_stats *stats);
 

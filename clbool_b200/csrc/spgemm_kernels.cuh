@@ -254,7 +254,8 @@ __device__ __forceinline__ void block_bitonic_sort(uint32_t *s, uint32_t M) {
 // flattened chunk, each lane walking its own entry cursor forward (one
 // binary search per warp chunk).  Consecutive lanes read consecutive columns
 // of one B row (coalesced) and each lane has U loads in flight before f runs.
-// f(col, valid) is called warp-uniformly (all 32 lanes, valid or not).
+// f(col, valid, idx) is called warp-uniformly (all 32 lanes, valid or not);
+// idx is the product's index in the row's flattened product list.
 template <int NT, int ECH, int U, class F>
 __device__ __forceinline__ void balanced_products(const AView &a, const BRows &b, uint32_t i, uint32_t *s_pre,
                                                   uint32_t *s_beg, uint32_t *scratch, F &&f) {
@@ -263,6 +264,7 @@ __device__ __forceinline__ void balanced_products(const AView &a, const BRows &b
     constexpr uint32_t WCH = 32u * U;
     const uint32_t lane = lane_id(), w = warp_id();
     const uint64_t ja = a.rpt[i], je = a.rpt[i + 1];
+    uint32_t done = 0;  // products of the row in earlier entry chunks
     for (uint64_t c0 = ja; c0 < je; c0 += ECH) {
         const uint32_t n = (uint32_t)min((uint64_t)ECH, je - c0);
         for (uint32_t e = threadIdx.x; e < n; e += NT) {
@@ -327,8 +329,9 @@ __device__ __forceinline__ void balanced_products(const AView &a, const BRows &b
                 col[s] = val[s] ? __ldg(b.cols + (q + off)) : 0u;
             }
 #pragma unroll
-            for (int s = 0; s < U; ++s) f(col[s], val[s]);
+            for (int s = 0; s < U; ++s) f(col[s], val[s], done + p + (uint32_t)s * 32u);
         }
+        done += total;
         __syncthreads();
     }
 }
@@ -352,7 +355,7 @@ __global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AVie
     __shared__ uint32_t s_pre[HASH_ECH + 1];
     __shared__ uint32_t s_beg[HASH_ECH];
     __shared__ uint32_t scratch[33];
-    __shared__ uint32_t s_slot;
+    __shared__ uint32_t s_slot, s_full;
     uint32_t beg, cnt;
     bin_range(bl, bin, beg, cnt);
     for (;;) {
@@ -360,11 +363,20 @@ __global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AVie
         if (item >= cnt) break;
         const uint32_t i = bl.list[beg + item];
         for (int s = threadIdx.x; s < T; s += NT) table[s] = EMPTY;
+        if (threadIdx.x == 0) s_full = 0;
         __syncthreads();
         uint32_t mine = 0;
-        balanced_products<NT, HASH_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
-            if (valid) mine += hash_insert<T>(table, c, o.status);
+        // With capacities (single-pass forms) a table that fills up means the
+        // row outgrew its capacity: flag the row instead of the device status.
+        uint32_t *probe_flag = o.row_cap ? &s_full : o.status;
+        balanced_products<NT, HASH_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t) {
+            if (valid) mine += hash_insert<T>(table, c, probe_flag);
         });
+        if (o.row_cap && s_full) {  // block-uniform after the iterator's barrier
+            if (threadIdx.x == 0) o.overflow[i] = 1;
+            __syncthreads();
+            continue;
+        }
         if (!NUMERIC) {
             uint32_t total = block_sum<uint32_t, NT>(mine, scratch);
             if (threadIdx.x == 0) o.row_nnz[i] = total;
@@ -504,14 +516,14 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
         bool overflowed = false;
         for (uint64_t c0 = 0; c0 < (MULTI ? ncols : 1); c0 += chunk_cols) {
             if (MULTI) {
-                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
+                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t) {
                     // unsigned wrap sends columns below c0 out of range too
                     const uint64_t r = (uint64_t)c - c0;
                     const bool in = valid && r < chunk_cols;
                     bitmap_set(bm, (uint32_t)r, in);
                 });
             } else {
-                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid) {
+                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t) {
                     if (valid && c < (uint32_t)chunk_cols) atomicOr(bm + (c >> 5), 1u << (c & 31));
                 });
             }

@@ -137,7 +137,7 @@ int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const B
 
 template <bool NUM>
 int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o, uint64_t ncols,
-               uint64_t nmax) {
+               uint64_t nmax, bool hash_bins = true) {
     // work counters of the dynamically scheduled launches
     Temp<uint32_t> ctr;
     CLB_RETURN_IF(ctr.alloc(ctl, 8));
@@ -145,14 +145,16 @@ int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRow
     // Heavy bins first so the long rows start early.
     CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, a, b, o, ncols, nmax, ctr.ptr + 0,
                                      NUM ? "bitmap_numeric" : "bitmap_symbolic"));
-    CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax, ctr.ptr + 1,
-                                               NUM ? "hash8k_numeric" : "hash8k_symbolic")));
-    CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, nmax, ctr.ptr + 2,
-                                               NUM ? "hash4k_numeric" : "hash4k_symbolic")));
-    CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, nmax, ctr.ptr + 3,
-                                               NUM ? "hash2k_numeric" : "hash2k_symbolic")));
-    CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, nmax, ctr.ptr + 4,
-                                               NUM ? "hash1k_numeric" : "hash1k_symbolic")));
+    if (hash_bins) {
+        CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax, ctr.ptr + 1,
+                                                   NUM ? "hash8k_numeric" : "hash8k_symbolic")));
+        CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, nmax, ctr.ptr + 2,
+                                                   NUM ? "hash4k_numeric" : "hash4k_symbolic")));
+        CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, nmax, ctr.ptr + 3,
+                                                   NUM ? "hash2k_numeric" : "hash2k_symbolic")));
+        CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, nmax, ctr.ptr + 4,
+                                                   NUM ? "hash1k_numeric" : "hash1k_symbolic")));
+    }
     CLB_RETURN_IF((launch_esc<8, NUM>(ctl, bl, BIN_W8, a, b, o, nmax, NUM ? "esc256_numeric" : "esc256_symbolic")));
     CLB_RETURN_IF((launch_esc<4, NUM>(ctl, bl, BIN_W4, a, b, o, nmax, NUM ? "esc128_numeric" : "esc128_symbolic")));
     CLB_RETURN_IF((launch_esc<2, NUM>(ctl, bl, BIN_W2, a, b, o, nmax, NUM ? "esc64_numeric" : "esc64_symbolic")));
@@ -177,6 +179,11 @@ int launch_binning(clb_controls *ctl, const uint32_t *work, const uint32_t *cap,
 int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, const AView &a, const BRows &b,
                         const RowOut &o, uint64_t ncols, uint64_t nmax) {
     return numeric ? launch_all<true>(ctl, bl, a, b, o, ncols, nmax) : launch_all<false>(ctl, bl, a, b, o, ncols, nmax);
+}
+
+int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
+                               const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins) {
+    return launch_all<true>(ctl, bl, a, b, o, ncols, nmax, hash_bins);
 }
 
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,

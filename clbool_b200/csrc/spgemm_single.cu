@@ -1,0 +1,394 @@
+// spgemm_single.cu -- single-pass SpGEMM forms: ESC/merge (dcsr::matrix_multiplication)
+// and the learned-capacity form.
+//
+// Reference ESC form: src/dcsr/dcsr_matrix_multiplication.cpp:26-97 -- count the
+// workload, bin rows by it, give every row its upper bound of slots in a
+// "pre" matrix (build_groups_and_allocate_new_matrix, :319-375), run one
+// numeric kernel per group (copy_one_value / heap_merge / bitonic_esc /
+// merge_large_rows, :193-317), then compact into C (create_final_matrix,
+// :100-168).
+//
+// Here both single-pass forms share one driver:
+//   capacity[i] -> slots (scan) -> one numeric pass into the slots, every row
+//   recording its exact count and flagging overflow -> overflowed rows
+//   re-run by the exact two-pass form -> compaction into contiguous C.
+// ESC form: capacity = min(products, ncols) (an exact upper bound, never
+//   overflows); accumulators: warp ESC (<= 256 products), CTA ESC -- expand
+//   into shared memory, bitonic sort, keep first of every run -- (<= 4096
+//   products), bitmap (the rest).
+// Learned form: capacity from the row-size predictor (mlp.cu); accumulators
+//   binned by the capacity; rows whose count exceeds it are re-run exactly.
+#include <string>
+
+#include "spgemm.cuh"
+
+namespace clb {
+
+namespace {
+
+// ------------------------------------------------------------ CTA ESC ----
+template <int NP, int NT>
+__global__ void __launch_bounds__(NT) cta_esc_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o,
+                                                     const uint32_t *__restrict__ work, uint32_t *counter) {
+    constexpr int SPT = NP / NT;
+    __shared__ uint32_t keys[NP];
+    __shared__ uint32_t s_pre[HASH_ECH + 1];
+    __shared__ uint32_t s_beg[HASH_ECH];
+    __shared__ uint32_t scratch[33];
+    __shared__ uint32_t s_slot;
+    uint32_t beg, cnt;
+    bin_range(bl, bin, beg, cnt);
+    for (;;) {
+        const uint32_t item = next_item(counter, &s_slot);
+        if (item >= cnt) break;
+        const uint32_t i = bl.list[beg + item];
+        uint32_t P = work[i];
+        if (P > (uint32_t)NP) {  // binning guarantees P <= NP
+            if (threadIdx.x == 0) raise_status(o.status, DEV_BOUNDS);
+            P = NP;
+        }
+        // expand: product idx of the row goes to keys[idx]
+        balanced_products<NT, HASH_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t idx) {
+            if (valid && idx < (uint32_t)NP) keys[idx] = c;
+        });
+        uint32_t M = 1;
+        while (M < P) M <<= 1;
+        for (uint32_t s = P + threadIdx.x; s < M; s += NT) keys[s] = EMPTY;
+        __syncthreads();
+        // sort
+        block_bitonic_sort<NT>(keys, M);
+        // compress: keep the first of every run (thread-contiguous segments)
+        uint32_t v[SPT], flags = 0, mine = 0;
+#pragma unroll
+        for (int k = 0; k < SPT; ++k) {
+            const uint32_t s = threadIdx.x * SPT + k;
+            v[k] = s < P ? keys[s] : EMPTY;
+            const bool f = s < P && (s == 0 || v[k] != keys[s - 1]);
+            flags |= (f ? 1u : 0u) << k;
+            mine += f ? 1u : 0u;
+        }
+        uint32_t nnz;
+        uint32_t pos = block_exclusive_scan<uint32_t, NT>(mine, scratch, &nnz);
+        if (o.row_cap && nnz > o.row_cap[i]) {
+            if (threadIdx.x == 0) o.overflow[i] = 1;
+            continue;
+        }
+        uint32_t *dst = o.cols + o.row_off[i] + pos;
+#pragma unroll
+        for (int k = 0; k < SPT; ++k)
+            if (flags & (1u << k)) *dst++ = v[k];
+        if (threadIdx.x == 0) o.row_nnz[i] = nnz;
+        __syncthreads();
+    }
+}
+
+// capacity = min(products, ncols): the exact upper bound of a row's count.
+__global__ void upper_bound_cap_kernel(const uint32_t *__restrict__ work, uint64_t n, uint64_t ncols,
+                                       uint32_t *__restrict__ cap) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t p = work[i];
+        cap[i] = (uint32_t)(p < ncols ? p : ncols);
+    }
+}
+
+// The overflowed rows of A as their own DCSR (A'), plus pos[i] = index of
+// row i in A' for overflowed rows.
+__global__ void gather_rows_lengths_kernel(const uint32_t *__restrict__ ovf, const uint64_t *__restrict__ arpt, uint64_t n,
+                                           uint32_t *__restrict__ len) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        len[i] = ovf[i] ? (uint32_t)(arpt[i + 1] - arpt[i]) : 0u;
+}
+
+__global__ void gather_rows_kernel(const uint32_t *__restrict__ ovf, const uint32_t *__restrict__ pos,
+                                   const uint64_t *__restrict__ dst_off, const uint64_t *__restrict__ arpt,
+                                   const uint32_t *__restrict__ arows, const uint32_t *__restrict__ acols, uint64_t n,
+                                   uint64_t *__restrict__ sub_rpt, uint32_t *__restrict__ sub_rows,
+                                   uint32_t *__restrict__ sub_cols, uint64_t sub_nzr, uint64_t sub_nnz) {
+    const uint32_t lane = lane_id();
+    const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); i < n; i += nw) {
+        if (!ovf[i]) continue;
+        const uint32_t k = pos[i];
+        const uint64_t s = arpt[i], e = arpt[i + 1], d = dst_off[i];
+        if (lane == 0) {
+            sub_rpt[k] = d;
+            sub_rows[k] = arows[i];
+        }
+        for (uint64_t j = s + lane; j < e; j += 32) sub_cols[d + (j - s)] = acols[j];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) sub_rpt[sub_nzr] = sub_nnz;
+}
+
+// Exact counts of the overflowed rows from the re-run product C'.
+__global__ void fallback_counts_kernel(const uint32_t *__restrict__ ovf, const uint32_t *__restrict__ pos,
+                                       const uint64_t *__restrict__ sub_crpt, uint64_t n, uint32_t *__restrict__ row_nnz) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (ovf[i]) row_nnz[i] = (uint32_t)(sub_crpt[pos[i] + 1] - sub_crpt[pos[i]]);
+}
+
+// C.cols <- every row from its slot (or from C' for overflowed rows).  One
+// warp per row, 4 independent 32-bit copies per lane in flight.
+__global__ void compact_rows_kernel(const uint32_t *__restrict__ row_nnz, const uint64_t *__restrict__ slot_off,
+                                    const uint64_t *__restrict__ off, const uint32_t *__restrict__ pre,
+                                    const uint32_t *__restrict__ ovf, const uint32_t *__restrict__ pos,
+                                    const uint64_t *__restrict__ sub_crpt, const uint32_t *__restrict__ sub_ccols,
+                                    uint64_t n, uint32_t *__restrict__ ccols) {
+    const uint32_t lane = lane_id();
+    const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); i < n; i += nw) {
+        const uint32_t len = row_nnz[i];
+        if (!len) continue;
+        const uint32_t *src = (ovf && ovf[i]) ? sub_ccols + sub_crpt[pos[i]] : pre + slot_off[i];
+        uint32_t *dst = ccols + off[i];
+        uint32_t t = lane;
+        for (; t + 96 < len; t += 128) {
+            const uint32_t x0 = __ldg(src + t), x1 = __ldg(src + t + 32), x2 = __ldg(src + t + 64),
+                           x3 = __ldg(src + t + 96);
+            dst[t] = x0;
+            dst[t + 32] = x1;
+            dst[t + 64] = x2;
+            dst[t + 96] = x3;
+        }
+        for (; t < len; t += 32) dst[t] = __ldg(src + t);
+    }
+}
+
+// Number of nonzero entries of a u32 array (the overflowed rows).
+__global__ void count_nonzero_kernel(const uint32_t *__restrict__ a, uint64_t n, unsigned long long *__restrict__ out) {
+    unsigned long long mine = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        mine += a[i] != 0;
+    mine = warp_sum(mine);
+    if (lane_id() == 0 && mine) atomicAdd(out, mine);
+}
+
+template <class K>
+int occupancy_of(K kernel, int nt) {
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, nt, 0) != cudaSuccess) {
+        cudaGetLastError();
+        blocks = 1;
+    }
+    return blocks > 0 ? blocks : 1;
+}
+
+template <int NP, int NT>
+int launch_cta_esc(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
+                   const uint32_t *work, uint64_t nmax, uint32_t *counter, const char *name) {
+    static int occ = occupancy_of(cta_esc_kernel<NP, NT>, NT);
+    unsigned grid = persistent_grid(ctl, occ, nmax);
+    ProfScope ps(ctl, name);
+    cta_esc_kernel<NP, NT><<<grid, NT, 0, ctl->stream>>>(bl, bin, a, b, o, work, counter);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+unsigned grid_for(const clb_controls *ctl, uint64_t n, int per_sm = 16) {
+    uint64_t g = (n + 255) / 256, cap = (uint64_t)ctl->sm_count * per_sm;
+    return (unsigned)(g > cap ? cap : (g ? g : 1));
+}
+
+}  // namespace
+
+// The accumulators of the ESC form for rows of up to 4096 products.
+int launch_esc_accumulators(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
+                            const uint32_t *work, uint64_t nmax) {
+    Temp<uint32_t> ctr;
+    CLB_RETURN_IF(ctr.alloc(ctl, 4));
+    CLB_TRY_CUDA(cudaMemsetAsync(ctr.ptr, 0, 4 * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_RETURN_IF((launch_cta_esc<4096, 512>(ctl, bl, BIN_H8K, a, b, o, work, nmax, ctr.ptr + 0, "cta_esc4096")));
+    CLB_RETURN_IF((launch_cta_esc<2048, 256>(ctl, bl, BIN_H4K, a, b, o, work, nmax, ctr.ptr + 1, "cta_esc2048")));
+    CLB_RETURN_IF((launch_cta_esc<1024, 256>(ctl, bl, BIN_H2K, a, b, o, work, nmax, ctr.ptr + 2, "cta_esc1024")));
+    CLB_RETURN_IF((launch_cta_esc<512, 128>(ctl, bl, BIN_H1K, a, b, o, work, nmax, ctr.ptr + 3, "cta_esc512")));
+    return CLB_SUCCESS;
+}
+
+// Single-pass driver.  `cap` (device, nzr_A entries) = capacity per A row; the
+// ESC form passes the upper bound, the learned form the predicted capacity.
+// `esc` selects the ESC accumulators for rows of <= 4096 products and bins
+// those rows by products; otherwise rows are binned by capacity and use the
+// hash accumulators.
+int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
+                       const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
+                       clb_spgemm_stats *st) {
+    const uint64_t n = A.nzr;
+    clb_dcsr C{};
+    C.nrows = A.nrows;
+    C.ncols = B.ncols;
+    Temp<uint32_t> list, info, flags, row_nnz, ovf, opos;
+    Temp<uint64_t> slot_off, off, scal;
+    CLB_RETURN_IF(list.alloc(ctl, n));
+    CLB_RETURN_IF(info.alloc(ctl, 2 * NUM_BINS));
+    CLB_RETURN_IF(flags.alloc(ctl, n));
+    CLB_RETURN_IF(row_nnz.alloc(ctl, n));
+    CLB_RETURN_IF(ovf.alloc(ctl, n));
+    CLB_RETURN_IF(slot_off.alloc(ctl, n));
+    CLB_RETURN_IF(off.alloc(ctl, n));
+    CLB_RETURN_IF(scal.alloc(ctl, 8));
+    CLB_TRY_CUDA(cudaMemsetAsync(scal.ptr, 0, 8 * sizeof(uint64_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(row_nnz.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(ovf.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+
+    // bins: ESC by products (CTA ESC up to 4096), learned by capacity
+    CLB_RETURN_IF(launch_binning(ctl, work, esc ? work : cap, n, B.ncols, info.ptr, list.ptr, flags.ptr));
+    CLB_RETURN_IF(scan_u32_inplace(ctl, flags.ptr, n, scal.ptr + 0));        // C row positions, nzr
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, cap, slot_off.ptr, n, scal.ptr + 1));  // slots, capacity
+    uint64_t h[2];
+    CLB_RETURN_IF(read_scalars(ctl, scal.ptr, h, 2));
+    const uint64_t nzr = h[0], capacity = h[1];
+    if (st) {
+        uint32_t hinfo[NUM_BINS];
+        CLB_TRY_CUDA(cudaMemcpy(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost), CLB_READ_BUFFER_ERROR);
+        for (int k = 0; k < NUM_BINS; ++k) st->rows_per_bin[k] = hinfo[k];
+        st->capacity = capacity;
+    }
+    Temp<uint32_t> pre;
+    CLB_RETURN_IF(pre.alloc(ctl, capacity ? capacity : 1));
+
+    BinLists bl{list.ptr, info.ptr};
+    RowOut num{row_nnz.ptr, slot_off.ptr, cap, ovf.ptr, pre.ptr, ctl->d_status};
+    if (esc) {
+        // warp ESC and bitmap rows through the shared launcher's bins; rows of
+        // the hash bins go to the CTA ESC kernels instead.
+        CLB_RETURN_IF(launch_esc_accumulators(ctl, bl, a, b, num, work, n));
+        CLB_RETURN_IF(launch_accumulators_subset(ctl, bl, a, b, num, B.ncols, n, /*hash_bins=*/false));
+    } else {
+        CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n));
+    }
+
+    // the fallback below resets the device status word: check it first
+    CLB_RETURN_IF(check_status(ctl, esc ? "matrix_multiplication" : "matrix_multiplication_learned"));
+    // rows that outgrew their capacity: re-run them with the exact two-pass form
+    unsigned long long *d_novf = (unsigned long long *)(scal.ptr + 2);
+    count_nonzero_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, n, d_novf);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    uint64_t novf = 0;
+    CLB_RETURN_IF(read_scalars(ctl, scal.ptr + 2, &novf, 1));
+    if (st) st->fallback_rows = novf;
+    clb_dcsr sub_c{};
+    Temp<uint64_t> sub_rpt, sub_off;
+    Temp<uint32_t> sub_rows, sub_cols, sub_len;
+    if (novf) {
+        CLB_RETURN_IF(opos.alloc(ctl, n));
+        CLB_RETURN_IF(sub_len.alloc(ctl, n));
+        CLB_RETURN_IF(sub_off.alloc(ctl, n));
+        CLB_TRY_CUDA(cudaMemcpyAsync(opos.ptr, ovf.ptr, n * 4, cudaMemcpyDeviceToDevice, ctl->stream),
+                     CLB_COPY_BUFFER_ERROR);
+        CLB_RETURN_IF(scan_u32_inplace(ctl, opos.ptr, n, scal.ptr + 3));
+        gather_rows_lengths_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, A.rpt, n, sub_len.ptr);
+        ctl->launches += 1;
+        CLB_CHECK_LAUNCH();
+        CLB_RETURN_IF(scan_u32_to_u64(ctl, sub_len.ptr, sub_off.ptr, n, scal.ptr + 4));
+        uint64_t sub_nnz = 0;
+        CLB_RETURN_IF(read_scalars(ctl, scal.ptr + 4, &sub_nnz, 1));
+        CLB_RETURN_IF(sub_rpt.alloc(ctl, novf + 1));
+        CLB_RETURN_IF(sub_rows.alloc(ctl, novf));
+        CLB_RETURN_IF(sub_cols.alloc(ctl, sub_nnz ? sub_nnz : 1));
+        gather_rows_kernel<<<grid_for(ctl, n * 32), 256, 0, ctl->stream>>>(ovf.ptr, opos.ptr, sub_off.ptr, A.rpt,
+                                                                           A.rows, A.cols, n, sub_rpt.ptr,
+                                                                           sub_rows.ptr, sub_cols.ptr, novf, sub_nnz);
+        ctl->launches += 1;
+        CLB_CHECK_LAUNCH();
+        clb_dcsr subA{A.nrows, A.ncols, sub_nnz, novf, sub_rpt.ptr, sub_rows.ptr, sub_cols.ptr};
+        const uint32_t launches = ctl->launches;
+        CLB_RETURN_IF(spgemm_hash_two_pass(ctl, subA, B, &sub_c, nullptr));
+        ctl->launches += launches;
+        if (sub_c.nzr != novf) {
+            clb_dcsr_release(ctl, &sub_c);
+            return fail(CLB_RUN_KERNEL_FAILURE, "fallback rows lost their products");
+        }
+        fallback_counts_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, opos.ptr, sub_c.rpt, n,
+                                                                           row_nnz.ptr);
+        ctl->launches += 1;
+        CLB_CHECK_LAUNCH();
+    }
+
+    // final layout
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, row_nnz.ptr, off.ptr, n, scal.ptr + 5));
+    uint64_t nnz = 0;
+    CLB_RETURN_IF(read_scalars(ctl, scal.ptr + 5, &nnz, 1));
+    int rc = CLB_SUCCESS;
+    Temp<uint64_t> c_rpt;
+    Temp<uint32_t> c_rows, c_cols;
+    if (nnz) {
+        rc = c_rpt.alloc(ctl, nzr + 1);
+        if (rc == CLB_SUCCESS) rc = c_rows.alloc(ctl, nzr);
+        if (rc == CLB_SUCCESS) rc = c_cols.alloc(ctl, nnz);
+        if (rc == CLB_SUCCESS)
+            rc = launch_assemble(ctl, work, flags.ptr, off.ptr, A.rows, n, c_rpt.ptr, c_rows.ptr, nzr, nnz);
+        if (rc == CLB_SUCCESS) {
+            ProfScope ps(ctl, "compact");
+            compact_rows_kernel<<<grid_for(ctl, n * 32, 32), 256, 0, ctl->stream>>>(
+                row_nnz.ptr, slot_off.ptr, off.ptr, pre.ptr, novf ? ovf.ptr : nullptr, opos.ptr, sub_c.rpt,
+                sub_c.cols, n, c_cols.ptr);
+            ctl->launches += 1;
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) rc = fail(CLB_RUN_KERNEL_FAILURE, cudaGetErrorString(e));
+        }
+    }
+    if (rc == CLB_SUCCESS) rc = check_status(ctl, esc ? "matrix_multiplication" : "matrix_multiplication_learned");
+    if (sub_c.rpt) clb_dcsr_release(ctl, &sub_c);
+    if (rc != CLB_SUCCESS) return rc;
+    if (nnz) {
+        C.nnz = nnz;
+        C.nzr = nzr;
+        C.rpt = c_rpt.release_ownership();
+        C.rows = c_rows.release_ownership();
+        C.cols = c_cols.release_ownership();
+    }
+    if (st) {
+        st->products = products;
+        st->nnz = nnz;
+        st->nzr = C.nzr;
+    }
+    *out = C;
+    return CLB_SUCCESS;
+}
+
+}  // namespace clb
+
+using namespace clb;
+
+extern "C" {
+
+int clb_dcsr_spgemm_esc(clb_controls *ctl, const clb_dcsr *a_, const clb_dcsr *b_, clb_dcsr *c,
+                        clb_spgemm_stats *stats) {
+    if (!ctl || !a_ || !b_ || !c) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    const clb_dcsr A = *a_, B = *b_;
+    CLB_RETURN_IF(validate_spgemm(A, B));
+    DeviceGuard g(ctl);
+    clb_spgemm_stats st{};
+    ctl->launches = 0;
+    if (A.nnz == 0 || B.nnz == 0 || A.nzr == 0 || B.nzr == 0) {
+        clb_dcsr C{};
+        C.nrows = A.nrows;
+        C.ncols = B.ncols;
+        *c = C;
+        if (stats) *stats = st;
+        return CLB_SUCCESS;
+    }
+    CLB_RETURN_IF(clear_status(ctl));
+    const AView a{A.rpt, A.rows, A.cols, A.nzr};
+    BRows b;
+    Temp<uint64_t> dense, tot;
+    CLB_RETURN_IF(prepare_b(ctl, B, dense, b));
+    Temp<uint32_t> work, cap;
+    CLB_RETURN_IF(work.alloc(ctl, A.nzr));
+    CLB_RETURN_IF(cap.alloc(ctl, A.nzr));
+    CLB_RETURN_IF(tot.alloc(ctl, 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(tot.ptr, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, tot.ptr));
+    upper_bound_cap_kernel<<<grid_for(ctl, A.nzr), 256, 0, ctl->stream>>>(work.ptr, A.nzr, B.ncols, cap.ptr);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    uint64_t products = 0;
+    CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &products, 1));
+    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st);
+    st.kernel_launches = ctl->launches;
+    if (stats) *stats = st;
+    return rc;
+}
+
+}  // extern "C"

@@ -1,4 +1,6 @@
-"""clbool::dcsr namespace (src/dcsr/dcsr.hpp)."""
+"""clbool::dcsr namespace (src/dcsr/dcsr.hpp), plus the learned single-pass form."""
 from .ops import kronecker_product, matrix_multiplication, matrix_multiplication_hash, transpose, workload
+from .sizing import RowSizer, matrix_multiplication_learned, row_features, row_nnz
 
-__all__ = ["matrix_multiplication_hash", "matrix_multiplication", "kronecker_product", "transpose", "workload"]
+__all__ = ["matrix_multiplication_hash", "matrix_multiplication", "kronecker_product", "transpose", "workload",
+           "matrix_multiplication_learned", "RowSizer", "row_features", "row_nnz"]

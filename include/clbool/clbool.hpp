@@ -365,6 +365,13 @@ inline void matrix_multiplication_hash(Controls &c, matrix_dcsr &matrix_out, con
     matrix_out = matrix_dcsr::adopt(c, out);
 }
 
+inline void matrix_multiplication(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &a, const matrix_dcsr &b,
+                                  clb_spgemm_stats *stats = nullptr) {
+    clb_dcsr va = a.view(), vb = b.view(), out{};
+    details::check(clb_dcsr_spgemm_esc(c.get(), &va, &vb, &out, stats));
+    matrix_out = matrix_dcsr::adopt(c, out);
+}
+
 inline void kronecker_product(Controls &c, matrix_dcsr &matrix_c, const matrix_dcsr &matrix_a,
                               const matrix_dcsr &matrix_b) {
     clb_dcsr va = matrix_a.view(), vb = matrix_b.view(), out{};

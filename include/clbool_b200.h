@@ -216,6 +216,45 @@ CLB_API int clb_dcsr_kronecker(clb_controls *ctl, const clb_dcsr *a, const clb_d
 /* dcsr::transpose (src/dcsr/dcsr.hpp:17-19, dcsr_transpose.cpp:5-16). */
 CLB_API int clb_dcsr_transpose(clb_controls *ctl, const clb_dcsr *in, clb_dcsr *out);
 
+/* dcsr::matrix_multiplication (src/dcsr/dcsr.hpp:27-30,
+ * dcsr_matrix_multiplication.cpp:26-97): the ESC/merge form -- every row gets
+ * its upper bound of slots, one expand-sort-compress (or bitmap) pass fills
+ * them, and the rows are compacted into C. Same result as the hash form. */
+CLB_API int clb_dcsr_spgemm_esc(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
+                                clb_spgemm_stats *stats);
+
+/* ------------------------------------------------------ learned sizing -- */
+/* Not in the reference.  A row-size predictor (MLP 6 -> 64 -> 64 -> 1, ReLU,
+ * BF16 weights, FP32 accumulation) estimates log2(1 + nnz) of every row of
+ * C = A*B from six features of its A row; clb_dcsr_spgemm_learned gives each
+ * row that many output slots (times 2^margin_log2, plus slack, never above
+ * the exact bound min(products, ncols)), runs ONE numeric pass, and re-runs
+ * the rows that overflow with the exact two-pass form, so C is always exact. */
+typedef struct clb_sizer clb_sizer;
+CLB_API int clb_sizer_num_params(void);
+CLB_API int clb_sizer_create(clb_controls *ctl, uint64_t seed, clb_sizer **out);
+CLB_API int clb_sizer_destroy(clb_sizer *sizer);
+/* FP32 master weights (checkpoint): `count` must be clb_sizer_num_params(). */
+CLB_API int clb_sizer_get_params(clb_sizer *sizer, float *host, size_t count);
+CLB_API int clb_sizer_set_params(clb_sizer *sizer, const float *host, size_t count);
+/* Device arrays: features[6 * a->nzr] (scaled log2 features) and, when not
+ * NULL, workload[a->nzr] (products per A row). */
+CLB_API int clb_dcsr_row_features(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, float *features,
+                                  uint32_t *workload);
+/* Exact nnz of every C row (the symbolic pass alone), device u32[a->nzr]. */
+CLB_API int clb_dcsr_row_nnz(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, uint32_t *row_nnz);
+/* Predictions (scaled log2(1 + nnz)) of n rows; device arrays. */
+CLB_API int clb_sizer_predict(clb_sizer *sizer, const float *features, uint64_t n, float *out);
+/* Mean-squared-error loss and its gradient w.r.t. the BF16-rounded weights
+ * over n rows (device features/targets; host grads of num_params floats). */
+CLB_API int clb_sizer_gradients(clb_sizer *sizer, const float *features, const float *targets, uint64_t n,
+                                float *grads_host, float *loss_host);
+/* Adam training over n rows (device arrays; targets = log2(1 + nnz) / 16). */
+CLB_API int clb_sizer_train(clb_sizer *sizer, const float *features, const float *targets, uint64_t n,
+                            uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float *final_loss);
+CLB_API int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_sizer *sizer,
+                                    float margin_log2, float slack, clb_dcsr *c, clb_spgemm_stats *stats);
+
 /* Products per A row (count_workload, dcsr_matrix_multiplication.cpp:388-404):
  * workload has a->nzr entries in device memory; *total = their sum. */
 CLB_API int clb_dcsr_workload(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, uint32_t *workload,

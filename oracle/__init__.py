@@ -102,6 +102,10 @@ def lib():
         L.orc_csr_add.restype = C.c_uint64
         L.orc_kronecker.argtypes = [C.POINTER(_OrcDcsr), C.POINTER(_OrcDcsr), C.POINTER(_OrcDcsr)]
         L.orc_transpose.argtypes = [C.POINTER(_OrcDcsr), C.POINTER(_OrcDcsr)]
+        L.orc_mlp_num_params.restype = C.c_int
+        f32p = C.POINTER(C.c_float)
+        f64p = C.POINTER(C.c_double)
+        L.orc_mlp_grad.argtypes = [f32p, f32p, f32p, C.c_uint64, f64p, f64p, f64p]
         _lib = L
     return _lib
 
@@ -311,6 +315,58 @@ def transpose(a: Dcsr) -> Dcsr:
     sc = _OrcDcsr()
     lib().orc_transpose(C.byref(sa), C.byref(sc))
     return _from_orc(sc)
+
+
+def row_features(a: Dcsr, b: Dcsr) -> np.ndarray:
+    """Six features of every A row of A*B (float64, shape [nzr_A, 6]), the
+    inputs of the row-size predictor: log2(1+|A_i|), log2(1+P_i),
+    log2(1+max |B_k|), log2(1+min nonzero |B_k|) -- k over the columns of A_i,
+    all divided by 16 -- then A.rows[i] / A.nrows and
+    log2(B.nrows * B.ncols / nnz(B)) / 16.  Not in the reference."""
+    nzr = len(a.rows) if len(a.cols) else 0
+    out = np.zeros((nzr, 6), np.float64)
+    if nzr == 0:
+        return out
+    blen = np.zeros(max(int(a.ncols), 1), np.int64)
+    if len(b.cols):
+        brpt = np.asarray(b.rpt, np.int64)
+        keep = np.asarray(b.rows, np.int64) < blen.size
+        blen[np.asarray(b.rows, np.int64)[keep]] = np.diff(brpt)[keep]
+    arpt = np.asarray(a.rpt, np.int64)
+    lens = blen[np.asarray(a.cols, np.int64)]
+    seg = np.repeat(np.arange(nzr), np.diff(arpt))
+    P = np.bincount(seg, weights=lens, minlength=nzr)
+    mx = np.zeros(nzr)
+    np.maximum.at(mx, seg, lens)
+    mn = np.full(nzr, np.inf)
+    nzl = lens > 0
+    np.minimum.at(mn, seg[nzl], lens[nzl])
+    mn[np.isinf(mn)] = 0
+    out[:, 0] = np.log2(1.0 + np.diff(arpt)) / 16
+    out[:, 1] = np.log2(1.0 + P) / 16
+    out[:, 2] = np.log2(1.0 + mx) / 16
+    out[:, 3] = np.log2(1.0 + mn) / 16
+    out[:, 4] = np.asarray(a.rows, np.float64) / float(a.nrows) if a.nrows else 0.0
+    nnzb = len(b.cols)
+    out[:, 5] = np.log2(float(b.nrows) * float(b.ncols) / nnzb) / 16 if nnzb else 0.0
+    return out
+
+
+def mlp_grad(params, features, targets):
+    """FP64 loss, gradient and predictions of the row-size predictor
+    (6 -> 64 -> 64 -> 1, ReLU, BF16-rounded weights, MSE)."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1)
+    t = np.ascontiguousarray(targets, dtype=np.float32)
+    n = t.size
+    g = np.zeros(lib().orc_mlp_num_params(), np.float64)
+    pr = np.zeros(max(n, 1), np.float64)
+    loss = C.c_double()
+    f32p = C.POINTER(C.c_float)
+    f64p = C.POINTER(C.c_double)
+    lib().orc_mlp_grad(p.ctypes.data_as(f32p), f.ctypes.data_as(f32p), t.ctypes.data_as(f32p), n,
+                       g.ctypes.data_as(f64p), C.byref(loss), pr.ctypes.data_as(f64p))
+    return float(loss.value), g, pr[:n]
 
 
 # ------------------------------------------------------- reference library

@@ -568,3 +568,75 @@ void orc_transpose(const orc_dcsr *a, orc_dcsr *c) {
     c->cols = cc;
     free(r);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Row-size predictor (learned sizing of the single-pass SpGEMM): FP64       */
+/* reference of the network the CUDA kernels train, used to check their      */
+/* gradients.  Architecture: 6 -> 64 -> 64 -> 1, ReLU; weights used as BF16  */
+/* (round to nearest even of the FP32 masters); loss = mean squared error.   */
+/* Parameter layout: W1[64][6], b1[64], W2[64][64], b2[64], w3[64], b3.      */
+/* ------------------------------------------------------------------------ */
+#define MLP_F 6
+#define MLP_H 64
+#define MLP_NP (MLP_H * MLP_F + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H + 1)
+
+static double bf16_round(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7F800000u) != 0x7F800000u) u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    else u &= 0xFFFF0000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return (double)r;
+}
+
+int orc_mlp_num_params(void) { return MLP_NP; }
+
+/* Loss and gradient over n rows; grads (MLP_NP doubles) w.r.t. the rounded
+ * weights.  preds (n doubles) may be NULL. */
+void orc_mlp_grad(const float *params, const float *feat, const float *target, uint64_t n, double *grads,
+                  double *loss, double *preds) {
+    double w[MLP_NP];
+    for (int k = 0; k < MLP_NP; ++k) w[k] = bf16_round(params[k]);
+    const double *W1 = w, *b1 = W1 + MLP_H * MLP_F, *W2 = b1 + MLP_H, *b2 = W2 + MLP_H * MLP_H, *w3 = b2 + MLP_H,
+                 *b3 = w3 + MLP_H;
+    memset(grads, 0, sizeof(double) * MLP_NP);
+    double *gW1 = grads, *gb1 = gW1 + MLP_H * MLP_F, *gW2 = gb1 + MLP_H, *gb2 = gW2 + MLP_H * MLP_H,
+           *gw3 = gb2 + MLP_H, *gb3 = gw3 + MLP_H;
+    double L = 0;
+    for (uint64_t r = 0; r < n; ++r) {
+        const float *x = feat + r * MLP_F;
+        double h1[MLP_H], h2[MLP_H], y = *b3;
+        for (int j = 0; j < MLP_H; ++j) {
+            double a = b1[j];
+            for (int f = 0; f < MLP_F; ++f) a += W1[j * MLP_F + f] * x[f];
+            h1[j] = a > 0 ? a : 0;
+        }
+        for (int j = 0; j < MLP_H; ++j) {
+            double a = b2[j];
+            for (int k = 0; k < MLP_H; ++k) a += W2[j * MLP_H + k] * h1[k];
+            h2[j] = a > 0 ? a : 0;
+            y += w3[j] * h2[j];
+        }
+        if (preds) preds[r] = y;
+        const double e = y - target[r];
+        L += e * e / (double)n;
+        const double dy = 2.0 * e / (double)n;
+        double g2[MLP_H], g1[MLP_H];
+        *gb3 += dy;
+        for (int j = 0; j < MLP_H; ++j) {
+            gw3[j] += dy * h2[j];
+            g2[j] = h2[j] > 0 ? dy * w3[j] : 0;
+            gb2[j] += g2[j];
+            for (int k = 0; k < MLP_H; ++k) gW2[j * MLP_H + k] += g2[j] * h1[k];
+        }
+        for (int k = 0; k < MLP_H; ++k) {
+            double a = 0;
+            for (int j = 0; j < MLP_H; ++j) a += W2[j * MLP_H + k] * g2[j];
+            g1[k] = h1[k] > 0 ? a : 0;
+            gb1[k] += g1[k];
+            for (int f = 0; f < MLP_F; ++f) gW1[k * MLP_F + f] += g1[k] * x[f];
+        }
+    }
+    *loss = L;
+}
