@@ -245,9 +245,15 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     A_full = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(rpt, rows, cols), n)
     work_buf, total_products = cb.dcsr.workload(ctl, A_full, A_full)
     work = work_buf.to_host(rows.size).astype(np.int64)
+    # left operand: A itself, or (for profiling) a seeded sample of its rows
+    lrpt, lrows, lcols = rpt, rows, cols
+    if args.row_fraction < 1.0:
+        pick = _row_sample(rows.size, args.row_fraction, seed=3)
+        lrpt, lrows, lcols = _sub_dcsr(rpt, rows, cols, pick)
+        work = work[pick]
     lo, hi = shard_rows(work, world, rank)
-    srpt = (rpt[lo:hi + 1] - rpt[lo]).astype(np.uint64)
-    srows, scols = rows[lo:hi], cols[int(rpt[lo]):int(rpt[hi])]
+    srpt = (lrpt[lo:hi + 1] - lrpt[lo]).astype(np.uint64)
+    srows, scols = lrows[lo:hi], lcols[int(lrpt[lo]):int(lrpt[hi])]
     A = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(srpt, srows, scols), n) if hi > lo else \
         cb.matrix_dcsr.zeros(n, n)
     my_products = int(work[lo:hi].sum())
@@ -321,7 +327,9 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic", "impl": "ours",
-        "config": {"workload": f"rmat_s{args.scale}_AxA_{args.form}", "scale": args.scale, "edge_factor": 16,
+        "config": {"workload": f"rmat_s{args.scale}_AxA_{args.form}" + (
+                       f"_rows{args.row_fraction:g}" if args.row_fraction < 1.0 else ""),
+                   "scale": args.scale, "edge_factor": 16,
                    "abcd": [0.57, 0.19, 0.19, 0.05], "nnz_A": int(nnz_a), "products": int(products_all),
                    "nnz_C": int(nnz_all), "form": args.form, "parallelism": f"rows{world}",
                    "l2": "256 MiB device memset between steps, outside the step events; C (>30 GB) also exceeds L2"},
@@ -500,6 +508,8 @@ def main():
     ap.add_argument("--sizer", default=os.path.join(ROOT, "clbool_b200", "sizer_rmat.npz"),
                     help="predictor checkpoint of the learned form")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the two-pass form beside it")
+    ap.add_argument("--row-fraction", type=float, default=1.0,
+                    help="left operand = this seeded fraction of A's stored rows (profiling captures)")
     ap.add_argument("--ref-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

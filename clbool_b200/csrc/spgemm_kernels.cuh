@@ -414,21 +414,28 @@ __global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AVie
 // ----------------------------------------------------------- CTA bitmap ----
 constexpr int BMP_NT = 1024;
 constexpr int BMP_NW = BMP_NT / 32;
-constexpr int BMP_ECH = 2048;
-constexpr uint32_t BMP_MAX_WORDS = 32768;  // 128 KB: 2^20 columns per chunk
-constexpr uint32_t BMP_UNIT = 4u * 32u * BMP_NW;  // words per emission sweep (4 per lane)
+constexpr int BMP_ECH = 1024;                 // A entries staged per chunk
+constexpr uint32_t BMP_MAX_WORDS = 32768;     // 128 KB: 2^20 columns per chunk
+constexpr int BMP_U = 8;                      // B-column loads in flight per lane
+constexpr uint32_t BMP_STEP_WORDS = 128;      // emission step: 4 words per lane
+constexpr uint32_t BMP_MAX_STEPS = BMP_MAX_WORDS / BMP_STEP_WORDS;
+constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (columns)
 
-// Words of the bitmap for `ncols` columns: a multiple of BMP_UNIT so the
-// warps split it evenly in 4-word lane steps, at most BMP_MAX_WORDS.
+// Words of the bitmap for `ncols` columns: a multiple of the emission step,
+// at most BMP_MAX_WORDS.
 inline uint32_t bitmap_words(uint64_t ncols) {
     uint64_t w = (ncols + 31) / 32;
-    w = (w + BMP_UNIT - 1) / BMP_UNIT * BMP_UNIT;
+    w = (w + BMP_STEP_WORDS - 1) / BMP_STEP_WORDS * BMP_STEP_WORDS;
     if (w > BMP_MAX_WORDS) w = BMP_MAX_WORDS;
     return (uint32_t)w;
 }
 
-// Dynamic shared memory of the bitmap kernel: W words + the entry stage.
-inline size_t bitmap_smem_bytes(uint32_t W) { return ((size_t)W + 2 * BMP_ECH + 4 + BMP_NT + 4) * 4; }
+// Dynamic shared memory of the bitmap kernel (32-bit words): bitmap W |
+// entry stage (B row start, length, unit prefix) | non-empty step list and
+// output offsets | per-warp output staging.
+inline size_t bitmap_smem_bytes(uint32_t W) {
+    return ((size_t)W + 3 * BMP_ECH + 1 + 2 * BMP_MAX_STEPS + 1 + BMP_NW * BMP_STAGE) * 4;
+}
 
 // Position of the n-th (0-based) set bit of w; w has more than n set bits.
 __device__ __forceinline__ uint32_t nth_set_bit(uint32_t w, uint32_t n) {
@@ -446,84 +453,147 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t w, uint32_t n) {
     return pos;
 }
 
-// One warp-uniform step of bitmap insertion: lane sets bit `r` (if `in`).
-// Lanes reading one B row hold ascending columns, so lanes that hit the same
-// word form contiguous runs (heads = first lane of each run).  All branches
-// below are warp-uniform:
-//   * every lane its own run  -> one atomic per lane;
-//   * at most 4 distinct words (dense hub rows) -> a full-warp OR reduction
-//     per word and one atomic per word;
-//   * otherwise a shuffle segmented OR and one atomic per run.
-__device__ __forceinline__ void bitmap_set(uint32_t *bm, uint32_t r, bool in) {
-    const uint32_t lane = lane_id();
-    const uint32_t wd = in ? (r >> 5) : 0xFFFFFFFFu;
-    uint32_t bit = in ? (1u << (r & 31)) : 0u;
-    const uint32_t upw = __shfl_up_sync(0xFFFFFFFFu, wd, 1);
-    const bool head = lane == 0 || upw != wd;
-    const uint32_t heads = __ballot_sync(0xFFFFFFFFu, head);
-    if (heads == 0xFFFFFFFFu) {
-        if (in) atomicOr(bm + wd, bit);
-        return;
-    }
-    if (__popc(heads) <= 4) {
-        uint32_t hm = heads;
-        while (hm) {
-            const int h = __ffs(hm) - 1;
-            hm &= hm - 1;
-            const uint32_t ww = __shfl_sync(0xFFFFFFFFu, wd, h);
-            const uint32_t x = __reduce_or_sync(0xFFFFFFFFu, wd == ww ? bit : 0u);
-            if ((int)lane == h && ww != 0xFFFFFFFFu) atomicOr(bm + ww, x);
-        }
-        return;
-    }
+// Products of A row i in units of up to 2^shift products that read ONE B
+// row: warp w takes units w, w + NW, ... of each staged chunk of ECH A
+// entries, and its lanes read the unit's B columns with stride 32 (coalesced,
+// BMP_U loads in flight per lane), calling f(col, valid) warp-uniformly for
+// every 32 consecutive positions.  No per-product search: the entry of a
+// unit is found once by a warp-wide ballot over the unit prefix (the warp's
+// cursor only moves forward).  Chunk stage: s_beg = B row start, s_len = B
+// row length, s_upre = exclusive prefix of units.  Requires B.nnz < 2^32.
+template <int NT, int ECH, class F>
+__device__ __forceinline__ void unit_products(const AView &a, const BRows &b, uint32_t i, uint32_t shift,
+                                              uint32_t *s_beg, uint32_t *s_len, uint32_t *s_upre, uint32_t *scratch,
+                                              F &&f) {
+    static_assert(ECH % NT == 0, "entry chunk must be a multiple of the block");
+    constexpr int EPT = ECH / NT;
+    constexpr int NW = NT / 32;
+    const uint32_t unit = 1u << shift;
+    const uint32_t lane = lane_id(), w = warp_id();
+    const uint64_t ja = a.rpt[i], je = a.rpt[i + 1];
+    for (uint64_t c0 = ja; c0 < je; c0 += ECH) {
+        const uint32_t n = (uint32_t)min((uint64_t)ECH, je - c0);
+        uint32_t units[EPT], sum = 0;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t ob = __shfl_down_sync(0xFFFFFFFFu, bit, d);
-        const uint32_t ow = __shfl_down_sync(0xFFFFFFFFu, wd, d);
-        if (lane + d < 32 && ow == wd) bit |= ob;
+        for (int k = 0; k < EPT; ++k) {
+            const uint32_t e = threadIdx.x * EPT + k;
+            uint32_t len = 0;
+            if (e < n) {
+                uint64_t bb;
+                len = b_row(b, __ldg(a.cols + c0 + e), bb);
+                s_beg[e] = (uint32_t)bb;
+                s_len[e] = len;
+            }
+            units[k] = (len + unit - 1) >> shift;
+            sum += units[k];
+        }
+        uint32_t total;
+        uint32_t run = block_exclusive_scan<uint32_t, NT>(sum, scratch, &total);
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const uint32_t e = threadIdx.x * EPT + k;
+            if (e < n) s_upre[e] = run;
+            run += units[k];
+        }
+        if (threadIdx.x == 0) s_upre[n] = total;
+        __syncthreads();
+        uint32_t e = 0;  // warp-uniform entry cursor
+        for (uint32_t u = w; u < total; u += NW) {
+            // largest e with s_upre[e] <= u: s_upre is non-decreasing and
+            // s_upre[n] = total > u, so the lanes that pass form a prefix
+            for (;;) {
+                const uint32_t idx = e + 1 + lane;
+                const bool le = idx <= n && s_upre[idx] <= u;
+                const uint32_t m = __ballot_sync(0xFFFFFFFFu, le);
+                e += __popc(m);
+                if (m != 0xFFFFFFFFu) break;
+            }
+            const uint32_t first = (u - s_upre[e]) << shift;
+            const uint32_t cnt = min(unit, s_len[e] - first);
+            const uint32_t *src = b.cols + s_beg[e] + first;
+#pragma unroll 1
+            for (uint32_t k0 = 0; k0 < cnt; k0 += 32u * BMP_U) {
+                uint32_t col[BMP_U];
+#pragma unroll
+                for (int s = 0; s < BMP_U; ++s) {
+                    const uint32_t q = k0 + (uint32_t)s * 32u + lane;
+                    col[s] = q < cnt ? __ldg(src + q) : 0u;
+                }
+#pragma unroll
+                for (int s = 0; s < BMP_U; ++s) {
+                    if (k0 + (uint32_t)s * 32u < cnt)  // warp-uniform
+                        f(col[s], k0 + (uint32_t)s * 32u + lane < cnt);
+                }
+            }
+        }
+        __syncthreads();
     }
-    if (in && head) atomicOr(bm + wd, bit);
 }
 
 // Rows of bins [bin_lo, bin_hi] (contiguous in the list, heaviest first),
 // one row per CTA at a time, taken from `counter`.  MULTI: the columns do
 // not fit one bitmap chunk, so every chunk re-walks the row's products.
+// Insertion units: 512 products for rows over 2^17 products, 256 below (so
+// the 32 warps of a lighter row still get several units each).  Plain
+// shared atomics: B rows are mostly sparse over 2^20 columns, and warp-level
+// aggregation of same-word bits cost more instructions than the conflicts
+// it saved (measured on R-MAT scale 20).
+//
+// Emission of a chunk, in steps of 128 words (4096 columns): groups of four
+// threads count one step; one block scan of (count << 11 | nonempty) gives
+// every non-empty step a slot in a compact list and its output offset.
+// Warps take list entries dynamically.  For a step, lane l holds words
+// 4l..4l+3 and a warp scan of their counts places them; the step's outputs
+// are then produced in windows of up to BMP_STAGE: the window's outputs are
+// split evenly over the lanes, each lane finds the word and bit of its first
+// output (shuffle search over the scan, then nth_set_bit) and walks the
+// bitmap from there, writing into the warp's staging buffer, which the warp
+// copies to C with coalesced stores.  Cost follows the non-empty steps and
+// the output, not the bitmap width, and is even across lanes.
 template <bool NUMERIC, bool MULTI>
 __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int bin_lo, int bin_hi, AView a, BRows b,
                                                                RowOut o, uint64_t ncols, uint32_t W,
                                                                uint32_t *counter) {
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t *bm = smem;
-    uint32_t *s_pre = smem + W;
-    uint32_t *s_beg = s_pre + BMP_ECH + 4;
-    uint32_t *soff = s_beg + BMP_ECH;  // step output offsets (<= BMP_NT + 1)
+    uint32_t *s_beg = smem + W;
+    uint32_t *s_len = s_beg + BMP_ECH;
+    uint32_t *s_upre = s_len + BMP_ECH;             // BMP_ECH + 1
+    uint32_t *s_list = s_upre + BMP_ECH + 1;        // BMP_MAX_STEPS
+    uint32_t *s_soff = s_list + BMP_MAX_STEPS;      // BMP_MAX_STEPS + 1
+    uint32_t *s_stage = s_soff + BMP_MAX_STEPS + 1; // BMP_NW * BMP_STAGE
     __shared__ uint32_t scratch[33];
     __shared__ uint32_t s_slot, s_next;
     uint32_t beg, cnt = 0, tmp;
     bin_range(bl, bin_lo, beg, tmp);
     for (int q = bin_lo; q <= bin_hi; ++q) cnt += bl.info[q];
+    // rows of the bins above BIN_BMP (over 2^17 products) come first
+    const uint32_t nheavy = bin_hi > bin_lo ? cnt - bl.info[bin_hi] : 0;
     for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) bm[w] = 0;
     __syncthreads();
     const uint32_t lane = lane_id(), wi = warp_id();
     const uint64_t chunk_cols = (uint64_t)W * 32;
+    const uint32_t nwg = W >> 5;  // 32-word groups, one per counting thread (<= BMP_NT)
     uint4 *bm4 = reinterpret_cast<uint4 *>(bm);
+    uint32_t *const stage = s_stage + wi * BMP_STAGE;
     for (;;) {
         const uint32_t item = next_item(counter, &s_slot);
         if (item >= cnt) break;
         const uint32_t i = bl.list[beg + item];
+        const uint32_t shift = item < nheavy ? 9u : 8u;
         uint64_t total = 0;
         const uint64_t out_base = NUMERIC ? o.row_off[i] : 0;
         bool overflowed = false;
         for (uint64_t c0 = 0; c0 < (MULTI ? ncols : 1); c0 += chunk_cols) {
             if (MULTI) {
-                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t) {
-                    // unsigned wrap sends columns below c0 out of range too
-                    const uint64_t r = (uint64_t)c - c0;
-                    const bool in = valid && r < chunk_cols;
-                    bitmap_set(bm, (uint32_t)r, in);
+                unit_products<BMP_NT, BMP_ECH>(a, b, i, shift, s_beg, s_len, s_upre, scratch,
+                                               [&](uint32_t c, bool valid) {
+                    const uint64_t r = (uint64_t)c - c0;  // wraps for columns below c0
+                    if (valid && r < chunk_cols) atomicOr(bm + (r >> 5), 1u << (r & 31));
                 });
             } else {
-                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t) {
+                unit_products<BMP_NT, BMP_ECH>(a, b, i, shift, s_beg, s_len, s_upre, scratch,
+                                               [&](uint32_t c, bool valid) {
                     if (valid && c < (uint32_t)chunk_cols) atomicOr(bm + (c >> 5), 1u << (c & 31));
                 });
             }
@@ -537,31 +607,33 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
                 total += block_sum<uint32_t, BMP_NT>(mine, scratch);
                 continue;
             }
-            // Emission, balanced by output: thread t counts 32-word step t,
-            // a block scan gives every step's output offset, and warp w takes
-            // the steps whose first output lies in the w-th 1/32 of the row's
-            // outputs (R-MAT columns are skewed: equal word ranges would give
-            // one warp most of the output).  Empty steps are skipped.
-            const uint32_t nsteps = W >> 5;
-            uint32_t scnt = 0;
-            if (threadIdx.x < nsteps) {
+            uint32_t c32 = 0;
+            if (threadIdx.x < nwg) {
                 const uint4 *p4 = bm4 + threadIdx.x * 8;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const uint4 x = p4[k];
-                    scnt += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+                    c32 += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
                 }
             }
-            uint32_t ctot;
-            const uint32_t ex = block_exclusive_scan<uint32_t, BMP_NT>(scnt, scratch, &ctot);
-            if (threadIdx.x < nsteps) soff[threadIdx.x] = ex;
+            uint32_t scnt = c32 + __shfl_xor_sync(0xFFFFFFFFu, c32, 1);
+            scnt += __shfl_xor_sync(0xFFFFFFFFu, scnt, 2);
+            if ((threadIdx.x & 3u) != 0) scnt = 0;  // thread 4s holds step s
+            // counts <= 4096 per step, <= 2^20 per chunk; flags <= 256 < 2^11
+            uint32_t ptot;
+            const uint32_t ex = block_exclusive_scan<uint32_t, BMP_NT>((scnt << 11) | (scnt ? 1u : 0u), scratch, &ptot);
+            const uint32_t ctot = ptot >> 11, nlist = ptot & 0x7FFu;
+            if (scnt) {
+                s_list[ex & 0x7FFu] = threadIdx.x >> 2;
+                s_soff[ex & 0x7FFu] = ex >> 11;
+            }
             if (threadIdx.x == 0) {
-                soff[nsteps] = ctot;
+                s_soff[nlist] = ctot;
                 s_next = 0;
             }
             __syncthreads();
             if (o.row_cap && total + ctot > o.row_cap[i]) {
-                // learned form: the row does not fit its slot; clear the
+                // single-pass forms: the row does not fit its slot; clear the
                 // bitmap and flag the row.
                 overflowed = true;
                 for (uint32_t w4 = threadIdx.x; w4 < W / 4; w4 += BMP_NT) bm4[w4] = make_uint4(0, 0, 0, 0);
@@ -570,38 +642,56 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
                 continue;
             }
             uint32_t *const out = o.cols + out_base + total;
-            // Steps are taken dynamically (two per grab): the cost of a step
-            // follows its non-empty words, which no static split predicts.
             for (;;) {
                 uint32_t g = 0;
-                if (lane == 0) g = atomicAdd(&s_next, 2u);
+                if (lane == 0) g = atomicAdd(&s_next, 1u);
                 g = __shfl_sync(0xFFFFFFFFu, g, 0);
-                if (g >= nsteps) break;
-                for (uint32_t st = g; st < g + 2 && st < nsteps; ++st) {
-                const uint32_t pos = soff[st];
-                const uint32_t T = soff[st + 1] - pos;
-                if (T == 0) continue;  // empty step (warp-uniform)
-                const uint32_t word = bm[st * 32 + lane];
-                if (word) bm[st * 32 + lane] = 0;
-                // Output k of the step is written by lane k % 32 (coalesced):
-                // its source word is the first lane whose inclusive count
-                // exceeds k, its column the matching set bit of that word.
-                const uint32_t pc = __popc(word);
+                if (g >= nlist) break;
+                const uint32_t st = s_list[g];
+                const uint32_t pos = s_soff[g];
+                const uint32_t T = s_soff[g + 1] - pos;
+                const uint32_t q4 = st * 32u + lane;  // lane's uint4 of the step
+                const uint4 x = bm4[q4];
+                const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
                 const uint32_t inc = warp_inclusive_scan(pc);
-                const uint32_t cb = (uint32_t)(c0 + (uint64_t)st * 1024u);
-                for (uint32_t k0 = 0; k0 < T; k0 += 32) {
-                    const uint32_t k = k0 + lane;
+                const uint32_t colbase = (uint32_t)c0;
+                for (uint32_t w0 = 0; w0 < T; w0 += BMP_STAGE) {
+                    const uint32_t m = min(BMP_STAGE, T - w0);
+                    const uint32_t per = (m + 31) >> 5;  // outputs per lane
+                    const uint32_t k = w0 + lane * per;
+                    const uint32_t kend = min(k + per, w0 + m);
+                    const uint32_t key = min(k, T - 1);
+                    // L = first lane whose inclusive count exceeds key
                     uint32_t L = 0;
 #pragma unroll
                     for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
                         const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, L + sft - 1);
-                        if (v <= k) L += sft;
+                        if (v <= key) L += sft;
                     }
-                    const uint32_t wL = __shfl_sync(0xFFFFFFFFu, word, L);
                     const uint32_t exL = __shfl_sync(0xFFFFFFFFu, inc - pc, L);
-                    if (k < T) out[pos + k] = cb + L * 32u + nth_set_bit(wL, k - exL);
+                    if (k < kend) {
+                        const uint4 y = bm4[st * 32u + L];
+                        uint32_t r = key - exL, wv = y.x, widx = (st * 32u + L) * 4u, c;
+                        c = __popc(y.x);
+                        if (r >= c) {
+                            r -= c; wv = y.y; ++widx; c = __popc(y.y);
+                            if (r >= c) {
+                                r -= c; wv = y.z; ++widx; c = __popc(y.z);
+                                if (r >= c) { r -= c; wv = y.w; ++widx; }
+                            }
+                        }
+                        uint32_t cur = wv & (0xFFFFFFFFu << nth_set_bit(wv, r));
+                        for (uint32_t kk = k; kk < kend; ++kk) {
+                            while (!cur) cur = bm[++widx];  // the step holds more outputs
+                            stage[kk - w0] = colbase + widx * 32u + (uint32_t)(__ffs(cur) - 1);
+                            cur &= cur - 1;
+                        }
+                    }
+                    __syncwarp();
+                    for (uint32_t t = lane; t < m; t += 32) out[pos + w0 + t] = stage[t];
+                    __syncwarp();
                 }
-                }
+                if (pc) bm4[q4] = make_uint4(0, 0, 0, 0);
             }
             total += ctot;
             __syncthreads();
