@@ -82,8 +82,9 @@ int validate_spgemm(const clb_dcsr &A, const clb_dcsr &B) {
         return fail(CLB_INVALID_ARGUMENT, "Invalid input matrix size! a : " + std::to_string(A.nrows) + " x " +
                                               std::to_string(A.ncols) + ", b: " + std::to_string(B.nrows) + " x " +
                                               std::to_string(B.ncols));
-    if (B.nnz >= (1ull << 32) || A.nzr >= (1ull << 32))
-        return fail(CLB_NOT_SUPPORTED, "right operand with 2^32 or more entries, or left with 2^32 stored rows");
+    // 32-bit positions into B.cols, with room for one aligned 1024-entry window
+    if (B.nnz > 0xFFFFF000ull || A.nzr >= (1ull << 32))
+        return fail(CLB_NOT_SUPPORTED, "right operand with 2^32 - 4096 or more entries, or left with 2^32 stored rows");
     if (B.ncols > 0xFFFFFFFFull) return fail(CLB_NOT_SUPPORTED, "more than 2^32-1 columns");
     if ((A.nnz && (!A.rpt || !A.rows || !A.cols)) || (B.nnz && (!B.rpt || !B.rows || !B.cols)))
         return fail(CLB_INVALID_ARGUMENT, "matrix with entries but NULL arrays");

@@ -511,8 +511,18 @@ __device__ __forceinline__ void unit_products(const AView &a, const BRows &b, ui
             const uint32_t first = (u - s_upre[e]) << shift;
             const uint32_t cnt = min(unit, s_len[e] - first);
             const uint32_t *src = b.cols + s_beg[e] + first;
+            // whole sweeps of 32 * BMP_U positions: no per-position checks
+            const uint32_t full = cnt / (32u * BMP_U) * (32u * BMP_U);
 #pragma unroll 1
-            for (uint32_t k0 = 0; k0 < cnt; k0 += 32u * BMP_U) {
+            for (uint32_t k0 = 0; k0 < full; k0 += 32u * BMP_U) {
+                uint32_t col[BMP_U];
+#pragma unroll
+                for (int s = 0; s < BMP_U; ++s) col[s] = __ldg(src + k0 + (uint32_t)s * 32u + lane);
+#pragma unroll
+                for (int s = 0; s < BMP_U; ++s) f(col[s], true);
+            }
+#pragma unroll 1
+            for (uint32_t k0 = full; k0 < cnt; k0 += 32u * BMP_U) {
                 uint32_t col[BMP_U];
 #pragma unroll
                 for (int s = 0; s < BMP_U; ++s) {
@@ -523,6 +533,98 @@ __device__ __forceinline__ void unit_products(const AView &a, const BRows &b, ui
                 for (int s = 0; s < BMP_U; ++s) {
                     if (k0 + (uint32_t)s * 32u < cnt)  // warp-uniform
                         f(col[s], k0 + (uint32_t)s * 32u + lane < cnt);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Single-chunk insertion (all columns fit the bitmap).  Units are the
+// intersections of a B row with ALIGNED windows of 2^shift positions of
+// B.cols, so all but a row's first and last unit are whole windows.  A warp
+// sweeps 256 positions at a time; lane l takes the 8 consecutive positions
+// 8l..8l+7 of the sweep (two 16-byte loads when B.cols is 16-byte aligned,
+// coalesced over the warp) and issues one atomic per position, slot by slot:
+// in each atomic instruction the lanes are 8 positions of a sorted B row
+// apart, so they rarely share a word or a bank (neighbouring positions did,
+// and those atomics serialised).  A 16-byte load is issued only when it
+// covers a valid position, so it never leaves the 16-byte block of a valid
+// column.  Columns are clamped to the bitmap (memory safety on malformed
+// input).  Requires B.nnz <= 2^32 - 4096.
+template <int NT, int ECH>
+__device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b, uint32_t i, uint32_t shift,
+                                                  uint32_t maxcol, uint32_t *bm, uint32_t *s_beg, uint32_t *s_len,
+                                                  uint32_t *s_upre, uint32_t *scratch) {
+    static_assert(ECH % NT == 0, "entry chunk must be a multiple of the block");
+    constexpr int EPT = ECH / NT;
+    constexpr int NW = NT / 32;
+    const uint32_t unit = 1u << shift;
+    const uint32_t lane = lane_id(), w = warp_id();
+    const bool vec = (reinterpret_cast<uintptr_t>(b.cols) & 15u) == 0;
+    const uint64_t ja = a.rpt[i], je = a.rpt[i + 1];
+    for (uint64_t c0 = ja; c0 < je; c0 += ECH) {
+        const uint32_t n = (uint32_t)min((uint64_t)ECH, je - c0);
+        uint32_t units[EPT], sum = 0;
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const uint32_t e = threadIdx.x * EPT + k;
+            units[k] = 0;
+            if (e < n) {
+                uint64_t bb;
+                const uint32_t len = b_row(b, __ldg(a.cols + c0 + e), bb);
+                s_beg[e] = (uint32_t)bb;
+                s_len[e] = len;
+                if (len) units[k] = (uint32_t)(((bb + len - 1) >> shift) - (bb >> shift) + 1);
+            }
+            sum += units[k];
+        }
+        uint32_t total;
+        uint32_t run = block_exclusive_scan<uint32_t, NT>(sum, scratch, &total);
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const uint32_t e = threadIdx.x * EPT + k;
+            if (e < n) s_upre[e] = run;
+            run += units[k];
+        }
+        if (threadIdx.x == 0) s_upre[n] = total;
+        __syncthreads();
+        uint32_t e = 0;  // warp-uniform entry cursor
+        for (uint32_t u = w; u < total; u += NW) {
+            for (;;) {
+                const uint32_t idx = e + 1 + lane;
+                const bool le = idx <= n && s_upre[idx] <= u;
+                const uint32_t m = __ballot_sync(0xFFFFFFFFu, le);
+                e += __popc(m);
+                if (m != 0xFFFFFFFFu) break;
+            }
+            const uint32_t beg = s_beg[e];
+            const uint32_t ws = ((beg >> shift) + (u - s_upre[e])) << shift;  // window start
+            const uint32_t vlo = max(beg, ws), vhi = min(beg + s_len[e], ws + unit);
+#pragma unroll 1
+            for (uint32_t k0 = ws; k0 < vhi; k0 += 256u) {
+                const uint32_t p0 = k0 + lane * 8u;
+                uint32_t v[8];
+                if (vec) {
+                    const uint4 *p4 = reinterpret_cast<const uint4 *>(b.cols + p0);
+                    const uint4 x = (p0 + 4u > vlo && p0 < vhi) ? __ldg(p4) : make_uint4(0, 0, 0, 0);
+                    const uint4 y = (p0 + 8u > vlo && p0 + 4u < vhi) ? __ldg(p4 + 1) : make_uint4(0, 0, 0, 0);
+                    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+                    v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const uint32_t q = p0 + (uint32_t)j;
+                        v[j] = (q >= vlo && q < vhi) ? __ldg(b.cols + q) : 0u;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const uint32_t q = p0 + (uint32_t)j;
+                    if (q >= vlo && q < vhi) {
+                        const uint32_t c = min(v[j], maxcol);
+                        atomicOr(bm + (c >> 5), 1u << (c & 31));
+                    }
                 }
             }
         }
@@ -592,10 +694,8 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
                     if (valid && r < chunk_cols) atomicOr(bm + (r >> 5), 1u << (r & 31));
                 });
             } else {
-                unit_products<BMP_NT, BMP_ECH>(a, b, i, shift, s_beg, s_len, s_upre, scratch,
-                                               [&](uint32_t c, bool valid) {
-                    if (valid && c < (uint32_t)chunk_cols) atomicOr(bm + (c >> 5), 1u << (c & 31));
-                });
+                bitmap_insert_row<BMP_NT, BMP_ECH>(a, b, i, shift, (uint32_t)(chunk_cols - 1), bm, s_beg, s_len,
+                                                   s_upre, scratch);
             }
             if (!NUMERIC || overflowed) {
                 uint32_t mine = 0;
