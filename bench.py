@@ -343,7 +343,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "e2e": e2e, "gpu_launches": run["launches"], "clocks": run["clocks"], "wall_s": run["wall"],
     }
     if args.form != "two_pass":
-        line["form_stats"] = {k: st.get(k) for k in ("capacity", "fallback_rows", "nzr", "nnz")}
+        line["form_stats"] = {k: st.get(k) for k in ("capacity", "fallback_rows", "spilled_rows", "nzr", "nnz")}
     if compare is not None:
         line["compare"] = compare
     if not args.no_cpu_baseline:

@@ -36,12 +36,13 @@ class clb_profile_entry(C.Structure):
 class clb_spgemm_stats(C.Structure):
     _fields_ = [("products", C.c_uint64), ("nnz", C.c_uint64), ("nzr", C.c_uint64),
                 ("rows_per_bin", C.c_uint64 * 16), ("fallback_rows", C.c_uint64), ("capacity", C.c_uint64),
-                ("kernel_launches", C.c_uint32), ("reserved", C.c_uint32)]
+                ("kernel_launches", C.c_uint32), ("reserved", C.c_uint32), ("spilled_rows", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {"products": self.products, "nnz": self.nnz, "nzr": self.nzr,
                 "rows_per_bin": list(self.rows_per_bin)[:12], "fallback_rows": self.fallback_rows,
-                "capacity": self.capacity, "kernel_launches": self.kernel_launches}
+                "capacity": self.capacity, "kernel_launches": self.kernel_launches,
+                "spilled_rows": self.spilled_rows}
 
 
 P = C.POINTER

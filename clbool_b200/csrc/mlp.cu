@@ -245,11 +245,19 @@ __global__ void __launch_bounds__(FT_NT) features_kernel(AView a, BRows b, uint6
     }
 }
 
-// capacity = clamp(ceil((2^(16 y + margin) - 1) + slack), 1, min(P, ncols))
+// capacity = clamp(ceil((2^(16 y + margin) - 1) + slack), 1, min(P, ncols)) for
+// the bitmap rows (more than `exact_below` products); the lighter rows get
+// their exact bound min(P, ncols): they hold a small share of the products,
+// and the ESC accumulators that serve them need no capacity check.
 __global__ void capacity_kernel(const float *__restrict__ pred, const uint32_t *__restrict__ work, uint64_t n,
-                                uint64_t ncols, float margin_log2, float slack, uint32_t *__restrict__ cap) {
+                                uint64_t ncols, float margin_log2, float slack, uint32_t exact_below,
+                                uint32_t *__restrict__ cap) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t ub = min((uint64_t)work[i], ncols);
+        if (work[i] <= exact_below) {
+            cap[i] = (uint32_t)ub;
+            continue;
+        }
         const float e = pred[i] / FEAT_SCALE + margin_log2;
         const float c = exp2f(fminf(e, 40.0f)) - 1.0f + slack;
         uint64_t k = c <= 1.0f ? 1 : (c >= 4.0e9f ? ub : (uint64_t)ceilf(c));
@@ -540,7 +548,7 @@ int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a_, const clb_dcs
         ProfScope ps(ctl, "predict");
         predict_kernel<<<grid_for(ctl, n, MLP_NT, 4), MLP_NT, 0, ctl->stream>>>(sizer->params, feat.ptr, n, pred.ptr);
         capacity_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(pred.ptr, work.ptr, n, B.ncols, margin_log2, slack,
-                                                                  cap.ptr);
+                                                                  ESC_MAX_PRODUCTS, cap.ptr);
         ctl->launches += 2;
         CLB_CHECK_LAUNCH();
     }
@@ -550,7 +558,9 @@ int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a_, const clb_dcs
     CLB_RETURN_IF(scan_u32_to_u64(ctl, work.ptr, wsum.ptr, n, tot.ptr));
     uint64_t products = 0;
     CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &products, 1));
-    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, false, products, c, &st);
+    // ESC accumulators for the rows up to ESC_MAX_PRODUCTS products, learned
+    // capacities and the spill arena (1/16 of the slots) for the bitmap rows
+    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st, 16);
     st.kernel_launches = ctl->launches;
     if (stats) *stats = st;
     return rc;

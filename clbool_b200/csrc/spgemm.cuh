@@ -28,7 +28,8 @@ int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AVie
 // exact fallback for rows that outgrew their capacity, compaction.
 int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                        const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
-                       clb_spgemm_stats *st);
+                       clb_spgemm_stats *st,
+                       uint64_t arena_div);
 int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
                          clb_spgemm_stats *stats);
 

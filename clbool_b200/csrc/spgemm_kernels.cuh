@@ -45,6 +45,10 @@ enum Bin : int {
     NUM_BINS = 12
 };
 
+// Rows with at most this many products never reach the bitmap accumulator
+// when binned by products (the ESC form): the CTA ESC kernels take them.
+constexpr uint32_t ESC_MAX_PRODUCTS = 4096;
+
 // Bin of a row from its product count and its distinct-column bound
 // (min(products, ncols), or a learned capacity).
 __host__ __device__ __forceinline__ int bin_of(uint64_t products, uint64_t distinct_bound) {
@@ -78,8 +82,11 @@ __device__ __forceinline__ void bin_range(const BinLists &bl, int bin, uint32_t 
 
 // Output side of an accumulator.  Symbolic: row_nnz[i] = distinct columns.
 // Numeric: columns written at cols + row_off[i]; when row_cap is non-null
-// (learned form) a row whose count exceeds row_cap[i] is not written and is
-// flagged in overflow[i] instead.
+// (single-pass forms) a row whose count exceeds row_cap[i] is not written
+// there.  A single-chunk bitmap row then reserves its exact count in the
+// spill arena (when one is given and has room), writes there and records the
+// arena offset in spill[i]; any other such row is flagged in overflow[i] and
+// recomputed by the exact two-pass form.
 struct RowOut {
     uint32_t *row_nnz;
     const uint64_t *row_off;
@@ -87,6 +94,10 @@ struct RowOut {
     uint32_t *overflow;
     uint32_t *cols;
     uint32_t *status;
+    uint64_t *spill = nullptr;                     // arena offset per row, ~0 = not spilled
+    uint32_t *arena = nullptr;
+    unsigned long long *arena_cursor = nullptr;    // entries reserved so far
+    uint64_t arena_cap = 0;                        // entries
 };
 
 // ------------------------------------------------------------- warp ESC ----
@@ -666,6 +677,7 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
     uint32_t *s_stage = s_soff + BMP_MAX_STEPS + 1; // BMP_NW * BMP_STAGE
     __shared__ uint32_t scratch[33];
     __shared__ uint32_t s_slot, s_next;
+    __shared__ unsigned long long s_spill;
     uint32_t beg, cnt = 0, tmp;
     bin_range(bl, bin_lo, beg, tmp);
     for (int q = bin_lo; q <= bin_hi; ++q) cnt += bl.info[q];
@@ -732,16 +744,29 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
                 s_next = 0;
             }
             __syncthreads();
+            uint32_t *out = o.cols + out_base + total;
             if (o.row_cap && total + ctot > o.row_cap[i]) {
-                // single-pass forms: the row does not fit its slot; clear the
-                // bitmap and flag the row.
-                overflowed = true;
-                for (uint32_t w4 = threadIdx.x; w4 < W / 4; w4 += BMP_NT) bm4[w4] = make_uint4(0, 0, 0, 0);
-                total += ctot;
-                __syncthreads();
-                continue;
+                // single-pass forms: the row does not fit its slot.  A
+                // single-chunk row knows its exact count now: reserve it in
+                // the spill arena and emit there.  Otherwise clear the bitmap
+                // and flag the row for the exact recomputation.
+                if (!MULTI && o.arena) {
+                    if (threadIdx.x == 0) {
+                        const unsigned long long at = atomicAdd(o.arena_cursor, (unsigned long long)ctot);
+                        s_spill = at + ctot <= o.arena_cap ? at : ~0ull;
+                    }
+                    __syncthreads();
+                }
+                if (MULTI || !o.arena || s_spill == ~0ull) {
+                    overflowed = true;
+                    for (uint32_t w4 = threadIdx.x; w4 < W / 4; w4 += BMP_NT) bm4[w4] = make_uint4(0, 0, 0, 0);
+                    total += ctot;
+                    __syncthreads();
+                    continue;
+                }
+                out = o.arena + s_spill;
+                if (threadIdx.x == 0) o.spill[i] = s_spill;
             }
-            uint32_t *const out = o.cols + out_base + total;
             for (;;) {
                 uint32_t g = 0;
                 if (lane == 0) g = atomicAdd(&s_next, 1u);

@@ -132,13 +132,16 @@ __global__ void compact_rows_kernel(const uint32_t *__restrict__ row_nnz, const 
                                     const uint64_t *__restrict__ off, const uint32_t *__restrict__ pre,
                                     const uint32_t *__restrict__ ovf, const uint32_t *__restrict__ pos,
                                     const uint64_t *__restrict__ sub_crpt, const uint32_t *__restrict__ sub_ccols,
+                                    const uint64_t *__restrict__ spill, const uint32_t *__restrict__ arena,
                                     uint64_t n, uint32_t *__restrict__ ccols) {
     const uint32_t lane = lane_id();
     const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
     for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); i < n; i += nw) {
         const uint32_t len = row_nnz[i];
         if (!len) continue;
-        const uint32_t *src = (ovf && ovf[i]) ? sub_ccols + sub_crpt[pos[i]] : pre + slot_off[i];
+        const uint64_t sp = spill ? spill[i] : ~0ull;
+        const uint32_t *src = (ovf && ovf[i]) ? sub_ccols + sub_crpt[pos[i]]
+                                               : (sp != ~0ull ? arena + sp : pre + slot_off[i]);
         uint32_t *dst = ccols + off[i];
         uint32_t t = lane;
         for (; t + 96 < len; t += 128) {
@@ -153,13 +156,18 @@ __global__ void compact_rows_kernel(const uint32_t *__restrict__ row_nnz, const 
     }
 }
 
-// Number of nonzero entries of a u32 array (the overflowed rows).
-__global__ void count_nonzero_kernel(const uint32_t *__restrict__ a, uint64_t n, unsigned long long *__restrict__ out) {
-    unsigned long long mine = 0;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        mine += a[i] != 0;
+// Number of overflowed rows (nonzero ovf) and of spilled rows (spill != ~0).
+__global__ void count_rows_kernel(const uint32_t *__restrict__ ovf, const uint64_t *__restrict__ spill, uint64_t n,
+                                  unsigned long long *__restrict__ out) {
+    unsigned long long mine = 0, sp = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        mine += ovf[i] != 0;
+        if (spill) sp += spill[i] != ~0ull;
+    }
     mine = warp_sum(mine);
+    sp = warp_sum(sp);
     if (lane_id() == 0 && mine) atomicAdd(out, mine);
+    if (lane_id() == 0 && sp) atomicAdd(out + 1, sp);
 }
 
 template <class K>
@@ -211,7 +219,7 @@ int launch_esc_accumulators(clb_controls *ctl, const BinLists &bl, const AView &
 // hash accumulators.
 int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                        const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
-                       clb_spgemm_stats *st) {
+                       clb_spgemm_stats *st, uint64_t arena_div) {
     const uint64_t n = A.nzr;
     clb_dcsr C{};
     C.nrows = A.nrows;
@@ -248,6 +256,20 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
 
     BinLists bl{list.ptr, info.ptr};
     RowOut num{row_nnz.ptr, slot_off.ptr, cap, ovf.ptr, pre.ptr, ctl->d_status};
+    // spill arena for single-chunk bitmap rows over their capacity
+    Temp<uint64_t> spill;
+    Temp<uint32_t> arena;
+    if (arena_div) {
+        uint64_t acap = capacity / arena_div;
+        if (acap < (1ull << 24)) acap = 1ull << 24;
+        CLB_RETURN_IF(spill.alloc(ctl, n));
+        CLB_RETURN_IF(arena.alloc(ctl, acap));
+        CLB_TRY_CUDA(cudaMemsetAsync(spill.ptr, 0xFF, n * 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+        num.spill = spill.ptr;
+        num.arena = arena.ptr;
+        num.arena_cursor = (unsigned long long *)(scal.ptr + 6);
+        num.arena_cap = acap;
+    }
     if (esc) {
         // warp ESC and bitmap rows through the shared launcher's bins; rows of
         // the hash bins go to the CTA ESC kernels instead.
@@ -260,13 +282,17 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     // the fallback below resets the device status word: check it first
     CLB_RETURN_IF(check_status(ctl, esc ? "matrix_multiplication" : "matrix_multiplication_learned"));
     // rows that outgrew their capacity: re-run them with the exact two-pass form
-    unsigned long long *d_novf = (unsigned long long *)(scal.ptr + 2);
-    count_nonzero_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, n, d_novf);
+    unsigned long long *d_novf = (unsigned long long *)(scal.ptr + 2);  // [2] overflowed, [3] spilled
+    count_rows_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, spill.ptr, n, d_novf);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
-    uint64_t novf = 0;
-    CLB_RETURN_IF(read_scalars(ctl, scal.ptr + 2, &novf, 1));
-    if (st) st->fallback_rows = novf;
+    uint64_t cnts[2] = {0, 0};
+    CLB_RETURN_IF(read_scalars(ctl, scal.ptr + 2, cnts, 2));
+    const uint64_t novf = cnts[0];
+    if (st) {
+        st->fallback_rows = novf;
+        st->spilled_rows = cnts[1];
+    }
     clb_dcsr sub_c{};
     Temp<uint64_t> sub_rpt, sub_off;
     Temp<uint32_t> sub_rows, sub_cols, sub_len;
@@ -276,7 +302,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
         CLB_RETURN_IF(sub_off.alloc(ctl, n));
         CLB_TRY_CUDA(cudaMemcpyAsync(opos.ptr, ovf.ptr, n * 4, cudaMemcpyDeviceToDevice, ctl->stream),
                      CLB_COPY_BUFFER_ERROR);
-        CLB_RETURN_IF(scan_u32_inplace(ctl, opos.ptr, n, scal.ptr + 3));
+        CLB_RETURN_IF(scan_u32_inplace(ctl, opos.ptr, n, scal.ptr + 7));
         gather_rows_lengths_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, A.rpt, n, sub_len.ptr);
         ctl->launches += 1;
         CLB_CHECK_LAUNCH();
@@ -322,7 +348,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
             ProfScope ps(ctl, "compact");
             compact_rows_kernel<<<grid_for(ctl, n * 32, 32), 256, 0, ctl->stream>>>(
                 row_nnz.ptr, slot_off.ptr, off.ptr, pre.ptr, novf ? ovf.ptr : nullptr, opos.ptr, sub_c.rpt,
-                sub_c.cols, n, c_cols.ptr);
+                sub_c.cols, spill.ptr, arena.ptr, n, c_cols.ptr);
             ctl->launches += 1;
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) rc = fail(CLB_RUN_KERNEL_FAILURE, cudaGetErrorString(e));
@@ -385,7 +411,7 @@ int clb_dcsr_spgemm_esc(clb_controls *ctl, const clb_dcsr *a_, const clb_dcsr *b
     CLB_CHECK_LAUNCH();
     uint64_t products = 0;
     CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &products, 1));
-    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st);
+    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st, 0);
     st.kernel_launches = ctl->launches;
     if (stats) *stats = st;
     return rc;

@@ -85,10 +85,12 @@ typedef struct clb_spgemm_stats {
     uint64_t products;        /* sum over A rows of the B-row lengths hit  */
     uint64_t nnz, nzr;        /* of C                                       */
     uint64_t rows_per_bin[16];/* A rows routed to each accumulator bin      */
-    uint64_t fallback_rows;   /* learned form: rows re-run by two passes    */
-    uint64_t capacity;        /* learned form: slots allocated for C        */
+    uint64_t fallback_rows;   /* single-pass forms: rows re-run by two passes */
+    uint64_t capacity;        /* single-pass forms: slots allocated for C   */
     uint32_t kernel_launches; /* kernels this call launched                 */
     uint32_t reserved;
+    uint64_t spilled_rows;    /* learned form: rows over their slot that went
+                                 to the spill arena in the same pass        */
 } clb_spgemm_stats;
 
 typedef struct clb_controls clb_controls;

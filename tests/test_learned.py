@@ -176,11 +176,17 @@ def test_learned_bit_exact_any_predictor(controls, margin):
         ub = np.minimum(O.workload(a, b), b.ncols).astype(np.int64)
         assert st["capacity"] <= int(ub.sum())
         if margin >= 1000.0:
-            assert st["fallback_rows"] == 0
+            assert st["fallback_rows"] == 0 and st["spilled_rows"] == 0
             assert st["capacity"] == int(ub.sum())
         if margin <= -1000.0:
-            # capacity 1 per row: exactly the rows with more than one output overflow
-            assert st["fallback_rows"] == int((np.diff(want.rpt.astype(np.int64)) > 1).sum())
+            # rows up to 4096 products get their exact bound; the heavier ones
+            # one slot, so exactly those with more than one output go to the
+            # spill arena (all columns fit one bitmap chunk here)
+            work = O.workload(a, b).astype(np.int64)
+            heavy = work[work > 0] > 4096
+            row_len = np.diff(want.rpt.astype(np.int64))
+            assert st["fallback_rows"] == 0
+            assert st["spilled_rows"] == int((heavy & (row_len > 1)).sum())
 
 
 @pytest.mark.gpu
@@ -231,7 +237,7 @@ def test_trained_predictor_gain(controls):
     assert st["capacity"] < 1.6 * len(want.cols), (st["capacity"], len(want.cols))
     # a small training set (scales 11-13, seconds of training): some rows
     # still fall back; the packaged predictor is tested separately
-    assert st["fallback_rows"] < 0.15 * nzr, (st["fallback_rows"], nzr)
+    assert st["fallback_rows"] + st["spilled_rows"] < 0.15 * nzr, st
     # without a predictor (ESC form: upper-bound capacity) the same product
     st_esc = {}
     c = cb.matrix_dcsr()
