@@ -45,6 +45,15 @@ class clb_spgemm_stats(C.Structure):
                 "spilled_rows": self.spilled_rows}
 
 
+class clb_spgemm_tuning(C.Structure):
+    _fields_ = [("form", C.c_uint32), ("warp_max", C.c_uint32), ("bitmap_min", C.c_uint32),
+                ("bitmap_threads", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+
+    def as_dict(self) -> dict:
+        return {"form": "two_pass" if self.form == 0 else "single_pass", "warp_max": self.warp_max,
+                "bitmap_min": self.bitmap_min, "bitmap_threads": self.bitmap_threads}
+
+
 P = C.POINTER
 
 # name -> (restype, argtypes)
@@ -104,6 +113,14 @@ _SIGS = {
                                   P(C.c_float)]),
     "clb_dcsr_spgemm_learned": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, C.c_float, C.c_float, P(clb_dcsr),
                                           P(clb_spgemm_stats)]),
+    # tuning and batching
+    "clb_spgemm_tuning_default": (None, [P(clb_spgemm_tuning)]),
+    "clb_dcsr_spgemm_tuned": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_tuning), P(clb_dcsr),
+                                        P(clb_spgemm_stats)]),
+    "clb_dcsr_spgemm_batched": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr),
+                                          P(clb_spgemm_tuning), P(clb_spgemm_stats)]),
+    "clb_spgemm_autotune": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_tuning),
+                                      P(clb_spgemm_tuning), P(C.c_double), C.c_uint32, P(C.c_uint32)]),
 }
 
 def _load():

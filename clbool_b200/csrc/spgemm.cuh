@@ -14,23 +14,25 @@ int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t 
 // distinct columns is cap[i] when cap is non-null, else min(work[i], ncols).
 // flags[i] = 1 for rows with products (input of the C row-position scan).
 int launch_binning(clb_controls *ctl, const uint32_t *work, const uint32_t *cap, uint64_t n, uint64_t ncols,
-                   uint32_t *info, uint32_t *list, uint32_t *flags);
+                   uint32_t *info, uint32_t *list, uint32_t *flags, const Tuning &t = Tuning());
 // Runs every bin's accumulator kernel (symbolic or numeric).
 int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, const AView &a, const BRows &b,
-                        const RowOut &o, uint64_t ncols, uint64_t nrows_max);
+                        const RowOut &o, uint64_t ncols, uint64_t nrows_max, const Tuning &t = Tuning());
 // C.rpt/C.rows from the row flags' exclusive scan (pos) and the row offsets.
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
                     const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz);
 // Numeric accumulators without (hash_bins = false) the hash bins.
 int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
-                               const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins);
+                               const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins,
+                               const Tuning &t = Tuning());
 // Single-pass forms (spgemm_single.cu): capacity slots, one numeric pass,
 // exact fallback for rows that outgrew their capacity, compaction.
 int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                        const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
-                       clb_spgemm_stats *st,
-                       uint64_t arena_div);
+                       clb_spgemm_stats *st, uint64_t arena_div, const Tuning &t = Tuning());
+// cap[i] = min(work[i], ncols): the exact upper bound of a row's count.
+int launch_upper_bound_caps(clb_controls *ctl, const uint32_t *work, uint64_t n, uint64_t ncols, uint32_t *cap);
 int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
-                         clb_spgemm_stats *stats);
+                         clb_spgemm_stats *stats, const Tuning &t = Tuning());
 
 }  // namespace clb

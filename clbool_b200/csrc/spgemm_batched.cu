@@ -1,0 +1,392 @@
+// spgemm_batched.cu -- many independent boolean products C_k = A_k * B_k in
+// one pass, plus the accumulator autotuner.  Not in the reference, which
+// multiplies one pair per call (src/dcsr/dcsr.hpp:27-36).
+//
+// The pairs are stacked block-diagonally:
+//   A' = [A_1; A_2; ...]  rows shifted by the rows of A_1..A_{k-1}, columns
+//                         shifted by the rows of B_1..B_{k-1};
+//   B' = [B_1; B_2; ...]  rows shifted likewise, columns NOT shifted
+//                         (B'.ncols = max_k B_k.ncols).
+// Row i of A' (pair k) only meets rows of B_k, so C' = A' B' holds C_k in the
+// rows of pair k with C_k's own column indices.  One SpGEMM over (A', B')
+// runs every pair in the same launches -- one workload pass, one binning,
+// one persistent launch per accumulator kind -- balanced across the whole
+// batch, so the launch count does not grow with the number of pairs.  A
+// split kernel then cuts C' into the C_k.
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "spgemm.cuh"
+
+namespace clb {
+
+namespace {
+
+struct PairDesc {
+    const uint64_t *rpt;
+    const uint32_t *rows;
+    const uint32_t *cols;
+    uint64_t nzr, nnz;
+    uint64_t nzr_off, nnz_off;  // position in the stacked matrix
+    uint32_t row_add, col_add;  // added to row ids / column ids
+};
+
+constexpr int CAT_NT = 256;
+
+// Stacks the pairs' matrices: blockIdx.y = pair.
+__global__ void __launch_bounds__(CAT_NT) stack_kernel(const PairDesc *__restrict__ d, uint64_t *__restrict__ rpt,
+                                                       uint32_t *__restrict__ rows, uint32_t *__restrict__ cols,
+                                                       uint64_t total_nzr, uint64_t total_nnz) {
+    const PairDesc p = d[blockIdx.y];
+    const uint64_t stride = (uint64_t)gridDim.x * CAT_NT;
+    const uint64_t t0 = (uint64_t)blockIdx.x * CAT_NT + threadIdx.x;
+    const uint64_t base = p.nzr ? p.rpt[0] : 0;
+    for (uint64_t r = t0; r < p.nzr; r += stride) {
+        rows[p.nzr_off + r] = p.rows[r] + p.row_add;
+        rpt[p.nzr_off + r] = p.rpt[r] - base + p.nnz_off;
+    }
+    for (uint64_t j = t0; j < p.nnz; j += stride) cols[p.nnz_off + j] = p.cols[j] + p.col_add;
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) rpt[total_nzr] = total_nnz;
+}
+
+// bounds[k] = first row of C' at or after row_start[k] (k <= count), and
+// nnz_bounds[k] = C'.rpt[bounds[k]].
+__global__ void split_bounds_kernel(const uint32_t *__restrict__ crows, const uint64_t *__restrict__ crpt, uint64_t nzr,
+                                    const uint64_t *__restrict__ row_start, uint32_t count,
+                                    uint64_t *__restrict__ bounds) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= count; k += gridDim.x * blockDim.x) {
+        const uint64_t key = row_start[k];
+        uint64_t lo = 0, hi = nzr;
+        while (lo < hi) {
+            const uint64_t m = lo + (hi - lo) / 2;
+            if ((uint64_t)crows[m] < key) lo = m + 1; else hi = m;
+        }
+        bounds[k] = lo;
+        bounds[count + 1 + k] = crpt[lo];
+    }
+}
+
+struct OutDesc {
+    uint64_t *rpt;
+    uint32_t *rows;
+    uint32_t *cols;
+    uint64_t r0, nzr;    // rows [r0, r0 + nzr) of C'
+    uint64_t j0, nnz;    // columns [j0, j0 + nnz) of C'
+    uint32_t row_sub;
+};
+
+__global__ void __launch_bounds__(CAT_NT) split_kernel(const OutDesc *__restrict__ d, const uint64_t *__restrict__ crpt,
+                                                       const uint32_t *__restrict__ crows,
+                                                       const uint32_t *__restrict__ ccols) {
+    const OutDesc o = d[blockIdx.y];
+    if (!o.nnz) return;
+    const uint64_t stride = (uint64_t)gridDim.x * CAT_NT;
+    const uint64_t t0 = (uint64_t)blockIdx.x * CAT_NT + threadIdx.x;
+    for (uint64_t r = t0; r <= o.nzr; r += stride) {
+        o.rpt[r] = crpt[o.r0 + r] - o.j0;
+        if (r < o.nzr) o.rows[r] = crows[o.r0 + r] - o.row_sub;
+    }
+    for (uint64_t j = t0; j < o.nnz; j += stride) o.cols[j] = ccols[o.j0 + j];
+}
+
+unsigned stack_grid_x(const clb_controls *ctl, uint64_t largest, uint32_t count) {
+    uint64_t gx = (largest + CAT_NT - 1) / CAT_NT;
+    const uint64_t cap = std::max<uint64_t>(1, (uint64_t)ctl->sm_count * 8 / std::max<uint32_t>(count, 1)) + 1;
+    gx = std::min<uint64_t>(std::max<uint64_t>(gx, 1), std::max<uint64_t>(cap, 4));
+    return (unsigned)gx;
+}
+
+Tuning to_tuning(const clb_spgemm_tuning *t) {
+    Tuning r;
+    if (!t) return r;
+    if (t->warp_max) r.warp_max = t->warp_max;
+    if (t->bitmap_min) r.bitmap_min = t->bitmap_min;
+    if (t->bitmap_threads) r.bitmap_threads = t->bitmap_threads;
+    return r;
+}
+
+int check_tuning(const clb_spgemm_tuning *t) {
+    if (!t) return CLB_SUCCESS;
+    if (t->form > 1) return fail(CLB_INVALID_VALUE, "tuning.form must be 0 (two-pass) or 1 (single pass)");
+    if (t->warp_max && t->warp_max != 32 && t->warp_max != 64 && t->warp_max != 128 && t->warp_max != 256)
+        return fail(CLB_INVALID_VALUE, "tuning.warp_max must be 32, 64, 128 or 256");
+    if (t->bitmap_min && (t->bitmap_min < 256 || t->bitmap_min > ESC_MAX_PRODUCTS))
+        return fail(CLB_INVALID_VALUE, "tuning.bitmap_min must be in [256, 4096]");
+    if (t->bitmap_threads && t->bitmap_threads != 256 && t->bitmap_threads != 512 && t->bitmap_threads != 1024)
+        return fail(CLB_INVALID_VALUE, "tuning.bitmap_threads must be 256, 512 or 1024");
+    return CLB_SUCCESS;
+}
+
+// One product with a tuning: the exact two-pass form or the single pass into
+// upper-bound slots (ESC accumulators for the rows below bitmap_min).
+int spgemm_tuned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, uint32_t form, const Tuning &t,
+                 clb_dcsr *c, clb_spgemm_stats *st) {
+    if (form == 0) return spgemm_hash_two_pass(ctl, A, B, c, st, t);
+    clb_spgemm_stats s{};
+    ctl->launches = 0;
+    if (A.nnz == 0 || B.nnz == 0 || A.nzr == 0 || B.nzr == 0) {
+        clb_dcsr C{};
+        C.nrows = A.nrows;
+        C.ncols = B.ncols;
+        *c = C;
+        if (st) *st = s;
+        return CLB_SUCCESS;
+    }
+    CLB_RETURN_IF(clear_status(ctl));
+    const AView a{A.rpt, A.rows, A.cols, A.nzr};
+    BRows b;
+    Temp<uint64_t> dense, tot;
+    CLB_RETURN_IF(prepare_b(ctl, B, dense, b));
+    Temp<uint32_t> work, cap;
+    CLB_RETURN_IF(work.alloc(ctl, A.nzr));
+    CLB_RETURN_IF(cap.alloc(ctl, A.nzr));
+    CLB_RETURN_IF(tot.alloc(ctl, 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(tot.ptr, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, tot.ptr));
+    CLB_RETURN_IF(launch_upper_bound_caps(ctl, work.ptr, A.nzr, B.ncols, cap.ptr));
+    uint64_t products = 0;
+    CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &products, 1));
+    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &s, 0, t);
+    s.kernel_launches = ctl->launches;
+    if (st) *st = s;
+    return rc;
+}
+
+}  // namespace
+
+}  // namespace clb
+
+using namespace clb;
+
+extern "C" {
+
+void clb_spgemm_tuning_default(clb_spgemm_tuning *t) {
+    if (!t) return;
+    *t = clb_spgemm_tuning{};
+    const Tuning d;
+    t->form = 0;
+    t->warp_max = d.warp_max;
+    t->bitmap_min = d.bitmap_min;
+    t->bitmap_threads = d.bitmap_threads;
+}
+
+int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_spgemm_tuning *tuning,
+                          clb_dcsr *c, clb_spgemm_stats *stats) {
+    if (!ctl || !a || !b || !c) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    CLB_RETURN_IF(check_tuning(tuning));
+    CLB_RETURN_IF(validate_spgemm(*a, *b));
+    DeviceGuard g(ctl);
+    return spgemm_tuned(ctl, *a, *b, tuning ? tuning->form : 0, to_tuning(tuning), c, stats);
+}
+
+int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
+                            const clb_spgemm_tuning *tuning, clb_spgemm_stats *stats) {
+    if (!ctl || (count && (!a || !b || !c))) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    if (count > 65535) return fail(CLB_NOT_SUPPORTED, "at most 65535 pairs per batch");
+    CLB_RETURN_IF(check_tuning(tuning));
+    clb_spgemm_stats st{};
+    if (stats) *stats = st;
+    if (count == 0) return CLB_SUCCESS;
+    // pair checks and offsets
+    std::vector<PairDesc> da(count), db(count);
+    std::vector<uint64_t> row_start(count + 1);
+    uint64_t arows = 0, brows = 0, anzr = 0, annz = 0, bnzr = 0, bnnz = 0, bcols = 0, amax = 0, bmax = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const int rc = validate_spgemm(a[k], b[k]);
+        if (rc != CLB_SUCCESS) return fail(rc, "pair " + std::to_string(k) + ": " + clb_last_error());
+        row_start[k] = arows;
+        const bool live = a[k].nnz && b[k].nnz;  // a pair without products contributes nothing
+        da[k] = PairDesc{a[k].rpt, a[k].rows, a[k].cols, live ? a[k].nzr : 0, live ? a[k].nnz : 0, anzr, annz,
+                         (uint32_t)arows, (uint32_t)brows};
+        db[k] = PairDesc{b[k].rpt, b[k].rows, b[k].cols, live ? b[k].nzr : 0, live ? b[k].nnz : 0, bnzr, bnnz,
+                         (uint32_t)brows, 0u};
+        if (live) {
+            anzr += a[k].nzr;
+            annz += a[k].nnz;
+            bnzr += b[k].nzr;
+            bnnz += b[k].nnz;
+            amax = std::max(amax, std::max(a[k].nnz, a[k].nzr + 1));
+            bmax = std::max(bmax, std::max(b[k].nnz, b[k].nzr + 1));
+        }
+        arows += a[k].nrows;
+        brows += b[k].nrows;
+        bcols = std::max(bcols, b[k].ncols);
+        if (arows > 0xFFFFFFFFull || brows > 0xFFFFFFFFull)
+            return fail(CLB_NOT_SUPPORTED, "the stacked batch exceeds 2^32 - 1 rows");
+    }
+    row_start[count] = arows;
+    for (uint32_t k = 0; k < count; ++k) {
+        clb_dcsr C{};
+        C.nrows = a[k].nrows;
+        C.ncols = b[k].ncols;
+        c[k] = C;
+    }
+    if (annz == 0) return CLB_SUCCESS;
+    DeviceGuard g(ctl);
+    const uint32_t form = tuning ? tuning->form : 0;
+    const Tuning t = to_tuning(tuning);
+
+    // stacked operands
+    Temp<PairDesc> dda, ddb;
+    Temp<uint64_t> arpt, brpt, rs;
+    Temp<uint32_t> arws, acls, brws, bcls;
+    CLB_RETURN_IF(dda.alloc(ctl, count));
+    CLB_RETURN_IF(ddb.alloc(ctl, count));
+    CLB_RETURN_IF(rs.alloc(ctl, count + 1));
+    CLB_RETURN_IF(arpt.alloc(ctl, anzr + 1));
+    CLB_RETURN_IF(arws.alloc(ctl, anzr));
+    CLB_RETURN_IF(acls.alloc(ctl, annz));
+    CLB_RETURN_IF(brpt.alloc(ctl, bnzr + 1));
+    CLB_RETURN_IF(brws.alloc(ctl, bnzr));
+    CLB_RETURN_IF(bcls.alloc(ctl, bnnz));
+    CLB_TRY_CUDA(cudaMemcpyAsync(dda.ptr, da.data(), count * sizeof(PairDesc), cudaMemcpyHostToDevice, ctl->stream),
+                 CLB_WRITE_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(ddb.ptr, db.data(), count * sizeof(PairDesc), cudaMemcpyHostToDevice, ctl->stream),
+                 CLB_WRITE_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(rs.ptr, row_start.data(), (count + 1) * 8, cudaMemcpyHostToDevice, ctl->stream),
+                 CLB_WRITE_BUFFER_ERROR);
+    {
+        ProfScope ps(ctl, "batch_stack");
+        stack_kernel<<<dim3(stack_grid_x(ctl, amax, count), count), CAT_NT, 0, ctl->stream>>>(dda.ptr, arpt.ptr,
+                                                                                             arws.ptr, acls.ptr, anzr,
+                                                                                             annz);
+        stack_kernel<<<dim3(stack_grid_x(ctl, bmax, count), count), CAT_NT, 0, ctl->stream>>>(ddb.ptr, brpt.ptr,
+                                                                                             brws.ptr, bcls.ptr, bnzr,
+                                                                                             bnnz);
+        CLB_CHECK_LAUNCH();
+    }
+    const clb_dcsr As{arows, brows, annz, anzr, arpt.ptr, arws.ptr, acls.ptr};
+    const clb_dcsr Bs{brows, bcols, bnnz, bnzr, brpt.ptr, brws.ptr, bcls.ptr};
+    CLB_RETURN_IF(validate_spgemm(As, Bs));
+    clb_dcsr Cs{};
+    CLB_RETURN_IF(spgemm_tuned(ctl, As, Bs, form, t, &Cs, &st));
+    const uint32_t inner_launches = st.kernel_launches;
+    if (Cs.nnz == 0) {
+        st.kernel_launches = inner_launches + 2;
+        if (stats) *stats = st;
+        return CLB_SUCCESS;
+    }
+    // split C' into the pairs' products
+    Temp<uint64_t> bounds;
+    int rc = bounds.alloc(ctl, 2 * (count + 1));
+    std::vector<uint64_t> hb(2 * (count + 1));
+    if (rc == CLB_SUCCESS) {
+        split_bounds_kernel<<<(count + 256) / 256, 256, 0, ctl->stream>>>(Cs.rows, Cs.rpt, Cs.nzr, rs.ptr, count,
+                                                                          bounds.ptr);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hb.data(), bounds.ptr, hb.size() * 8, cudaMemcpyDeviceToHost, ctl->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctl->stream);
+        if (e != cudaSuccess) rc = fail(CLB_RUN_KERNEL_FAILURE, cudaGetErrorString(e));
+    }
+    std::vector<OutDesc> od(count);
+    std::vector<clb_dcsr> outs(count);
+    uint64_t omax = 1;
+    for (uint32_t k = 0; k < count && rc == CLB_SUCCESS; ++k) {
+        const uint64_t r0 = hb[k], r1 = hb[k + 1], j0 = hb[count + 1 + k], j1 = hb[count + 1 + k + 1];
+        clb_dcsr C{};
+        C.nrows = a[k].nrows;
+        C.ncols = b[k].ncols;
+        OutDesc o{nullptr, nullptr, nullptr, r0, r1 - r0, j0, j1 - j0, (uint32_t)row_start[k]};
+        if (j1 > j0) {
+            Temp<uint64_t> p;
+            Temp<uint32_t> r, cc;
+            rc = p.alloc(ctl, r1 - r0 + 1);
+            if (rc == CLB_SUCCESS) rc = r.alloc(ctl, r1 - r0);
+            if (rc == CLB_SUCCESS) rc = cc.alloc(ctl, j1 - j0);
+            if (rc != CLB_SUCCESS) break;
+            o.rpt = p.ptr;
+            o.rows = r.ptr;
+            o.cols = cc.ptr;
+            C.nnz = j1 - j0;
+            C.nzr = r1 - r0;
+            C.rpt = p.release_ownership();
+            C.rows = r.release_ownership();
+            C.cols = cc.release_ownership();
+            omax = std::max(omax, std::max(C.nnz, C.nzr + 1));
+        }
+        od[k] = o;
+        outs[k] = C;
+    }
+    Temp<OutDesc> dod;
+    if (rc == CLB_SUCCESS) rc = dod.alloc(ctl, count);
+    if (rc == CLB_SUCCESS) {
+        cudaError_t e = cudaMemcpyAsync(dod.ptr, od.data(), count * sizeof(OutDesc), cudaMemcpyHostToDevice, ctl->stream);
+        if (e == cudaSuccess) {
+            ProfScope ps(ctl, "batch_split");
+            split_kernel<<<dim3(stack_grid_x(ctl, omax, count), count), CAT_NT, 0, ctl->stream>>>(dod.ptr, Cs.rpt,
+                                                                                                 Cs.rows, Cs.cols);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctl->stream);
+        if (e != cudaSuccess) rc = fail(CLB_RUN_KERNEL_FAILURE, cudaGetErrorString(e));
+    }
+    clb_dcsr_release(ctl, &Cs);
+    if (rc != CLB_SUCCESS) {
+        for (auto &o : outs) clb_dcsr_release(ctl, &o);
+        return rc;
+    }
+    for (uint32_t k = 0; k < count; ++k) c[k] = outs[k];
+    st.kernel_launches = inner_launches + 4;
+    if (stats) *stats = st;
+    return CLB_SUCCESS;
+}
+
+int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                        clb_spgemm_tuning *best, clb_spgemm_tuning *tried, double *ms, uint32_t max_tried,
+                        uint32_t *n_tried) {
+    if (!ctl || !best) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    std::vector<clb_spgemm_tuning> cand;
+    for (uint32_t form : {0u, 1u})
+        for (uint32_t bmin : {4096u, 1024u, 256u})
+            for (uint32_t bthr : {1024u, 256u})
+                for (uint32_t wmax : {256u, 64u}) {
+                    clb_spgemm_tuning t;
+                    clb_spgemm_tuning_default(&t);
+                    t.form = form;
+                    t.bitmap_min = bmin;
+                    t.bitmap_threads = bthr;
+                    t.warp_max = wmax;
+                    cand.push_back(t);
+                }
+    cudaEvent_t e0, e1;
+    CLB_TRY_CUDA(cudaEventCreate(&e0), CLB_RUN_KERNEL_FAILURE);
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(CLB_RUN_KERNEL_FAILURE, "event");
+    }
+    std::vector<clb_dcsr> out(std::max<uint32_t>(count, 1));
+    double best_ms = 1e300;
+    int rc = CLB_SUCCESS;
+    uint32_t n = 0;
+    for (const auto &t : cand) {
+        double tms = 1e300;
+        for (int rep = 0; rep < 2 && rc == CLB_SUCCESS; ++rep) {  // first run warms up
+            cudaEventRecord(e0, ctl->stream);
+            rc = clb_dcsr_spgemm_batched(ctl, count, a, b, out.data(), &t, nullptr);
+            cudaEventRecord(e1, ctl->stream);
+            cudaEventSynchronize(e1);
+            float f = 0.f;
+            cudaEventElapsedTime(&f, e0, e1);
+            for (uint32_t k = 0; k < count; ++k) clb_dcsr_release(ctl, &out[k]);
+            if (rep == 1) tms = f;
+        }
+        if (rc != CLB_SUCCESS) break;
+        if (n < max_tried) {
+            if (tried) tried[n] = t;
+            if (ms) ms[n] = tms;
+        }
+        ++n;
+        if (tms < best_ms) {
+            best_ms = tms;
+            *best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (n_tried) *n_tried = n;
+    return rc;
+}
+
+}  // extern "C"

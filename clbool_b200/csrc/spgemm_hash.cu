@@ -92,7 +92,7 @@ int validate_spgemm(const clb_dcsr &A, const clb_dcsr &B) {
 }
 
 int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
-                         clb_spgemm_stats *stats) {
+                         clb_spgemm_stats *stats, const Tuning &t) {
     clb_dcsr C{};
     C.nrows = A.nrows;
     C.ncols = B.ncols;
@@ -124,12 +124,12 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     CLB_RETURN_IF(off.alloc(ctl, n));
 
     CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, scal.ptr + 0));
-    CLB_RETURN_IF(launch_binning(ctl, work.ptr, nullptr, n, B.ncols, info.ptr, list.ptr, flags.ptr));
+    CLB_RETURN_IF(launch_binning(ctl, work.ptr, nullptr, n, B.ncols, info.ptr, list.ptr, flags.ptr, t));
     CLB_TRY_CUDA(cudaMemsetAsync(row_nnz.ptr, 0, n * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
 
     BinLists bl{list.ptr, info.ptr};
     RowOut sym{row_nnz.ptr, nullptr, nullptr, nullptr, nullptr, ctl->d_status};
-    CLB_RETURN_IF(launch_accumulators(ctl, false, bl, a, b, sym, B.ncols, n));
+    CLB_RETURN_IF(launch_accumulators(ctl, false, bl, a, b, sym, B.ncols, n, t));
 
     CLB_RETURN_IF(scan_u32_to_u64(ctl, row_nnz.ptr, off.ptr, n, scal.ptr + 1));
     CLB_RETURN_IF(scan_u32_inplace(ctl, flags.ptr, n, scal.ptr + 2));
@@ -158,7 +158,7 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     CLB_RETURN_IF(launch_assemble(ctl, work.ptr, flags.ptr, off.ptr, A.rows, n, c_rpt.ptr, c_rows.ptr, nzr, nnz));
 
     RowOut num{nullptr, off.ptr, nullptr, nullptr, c_cols.ptr, ctl->d_status};
-    CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n));
+    CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t));
     CLB_RETURN_IF(check_status(ctl, "matrix_multiplication_hash"));
 
     C.nnz = nnz;

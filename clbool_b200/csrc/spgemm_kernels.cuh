@@ -46,24 +46,42 @@ enum Bin : int {
 };
 
 // Rows with at most this many products never reach the bitmap accumulator
-// when binned by products (the ESC form): the CTA ESC kernels take them.
+// under the default tuning (the CTA hash / CTA ESC kernels take them).
 constexpr uint32_t ESC_MAX_PRODUCTS = 4096;
 
+// Accumulator tuning (all settings give the same C):
+//   warp_max       rows with at most this many products go to the warp ESC
+//                  kernels (32, 64, 128 or 256);
+//   bitmap_min     rows with more products go to the bitmap kernel (at most
+//                  ESC_MAX_PRODUCTS; lower values pay off when the bitmap is
+//                  narrow, i.e. few columns);
+//   bitmap_threads threads per bitmap row (256, 512 or 1024).
+struct Tuning {
+    uint32_t warp_max = 256;
+    uint32_t bitmap_min = ESC_MAX_PRODUCTS;
+    uint32_t bitmap_threads = 1024;
+};
+
 // Bin of a row from its product count and its distinct-column bound
-// (min(products, ncols), or a learned capacity).
-__host__ __device__ __forceinline__ int bin_of(uint64_t products, uint64_t distinct_bound) {
+// (min(products, ncols), or a capacity).
+__host__ __device__ __forceinline__ int bin_of(uint64_t products, uint64_t distinct_bound, uint32_t warp_max,
+                                               uint32_t bitmap_min) {
     if (products == 0) return BIN_NONE;
-    if (products <= 32) return BIN_W1;
-    if (products <= 64) return BIN_W2;
-    if (products <= 128) return BIN_W4;
-    if (products <= 256) return BIN_W8;
+    if (products <= warp_max) {
+        if (products <= 32) return BIN_W1;
+        if (products <= 64) return BIN_W2;
+        if (products <= 128) return BIN_W4;
+        return BIN_W8;
+    }
+    if (products > bitmap_min) {
+        if (products > (1u << 20)) return BIN_BMP_XL;
+        if (products > (1u << 17)) return BIN_BMP_L;
+        return BIN_BMP;
+    }
     if (distinct_bound <= 512) return BIN_H1K;
     if (distinct_bound <= 1024) return BIN_H2K;
     if (distinct_bound <= 2048) return BIN_H4K;
-    if (distinct_bound <= 4096) return BIN_H8K;
-    if (products > (1u << 20)) return BIN_BMP_XL;
-    if (products > (1u << 17)) return BIN_BMP_L;
-    return BIN_BMP;
+    return BIN_H8K;
 }
 
 // Row lists of all bins packed in one array; info[b] = count of bin b,
@@ -423,8 +441,6 @@ __global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AVie
 }
 
 // ----------------------------------------------------------- CTA bitmap ----
-constexpr int BMP_NT = 1024;
-constexpr int BMP_NW = BMP_NT / 32;
 constexpr int BMP_ECH = 1024;                 // A entries staged per chunk
 constexpr uint32_t BMP_MAX_WORDS = 32768;     // 128 KB: 2^20 columns per chunk
 constexpr int BMP_U = 8;                      // B-column loads in flight per lane
@@ -444,8 +460,8 @@ inline uint32_t bitmap_words(uint64_t ncols) {
 // Dynamic shared memory of the bitmap kernel (32-bit words): bitmap W |
 // entry stage (B row start, length, unit prefix) | non-empty step list and
 // output offsets | per-warp output staging.
-inline size_t bitmap_smem_bytes(uint32_t W) {
-    return ((size_t)W + 3 * BMP_ECH + 1 + 2 * BMP_MAX_STEPS + 1 + BMP_NW * BMP_STAGE) * 4;
+inline size_t bitmap_smem_bytes(uint32_t W, int nt) {
+    return ((size_t)W + 3 * BMP_ECH + 1 + 2 * BMP_MAX_STEPS + 1 + (size_t)(nt / 32) * BMP_STAGE) * 4;
 }
 
 // Position of the n-th (0-based) set bit of w; w has more than n set bits.
@@ -663,8 +679,8 @@ __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b
 // bitmap from there, writing into the warp's staging buffer, which the warp
 // copies to C with coalesced stores.  Cost follows the non-empty steps and
 // the output, not the bitmap width, and is even across lanes.
-template <bool NUMERIC, bool MULTI>
-__global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int bin_lo, int bin_hi, AView a, BRows b,
+template <bool NUMERIC, bool MULTI, int BMP_NT>
+__global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLists bl, int bin_lo, int bin_hi, AView a, BRows b,
                                                                RowOut o, uint64_t ncols, uint32_t W,
                                                                uint32_t *counter) {
     extern __shared__ __align__(16) uint32_t smem[];
@@ -674,7 +690,7 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
     uint32_t *s_upre = s_len + BMP_ECH;             // BMP_ECH + 1
     uint32_t *s_list = s_upre + BMP_ECH + 1;        // BMP_MAX_STEPS
     uint32_t *s_soff = s_list + BMP_MAX_STEPS;      // BMP_MAX_STEPS + 1
-    uint32_t *s_stage = s_soff + BMP_MAX_STEPS + 1; // BMP_NW * BMP_STAGE
+    uint32_t *s_stage = s_soff + BMP_MAX_STEPS + 1; // (BMP_NT / 32) * BMP_STAGE
     __shared__ uint32_t scratch[33];
     __shared__ uint32_t s_slot, s_next;
     __shared__ unsigned long long s_spill;
@@ -687,7 +703,9 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
     __syncthreads();
     const uint32_t lane = lane_id(), wi = warp_id();
     const uint64_t chunk_cols = (uint64_t)W * 32;
-    const uint32_t nwg = W >> 5;  // 32-word groups, one per counting thread (<= BMP_NT)
+    const uint32_t nsteps = W / BMP_STEP_WORDS;  // <= BMP_MAX_STEPS
+    constexpr int TPS = BMP_NT / (int)BMP_MAX_STEPS;  // counting threads per step
+    static_assert(TPS >= 1 && TPS <= 32 && (TPS & (TPS - 1)) == 0, "block size");
     uint4 *bm4 = reinterpret_cast<uint4 *>(bm);
     uint32_t *const stage = s_stage + wi * BMP_STAGE;
     for (;;) {
@@ -719,24 +737,26 @@ __global__ void __launch_bounds__(BMP_NT, 1) bitmap_cta_kernel(BinLists bl, int 
                 total += block_sum<uint32_t, BMP_NT>(mine, scratch);
                 continue;
             }
-            uint32_t c32 = 0;
-            if (threadIdx.x < nwg) {
-                const uint4 *p4 = bm4 + threadIdx.x * 8;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
+            // TPS threads count one 128-word step (32 uint4), thread TPS*s
+            // ends up holding step s
+            uint32_t scnt = 0;
+            if (threadIdx.x / TPS < nsteps) {
+                const uint4 *p4 = bm4 + (threadIdx.x / TPS) * 32 + (threadIdx.x % TPS) * (32 / TPS);
+#pragma unroll 8
+                for (int k = 0; k < 32 / TPS; ++k) {
                     const uint4 x = p4[k];
-                    c32 += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+                    scnt += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
                 }
             }
-            uint32_t scnt = c32 + __shfl_xor_sync(0xFFFFFFFFu, c32, 1);
-            scnt += __shfl_xor_sync(0xFFFFFFFFu, scnt, 2);
-            if ((threadIdx.x & 3u) != 0) scnt = 0;  // thread 4s holds step s
+#pragma unroll
+            for (int d = 1; d < TPS; d <<= 1) scnt += __shfl_xor_sync(0xFFFFFFFFu, scnt, d);
+            if ((threadIdx.x % TPS) != 0) scnt = 0;
             // counts <= 4096 per step, <= 2^20 per chunk; flags <= 256 < 2^11
             uint32_t ptot;
             const uint32_t ex = block_exclusive_scan<uint32_t, BMP_NT>((scnt << 11) | (scnt ? 1u : 0u), scratch, &ptot);
             const uint32_t ctot = ptot >> 11, nlist = ptot & 0x7FFu;
             if (scnt) {
-                s_list[ex & 0x7FFu] = threadIdx.x >> 2;
+                s_list[ex & 0x7FFu] = threadIdx.x / TPS;
                 s_soff[ex & 0x7FFu] = ex >> 11;
             }
             if (threadIdx.x == 0) {

@@ -11,6 +11,7 @@ constexpr int BIN_NT = 256;
 
 __global__ void __launch_bounds__(BIN_NT) bin_count_kernel(const uint32_t *__restrict__ work,
                                                            const uint32_t *__restrict__ cap, uint64_t n, uint64_t ncols,
+                                                           uint32_t warp_max, uint32_t bitmap_min,
                                                            uint32_t *__restrict__ info, uint32_t *__restrict__ flags) {
     __shared__ uint32_t hist[NUM_BINS];
     if (threadIdx.x < NUM_BINS) hist[threadIdx.x] = 0;
@@ -18,7 +19,7 @@ __global__ void __launch_bounds__(BIN_NT) bin_count_kernel(const uint32_t *__res
     for (uint64_t i = (uint64_t)blockIdx.x * BIN_NT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * BIN_NT) {
         uint32_t p = work[i];
         uint64_t bound = cap ? (uint64_t)cap[i] : (p < ncols ? (uint64_t)p : ncols);
-        int bin = bin_of(p, bound);
+        int bin = bin_of(p, bound, warp_max, bitmap_min);
         atomicAdd(&hist[bin], 1u);
         flags[i] = p > 0 ? 1u : 0u;
     }
@@ -28,7 +29,8 @@ __global__ void __launch_bounds__(BIN_NT) bin_count_kernel(const uint32_t *__res
 
 __global__ void __launch_bounds__(BIN_NT) bin_scatter_kernel(const uint32_t *__restrict__ work,
                                                              const uint32_t *__restrict__ cap, uint64_t n,
-                                                             uint64_t ncols, uint32_t *__restrict__ info,
+                                                             uint64_t ncols, uint32_t warp_max, uint32_t bitmap_min,
+                                                             uint32_t *__restrict__ info,
                                                              uint32_t *__restrict__ list) {
     __shared__ uint32_t boff[NUM_BINS];
     if (threadIdx.x == 0) {
@@ -46,7 +48,7 @@ __global__ void __launch_bounds__(BIN_NT) bin_scatter_kernel(const uint32_t *__r
         if (i < n) {
             uint32_t p = work[i];
             uint64_t bound = cap ? (uint64_t)cap[i] : (p < ncols ? (uint64_t)p : ncols);
-            bin = bin_of(p, bound);
+            bin = bin_of(p, bound, warp_max, bitmap_min);
         }
         // warp-aggregated reservation per bin
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
@@ -110,41 +112,49 @@ int launch_hash(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, 
     return CLB_SUCCESS;
 }
 
-template <bool NUM, bool MULTI>
+template <bool NUM, bool MULTI, int NT>
 int launch_bitmap_t(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
                     uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name) {
     const uint32_t W = bitmap_words(ncols);
-    const size_t smem = bitmap_smem_bytes(W);
-    auto kern = bitmap_cta_kernel<NUM, MULTI>;
+    const size_t smem = bitmap_smem_bytes(W, NT);
+    auto kern = bitmap_cta_kernel<NUM, MULTI, NT>;
     CLB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  CLB_RUN_KERNEL_FAILURE);
-    int occ = occupancy(kern, BMP_NT, smem);
+    int occ = occupancy(kern, NT, smem);
     unsigned grid = persistent_grid(ctl, occ, nmax);
     ProfScope ps(ctl, name);
-    kern<<<grid, BMP_NT, smem, ctl->stream>>>(bl, BIN_BMP_XL, BIN_BMP, a, b, o, ncols, W, counter);
+    kern<<<grid, NT, smem, ctl->stream>>>(bl, BIN_BMP_XL, BIN_BMP, a, b, o, ncols, W, counter);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
 }
 
+template <bool NUM, int NT>
+int launch_bitmap_nt(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
+                     uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name) {
+    const bool multi = ncols > (uint64_t)bitmap_words(ncols) * 32;
+    return multi ? launch_bitmap_t<NUM, true, NT>(ctl, bl, a, b, o, ncols, nmax, counter, name)
+                 : launch_bitmap_t<NUM, false, NT>(ctl, bl, a, b, o, ncols, nmax, counter, name);
+}
+
 template <bool NUM>
 int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
-                  uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name) {
-    const bool multi = ncols > (uint64_t)bitmap_words(ncols) * 32;
-    return multi ? launch_bitmap_t<NUM, true>(ctl, bl, a, b, o, ncols, nmax, counter, name)
-                 : launch_bitmap_t<NUM, false>(ctl, bl, a, b, o, ncols, nmax, counter, name);
+                  uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name, uint32_t threads) {
+    if (threads <= 256) return launch_bitmap_nt<NUM, 256>(ctl, bl, a, b, o, ncols, nmax, counter, name);
+    if (threads <= 512) return launch_bitmap_nt<NUM, 512>(ctl, bl, a, b, o, ncols, nmax, counter, name);
+    return launch_bitmap_nt<NUM, 1024>(ctl, bl, a, b, o, ncols, nmax, counter, name);
 }
 
 template <bool NUM>
 int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o, uint64_t ncols,
-               uint64_t nmax, bool hash_bins = true) {
+               uint64_t nmax, const Tuning &t, bool hash_bins = true) {
     // work counters of the dynamically scheduled launches
     Temp<uint32_t> ctr;
     CLB_RETURN_IF(ctr.alloc(ctl, 8));
     CLB_TRY_CUDA(cudaMemsetAsync(ctr.ptr, 0, 8 * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     // Heavy bins first so the long rows start early.
     CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, a, b, o, ncols, nmax, ctr.ptr + 0,
-                                     NUM ? "bitmap_numeric" : "bitmap_symbolic"));
+                                     NUM ? "bitmap_numeric" : "bitmap_symbolic", t.bitmap_threads));
     if (hash_bins) {
         CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax, ctr.ptr + 1,
                                                    NUM ? "hash8k_numeric" : "hash8k_symbolic")));
@@ -165,25 +175,26 @@ int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRow
 }  // namespace
 
 int launch_binning(clb_controls *ctl, const uint32_t *work, const uint32_t *cap, uint64_t n, uint64_t ncols,
-                   uint32_t *info, uint32_t *list, uint32_t *flags) {
+                   uint32_t *info, uint32_t *list, uint32_t *flags, const Tuning &t) {
     CLB_TRY_CUDA(cudaMemsetAsync(info, 0, 2 * NUM_BINS * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     unsigned grid = persistent_grid(ctl, 8, ceil_div_u(n, BIN_NT));
     ProfScope ps(ctl, "binning");
-    bin_count_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, info, flags);
-    bin_scatter_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, info, list);
+    bin_count_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, t.warp_max, t.bitmap_min, info, flags);
+    bin_scatter_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, t.warp_max, t.bitmap_min, info, list);
     ctl->launches += 2;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
 }
 
 int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, const AView &a, const BRows &b,
-                        const RowOut &o, uint64_t ncols, uint64_t nmax) {
-    return numeric ? launch_all<true>(ctl, bl, a, b, o, ncols, nmax) : launch_all<false>(ctl, bl, a, b, o, ncols, nmax);
+                        const RowOut &o, uint64_t ncols, uint64_t nmax, const Tuning &t) {
+    return numeric ? launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t)
+                   : launch_all<false>(ctl, bl, a, b, o, ncols, nmax, t);
 }
 
 int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
-                               const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins) {
-    return launch_all<true>(ctl, bl, a, b, o, ncols, nmax, hash_bins);
+                               const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins, const Tuning &t) {
+    return launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t, hash_bins);
 }
 
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,

@@ -199,6 +199,13 @@ unsigned grid_for(const clb_controls *ctl, uint64_t n, int per_sm = 16) {
 
 }  // namespace
 
+int launch_upper_bound_caps(clb_controls *ctl, const uint32_t *work, uint64_t n, uint64_t ncols, uint32_t *cap) {
+    upper_bound_cap_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(work, n, ncols, cap);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
 // The accumulators of the ESC form for rows of up to 4096 products.
 int launch_esc_accumulators(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
                             const uint32_t *work, uint64_t nmax) {
@@ -219,7 +226,7 @@ int launch_esc_accumulators(clb_controls *ctl, const BinLists &bl, const AView &
 // hash accumulators.
 int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                        const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
-                       clb_spgemm_stats *st, uint64_t arena_div) {
+                       clb_spgemm_stats *st, uint64_t arena_div, const Tuning &t) {
     const uint64_t n = A.nzr;
     clb_dcsr C{};
     C.nrows = A.nrows;
@@ -239,7 +246,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     CLB_TRY_CUDA(cudaMemsetAsync(ovf.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
 
     // bins: ESC by products (CTA ESC up to 4096), learned by capacity
-    CLB_RETURN_IF(launch_binning(ctl, work, esc ? work : cap, n, B.ncols, info.ptr, list.ptr, flags.ptr));
+    CLB_RETURN_IF(launch_binning(ctl, work, esc ? work : cap, n, B.ncols, info.ptr, list.ptr, flags.ptr, t));
     CLB_RETURN_IF(scan_u32_inplace(ctl, flags.ptr, n, scal.ptr + 0));        // C row positions, nzr
     CLB_RETURN_IF(scan_u32_to_u64(ctl, cap, slot_off.ptr, n, scal.ptr + 1));  // slots, capacity
     uint64_t h[2];
@@ -274,9 +281,9 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
         // warp ESC and bitmap rows through the shared launcher's bins; rows of
         // the hash bins go to the CTA ESC kernels instead.
         CLB_RETURN_IF(launch_esc_accumulators(ctl, bl, a, b, num, work, n));
-        CLB_RETURN_IF(launch_accumulators_subset(ctl, bl, a, b, num, B.ncols, n, /*hash_bins=*/false));
+        CLB_RETURN_IF(launch_accumulators_subset(ctl, bl, a, b, num, B.ncols, n, /*hash_bins=*/false, t));
     } else {
-        CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n));
+        CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t));
     }
 
     // the fallback below resets the device status word: check it first
@@ -319,7 +326,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
         CLB_CHECK_LAUNCH();
         clb_dcsr subA{A.nrows, A.ncols, sub_nnz, novf, sub_rpt.ptr, sub_rows.ptr, sub_cols.ptr};
         const uint32_t launches = ctl->launches;
-        CLB_RETURN_IF(spgemm_hash_two_pass(ctl, subA, B, &sub_c, nullptr));
+        CLB_RETURN_IF(spgemm_hash_two_pass(ctl, subA, B, &sub_c, nullptr, t));
         ctl->launches += launches;
         if (sub_c.nzr != novf) {
             clb_dcsr_release(ctl, &sub_c);
@@ -406,9 +413,7 @@ int clb_dcsr_spgemm_esc(clb_controls *ctl, const clb_dcsr *a_, const clb_dcsr *b
     CLB_RETURN_IF(tot.alloc(ctl, 1));
     CLB_TRY_CUDA(cudaMemsetAsync(tot.ptr, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
     CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, tot.ptr));
-    upper_bound_cap_kernel<<<grid_for(ctl, A.nzr), 256, 0, ctl->stream>>>(work.ptr, A.nzr, B.ncols, cap.ptr);
-    ctl->launches += 1;
-    CLB_CHECK_LAUNCH();
+    CLB_RETURN_IF(launch_upper_bound_caps(ctl, work.ptr, A.nzr, B.ncols, cap.ptr));
     uint64_t products = 0;
     CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &products, 1));
     int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st, 0);

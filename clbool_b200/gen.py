@@ -38,26 +38,30 @@ def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c:
 
 
 def _rows_without_replacement(lens: np.ndarray, ncols: int, rng: np.random.Generator):
-    lens = np.minimum(lens.astype(np.int64), ncols)
-    total = int(lens.sum())
-    rows = np.repeat(np.arange(lens.size, dtype=np.uint32), lens)
-    cols = np.empty(total, dtype=np.uint32)
-    off = 0
-    # Rows are short relative to ncols: draw with replacement and redraw the
-    # duplicates until every row has distinct columns.
-    for i, L in enumerate(lens):
-        if L == 0:
-            continue
-        if L * 4 > ncols:
-            pick = rng.choice(ncols, size=L, replace=False)
-        else:
-            pick = np.unique(rng.integers(0, ncols, size=L + L // 4 + 4))
-            while pick.size < L:
-                pick = np.unique(np.concatenate([pick, rng.integers(0, ncols, size=L)]))
-            pick = rng.permutation(pick)[:L]
-        cols[off:off + L] = np.sort(pick)
-        off += L
-    return rows, cols
+    """Sorted COO with exactly lens[i] distinct columns in row i (uniform
+    without replacement), vectorised: draw with replacement, drop duplicate
+    (row, col) pairs, redraw the missing ones until every row is full."""
+    lens = np.minimum(np.asarray(lens, dtype=np.int64), ncols)
+    nrows = lens.size
+    # rows longer than half the columns: drawn one by one without replacement
+    dense = np.flatnonzero(lens * 2 > ncols)
+    dkeys = [r * ncols + np.sort(rng.choice(ncols, size=int(lens[r]), replace=False)) for r in dense]
+    sparse = lens.copy()
+    sparse[dense] = 0
+    rows = np.repeat(np.arange(nrows, dtype=np.int64), sparse)
+    keys = np.unique(rows * ncols + rng.integers(0, ncols, size=rows.size))
+    for _ in range(200):
+        have = np.bincount(keys // ncols, minlength=nrows)
+        short = sparse - have
+        if not short.any():
+            break
+        extra = np.repeat(np.arange(nrows, dtype=np.int64), short)
+        keys = np.unique(np.concatenate([keys, extra * ncols + rng.integers(0, ncols, size=extra.size)]))
+    else:
+        raise RuntimeError("row generation did not converge")
+    if dkeys:
+        keys = np.sort(np.concatenate([keys] + dkeys))
+    return (keys // ncols).astype(np.uint32), (keys % ncols).astype(np.uint32)
 
 
 def poisson_rows(nrows: int, ncols: int, lam: float = 8.0, seed: int = 1):

@@ -257,6 +257,42 @@ CLB_API int clb_sizer_train(clb_sizer *sizer, const float *features, const float
 CLB_API int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_sizer *sizer,
                                     float margin_log2, float slack, clb_dcsr *c, clb_spgemm_stats *stats);
 
+/* ------------------------------------------------- tuning and batching -- */
+/* Not in the reference.  Accumulator tuning; every setting gives the same C.
+ *   form            0: exact two-pass (hash form), 1: one pass into
+ *                   upper-bound slots (ESC form) + compaction
+ *   warp_max        rows with at most this many products use the warp ESC
+ *                   kernels: 32, 64, 128 or 256 (threads per row: 32)
+ *   bitmap_min      rows with more products use the bitmap kernel: 256..4096
+ *                   (the rest use the CTA hash / CTA ESC kernels, whose table
+ *                   size follows the row's bound: 1K, 2K, 4K or 8K slots)
+ *   bitmap_threads  threads per bitmap row: 256, 512 or 1024
+ * Zero fields take the defaults (clb_spgemm_tuning_default). */
+typedef struct clb_spgemm_tuning {
+    uint32_t form;
+    uint32_t warp_max;
+    uint32_t bitmap_min;
+    uint32_t bitmap_threads;
+    uint32_t reserved[4];
+} clb_spgemm_tuning;
+CLB_API void clb_spgemm_tuning_default(clb_spgemm_tuning *tuning);
+/* C = A*B with a tuning (NULL = defaults, i.e. clb_dcsr_spgemm_hash). */
+CLB_API int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b,
+                                  const clb_spgemm_tuning *tuning, clb_dcsr *c, clb_spgemm_stats *stats);
+/* c[k] = a[k] * b[k] for k < count, all pairs in one pass: the pairs are
+ * stacked block-diagonally and multiplied by one set of launches (the launch
+ * count does not grow with the batch), then C is split per pair.  Each c[k]
+ * owns its buffers.  stats (optional) covers the whole batch. */
+CLB_API int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                                    clb_dcsr *c, const clb_spgemm_tuning *tuning, clb_spgemm_stats *stats);
+/* Times the batched product under every candidate tuning (24: form x
+ * bitmap_min x bitmap_threads x warp_max) on the given pairs and returns the
+ * fastest in *best; tried/ms (optional, max_tried entries) receive each
+ * candidate and its device time in ms, *n_tried their number. */
+CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                                clb_spgemm_tuning *best, clb_spgemm_tuning *tried, double *ms, uint32_t max_tried,
+                                uint32_t *n_tried);
+
 /* Products per A row (count_workload, dcsr_matrix_multiplication.cpp:388-404):
  * workload has a->nzr entries in device memory; *total = their sum. */
 CLB_API int clb_dcsr_workload(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, uint32_t *workload,
