@@ -123,20 +123,21 @@ def shard_rows(rpt_work: np.ndarray, world: int, rank: int) -> tuple[int, int]:
 
 
 def bin_of(p: np.ndarray, bound: np.ndarray) -> np.ndarray:
-    """The accumulator bin of every row (mirrors bin_of in spgemm_kernels.cuh)."""
+    """The accumulator bin of every row under the default tuning (mirrors
+    bin_of in spgemm_kernels.cuh)."""
     b = np.full(p.shape, 11, np.int32)
     b[p > (1 << 17)] = 10
     b[p > (1 << 20)] = 9
     for lim, k in ((4096, 8), (2048, 7), (1024, 6), (512, 5)):
-        b[bound <= lim] = k
-    for lim, k in ((256, 4), (128, 3), (64, 2), (32, 1)):
+        b[(p <= 4096) & (bound <= lim)] = k
+    for lim, k in ((256, 4), (128, 3), (64, 2), (32, 1), (16, 13), (8, 12)):
         b[p <= lim] = k
     b[p == 0] = 0
     return b
 
 
 KERNEL_BIN = {"bitmap": (9, 10, 11), "hash8k": 8, "hash4k": 7, "hash2k": 6, "hash1k": 5, "cta_esc4096": 8,
-              "cta_esc2048": 7, "cta_esc1024": 6, "cta_esc512": 5, "esc256": 4, "esc128": 3,
+              "cta_esc2048": 7, "cta_esc1024": 6, "cta_esc512": 5, "esc256": 4, "esc128": 3, "esc16": 13, "esc8": 12,
               "esc64": 2, "esc32": 1}
 
 
@@ -495,6 +496,119 @@ def run_reference(args) -> dict:
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# ------------------------------------------------------ secondary workloads --
+def _event_ms(stream, fn, reps: int):
+    """Per-call device time (CUDA events on the library's stream), median."""
+    import torch
+    out = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return statistics.median(out)
+
+
+def run_batch(args) -> dict:
+    """256 independent pairs (n log-uniform in [2^10, 2^18], power-law rows:
+    exponent 2.1, mean 6, at most 4096; seed per pair): one batched call
+    (default and autotuned tuning) against one call per pair."""
+    import torch
+
+    import clbool_b200 as cb
+    from clbool_b200 import gen
+    ctl = cb.create_controls(0, 0)
+    stream = torch.cuda.ExternalStream(ctl.stream, device="cuda:0")
+    rng = np.random.default_rng(17)
+    ns = np.exp(rng.uniform(np.log(1 << 10), np.log(1 << 18), size=args.pairs)).astype(int)
+    pairs = []
+    for k, n in enumerate(ns):
+        n = int(n)
+        mats = []
+        for s in (2 * k + 1, 2 * k + 2):
+            r, c = gen.power_law_rows(n, n, 2.1, 6.0, 4096, seed=1000 + s)
+            rpt, rows, cols = gen.to_dcsr(r, c)
+            mats.append(cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(rpt, rows, cols), n))
+        pairs.append(tuple(mats))
+    products = sum(cb.dcsr.workload(ctl, a, b)[1] for a, b in pairs)
+    default = cb.dcsr.tuning()
+    best, tried = cb.dcsr.autotune(ctl, pairs)
+    st = {}
+
+    def batched(t):
+        def f():
+            outs = cb.dcsr.matrix_multiplication_batched(ctl, pairs, tune=t, stats=st)
+            del outs
+        return f
+
+    def sequential():
+        for a, b in pairs:
+            c = cb.dcsr.matrix_multiplication_hash(ctl, None, a, b)
+            del c
+
+    for _ in range(args.warmup):
+        batched(best)()
+        sequential()
+    ms_best = _event_ms(stream, batched(best), args.steps)
+    ms_default = _event_ms(stream, batched(default), args.steps)
+    ms_seq = _event_ms(stream, sequential, max(1, args.steps // 2))
+    batched(best)()
+    return {"metric": METRIC, "workload": f"batch{args.pairs}_powerlaw", "value": products / (ms_best / 1e3),
+            "unit": UNIT, "ms_per_step": ms_best, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
+            "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"batch{args.pairs}_powerlaw", "pairs": args.pairs, "n_min": int(ns.min()),
+                       "n_max": int(ns.max()), "products": int(products), "nnz_C": int(st.get("nnz", 0)),
+                       "row_lengths": "power law 2.1, mean 6, max 4096"},
+            "autotuned": best.as_dict(), "default_ms": ms_default, "sequential_ms": ms_seq,
+            "batched_over_sequential": ms_seq / ms_best,
+            "kernel_launches_per_batch": st.get("kernel_launches"),
+            "candidates_ms": sorted(((t, round(m, 3)) for t, m in tried), key=lambda x: x[1])}
+
+
+def run_small(args) -> dict:
+    """4096 x 4096, Poisson(8) rows (columns uniform without replacement, seeds
+    1 and 2): latency of one A*B (each form) and of one COO A+B."""
+    import torch
+
+    import clbool_b200 as cb
+    from clbool_b200 import gen
+    ctl = cb.create_controls(0, 0)
+    stream = torch.cuda.ExternalStream(ctl.stream, device="cuda:0")
+    n = 4096
+    mats = []
+    for seed in (1, 2):
+        r, c = gen.poisson_rows(n, n, 8.0, seed=seed)
+        mats.append((r, c))
+    (ra, ca), (rb, cb_) = mats
+    A = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(*gen.to_dcsr(ra, ca)), n)
+    B = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(*gen.to_dcsr(rb, cb_)), n)
+    Ac = cb.matrix_coo.from_host(ctl, ra, ca, n, n)
+    Bc = cb.matrix_coo.from_host(ctl, rb, cb_, n, n)
+    products = cb.dcsr.workload(ctl, A, B)[1]
+    best, _ = cb.dcsr.autotune(ctl, [(A, B)])
+    out = {}
+    calls = {
+        "hash_two_pass": lambda st: cb.dcsr.matrix_multiplication_hash(ctl, None, A, B, stats=st),
+        "esc_single_pass": lambda st: cb.dcsr.matrix_multiplication(ctl, None, A, B, stats=st),
+        "autotuned": lambda st: cb.dcsr.matrix_multiplication_tuned(ctl, None, A, B, best, stats=st),
+        "coo_add": lambda st: cb.coo.matrix_addition(ctl, None, Ac, Bc),
+    }
+    for name, f in calls.items():
+        st = {}
+        for _ in range(max(3, args.warmup)):
+            f(st)
+        ms = _event_ms(stream, lambda: f(st), max(20, args.steps))
+        out[name] = {"us": ms * 1e3, "launches": st.get("kernel_launches")}
+        if name != "coo_add":
+            out[name]["products_per_s"] = products / (ms / 1e3)
+    out["autotuned"]["tuning"] = best.as_dict()
+    return {"metric": METRIC, "workload": "poisson4096", "unit": UNIT, "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": "poisson4096_AxB", "n": n, "lambda": 8, "products": int(products),
+                       "nnz_A": int(ra.size), "nnz_B": int(rb.size)}, "calls": out}
+
+
 # --------------------------------------------------------------------- main --
 def main():
     ap = argparse.ArgumentParser()
@@ -512,7 +626,13 @@ def main():
                     help="left operand = this seeded fraction of A's stored rows (profiling captures)")
     ap.add_argument("--ref-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="rmat", choices=["rmat", "batch", "poisson4096"],
+                    help="rmat: the headline A*A; batch / poisson4096: secondary workloads (own JSON line)")
+    ap.add_argument("--pairs", type=int, default=256)
     args = ap.parse_args()
+    if args.workload != "rmat":
+        print(json.dumps(run_batch(args) if args.workload == "batch" else run_small(args)), flush=True)
+        return
     if args.form is None:
         args.form = "learned" if os.path.exists(args.sizer) else "two_pass"
 

@@ -40,18 +40,19 @@ class clb_spgemm_stats(C.Structure):
 
     def as_dict(self) -> dict:
         return {"products": self.products, "nnz": self.nnz, "nzr": self.nzr,
-                "rows_per_bin": list(self.rows_per_bin)[:12], "fallback_rows": self.fallback_rows,
+                "rows_per_bin": list(self.rows_per_bin)[:14], "fallback_rows": self.fallback_rows,
                 "capacity": self.capacity, "kernel_launches": self.kernel_launches,
                 "spilled_rows": self.spilled_rows}
 
 
 class clb_spgemm_tuning(C.Structure):
     _fields_ = [("form", C.c_uint32), ("warp_max", C.c_uint32), ("bitmap_min", C.c_uint32),
-                ("bitmap_threads", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("bitmap_threads", C.c_uint32), ("small_lanes", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
     def as_dict(self) -> dict:
         return {"form": "two_pass" if self.form == 0 else "single_pass", "warp_max": self.warp_max,
-                "bitmap_min": self.bitmap_min, "bitmap_threads": self.bitmap_threads}
+                "bitmap_min": self.bitmap_min, "bitmap_threads": self.bitmap_threads,
+                "small_lanes": self.small_lanes}
 
 
 P = C.POINTER

@@ -14,8 +14,8 @@ from ._capi import clb_dcsr, clb_spgemm_stats, clb_spgemm_tuning, lib
 from .core import ClBoolException, Controls, check, matrix_dcsr
 
 
-def tuning(form: str | int = "two_pass", warp_max: int = 0, bitmap_min: int = 0,
-           bitmap_threads: int = 0) -> clb_spgemm_tuning:
+def tuning(form: str | int = "two_pass", warp_max: int = 0, bitmap_min: int = 0, bitmap_threads: int = 0,
+           small_lanes: int = 0) -> clb_spgemm_tuning:
     """A tuning; zero fields take the library defaults."""
     t = clb_spgemm_tuning()
     lib.clb_spgemm_tuning_default(C.byref(t))
@@ -26,6 +26,8 @@ def tuning(form: str | int = "two_pass", warp_max: int = 0, bitmap_min: int = 0,
         t.bitmap_min = bitmap_min
     if bitmap_threads:
         t.bitmap_threads = bitmap_threads
+    if small_lanes:
+        t.small_lanes = small_lanes
     return t
 
 

@@ -330,9 +330,12 @@ int clb_sizer_create(clb_controls *ctl, uint64_t seed, clb_sizer **out) {
     for (int k = 0; k < H * F; ++k) h[OFF_W1 + k] = uni(std::sqrt(6.0f / F));
     for (int k = 0; k < H * H; ++k) h[OFF_W2 + k] = uni(std::sqrt(6.0f / H));
     for (int k = 0; k < H; ++k) h[OFF_W3 + k] = uni(std::sqrt(3.0f / H));
-    CLB_TRY_CUDA(cudaMemcpy(s->params, h.data(), NPARAM * 4, cudaMemcpyHostToDevice), CLB_WRITE_BUFFER_ERROR);
-    CLB_TRY_CUDA(cudaMemset(s->m, 0, NPARAM * 4), CLB_RUN_KERNEL_FAILURE);
-    CLB_TRY_CUDA(cudaMemset(s->v, 0, NPARAM * 4), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemcpyAsync(s->params, h.data(), NPARAM * 4, cudaMemcpyHostToDevice, ctl->stream),
+                 CLB_WRITE_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    CLB_TRY_CUDA(cudaMemsetAsync(s->m, 0, NPARAM * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(s->v, 0, NPARAM * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
     *out = s;
     return CLB_SUCCESS;
 }
@@ -350,16 +353,20 @@ int clb_sizer_destroy(clb_sizer *s) {
 int clb_sizer_get_params(clb_sizer *s, float *host, size_t count) {
     if (!s || !host || count != (size_t)NPARAM) return fail(CLB_INVALID_ARGUMENT, "expected clb_sizer_num_params() floats");
     DeviceGuard g(s->ctl);
-    CLB_TRY_CUDA(cudaMemcpy(host, s->params, NPARAM * 4, cudaMemcpyDeviceToHost), CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(host, s->params, NPARAM * 4, cudaMemcpyDeviceToHost, s->ctl->stream),
+                 CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(s->ctl->stream), CLB_EVENT_WAITING_ERROR);
     return CLB_SUCCESS;
 }
 
 int clb_sizer_set_params(clb_sizer *s, const float *host, size_t count) {
     if (!s || !host || count != (size_t)NPARAM) return fail(CLB_INVALID_ARGUMENT, "expected clb_sizer_num_params() floats");
     DeviceGuard g(s->ctl);
-    CLB_TRY_CUDA(cudaMemcpy(s->params, host, NPARAM * 4, cudaMemcpyHostToDevice), CLB_WRITE_BUFFER_ERROR);
-    CLB_TRY_CUDA(cudaMemset(s->m, 0, NPARAM * 4), CLB_RUN_KERNEL_FAILURE);
-    CLB_TRY_CUDA(cudaMemset(s->v, 0, NPARAM * 4), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemcpyAsync(s->params, host, NPARAM * 4, cudaMemcpyHostToDevice, s->ctl->stream),
+                 CLB_WRITE_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemsetAsync(s->m, 0, NPARAM * 4, s->ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(s->v, 0, NPARAM * 4, s->ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaStreamSynchronize(s->ctl->stream), CLB_EVENT_WAITING_ERROR);
     s->step = 0;
     return CLB_SUCCESS;
 }
@@ -480,8 +487,11 @@ int clb_sizer_train(clb_sizer *s, const float *features, const float *targets, u
     uint64_t st = seed ? seed : 1;
     for (uint64_t i = n - 1; i > 0; --i) std::swap(perm[i], perm[splitmix(st) % (i + 1)]);
     std::vector<float> hf(n * F), ht(n), sf(n * F), stg(n);
-    CLB_TRY_CUDA(cudaMemcpy(hf.data(), features, n * F * 4, cudaMemcpyDeviceToHost), CLB_READ_BUFFER_ERROR);
-    CLB_TRY_CUDA(cudaMemcpy(ht.data(), targets, n * 4, cudaMemcpyDeviceToHost), CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(hf.data(), features, n * F * 4, cudaMemcpyDeviceToHost, ctl->stream),
+                 CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(ht.data(), targets, n * 4, cudaMemcpyDeviceToHost, ctl->stream),
+                 CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
     for (uint64_t i = 0; i < n; ++i) {
         memcpy(&sf[i * F], &hf[perm[i] * F], F * 4);
         stg[i] = ht[perm[i]];

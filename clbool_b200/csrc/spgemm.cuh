@@ -15,16 +15,18 @@ int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t 
 // flags[i] = 1 for rows with products (input of the C row-position scan).
 int launch_binning(clb_controls *ctl, const uint32_t *work, const uint32_t *cap, uint64_t n, uint64_t ncols,
                    uint32_t *info, uint32_t *list, uint32_t *flags, const Tuning &t = Tuning());
-// Runs every bin's accumulator kernel (symbolic or numeric).
+// Runs every bin's accumulator kernel (symbolic or numeric).  bin_rows
+// (host, optional): rows per bin; empty bins are then skipped.
 int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, const AView &a, const BRows &b,
-                        const RowOut &o, uint64_t ncols, uint64_t nrows_max, const Tuning &t = Tuning());
+                        const RowOut &o, uint64_t ncols, uint64_t nrows_max, const Tuning &t = Tuning(),
+                        const uint32_t *bin_rows = nullptr);
 // C.rpt/C.rows from the row flags' exclusive scan (pos) and the row offsets.
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
                     const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz);
 // Numeric accumulators without (hash_bins = false) the hash bins.
 int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
                                const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins,
-                               const Tuning &t = Tuning());
+                               const Tuning &t = Tuning(), const uint32_t *bin_rows = nullptr);
 // Single-pass forms (spgemm_single.cu): capacity slots, one numeric pass,
 // exact fallback for rows that outgrew their capacity, compaction.
 int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,

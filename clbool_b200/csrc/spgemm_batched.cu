@@ -30,14 +30,17 @@ struct PairDesc {
     uint64_t nzr, nnz;
     uint64_t nzr_off, nnz_off;  // position in the stacked matrix
     uint32_t row_add, col_add;  // added to row ids / column ids
+    uint32_t ncols;             // columns of the pair's product
 };
 
 constexpr int CAT_NT = 256;
 
 // Stacks the pairs' matrices: blockIdx.y = pair.
+// row_ncols (may be null): per stacked row, the columns of its pair's product.
 __global__ void __launch_bounds__(CAT_NT) stack_kernel(const PairDesc *__restrict__ d, uint64_t *__restrict__ rpt,
                                                        uint32_t *__restrict__ rows, uint32_t *__restrict__ cols,
-                                                       uint64_t total_nzr, uint64_t total_nnz) {
+                                                       uint32_t *__restrict__ row_ncols, uint64_t total_nzr,
+                                                       uint64_t total_nnz) {
     const PairDesc p = d[blockIdx.y];
     const uint64_t stride = (uint64_t)gridDim.x * CAT_NT;
     const uint64_t t0 = (uint64_t)blockIdx.x * CAT_NT + threadIdx.x;
@@ -45,6 +48,7 @@ __global__ void __launch_bounds__(CAT_NT) stack_kernel(const PairDesc *__restric
     for (uint64_t r = t0; r < p.nzr; r += stride) {
         rows[p.nzr_off + r] = p.rows[r] + p.row_add;
         rpt[p.nzr_off + r] = p.rpt[r] - base + p.nnz_off;
+        if (row_ncols) row_ncols[p.nzr_off + r] = p.ncols;
     }
     for (uint64_t j = t0; j < p.nnz; j += stride) cols[p.nnz_off + j] = p.cols[j] + p.col_add;
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) rpt[total_nzr] = total_nnz;
@@ -90,11 +94,13 @@ __global__ void __launch_bounds__(CAT_NT) split_kernel(const OutDesc *__restrict
     for (uint64_t j = t0; j < o.nnz; j += stride) o.cols[j] = ccols[o.j0 + j];
 }
 
+// Blocks per pair: enough for the largest pair to be copied with ~4 items
+// per thread; blocks of smaller pairs find nothing to do and exit.
 unsigned stack_grid_x(const clb_controls *ctl, uint64_t largest, uint32_t count) {
-    uint64_t gx = (largest + CAT_NT - 1) / CAT_NT;
-    const uint64_t cap = std::max<uint64_t>(1, (uint64_t)ctl->sm_count * 8 / std::max<uint32_t>(count, 1)) + 1;
-    gx = std::min<uint64_t>(std::max<uint64_t>(gx, 1), std::max<uint64_t>(cap, 4));
-    return (unsigned)gx;
+    (void)ctl;
+    (void)count;
+    const uint64_t gx = (largest + 4 * CAT_NT - 1) / (4 * CAT_NT);
+    return (unsigned)std::min<uint64_t>(std::max<uint64_t>(gx, 1), 65535);
 }
 
 Tuning to_tuning(const clb_spgemm_tuning *t) {
@@ -103,6 +109,7 @@ Tuning to_tuning(const clb_spgemm_tuning *t) {
     if (t->warp_max) r.warp_max = t->warp_max;
     if (t->bitmap_min) r.bitmap_min = t->bitmap_min;
     if (t->bitmap_threads) r.bitmap_threads = t->bitmap_threads;
+    if (t->small_lanes) r.small_lanes = t->small_lanes;
     return r;
 }
 
@@ -115,6 +122,8 @@ int check_tuning(const clb_spgemm_tuning *t) {
         return fail(CLB_INVALID_VALUE, "tuning.bitmap_min must be in [256, 4096]");
     if (t->bitmap_threads && t->bitmap_threads != 256 && t->bitmap_threads != 512 && t->bitmap_threads != 1024)
         return fail(CLB_INVALID_VALUE, "tuning.bitmap_threads must be 256, 512 or 1024");
+    if (t->small_lanes && t->small_lanes != 8 && t->small_lanes != 16 && t->small_lanes != 32)
+        return fail(CLB_INVALID_VALUE, "tuning.small_lanes must be 8, 16 or 32");
     return CLB_SUCCESS;
 }
 
@@ -169,6 +178,7 @@ void clb_spgemm_tuning_default(clb_spgemm_tuning *t) {
     t->warp_max = d.warp_max;
     t->bitmap_min = d.bitmap_min;
     t->bitmap_threads = d.bitmap_threads;
+    t->small_lanes = d.small_lanes;
 }
 
 int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_spgemm_tuning *tuning,
@@ -198,9 +208,9 @@ int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a
         row_start[k] = arows;
         const bool live = a[k].nnz && b[k].nnz;  // a pair without products contributes nothing
         da[k] = PairDesc{a[k].rpt, a[k].rows, a[k].cols, live ? a[k].nzr : 0, live ? a[k].nnz : 0, anzr, annz,
-                         (uint32_t)arows, (uint32_t)brows};
+                         (uint32_t)arows, (uint32_t)brows, (uint32_t)b[k].ncols};
         db[k] = PairDesc{b[k].rpt, b[k].rows, b[k].cols, live ? b[k].nzr : 0, live ? b[k].nnz : 0, bnzr, bnnz,
-                         (uint32_t)brows, 0u};
+                         (uint32_t)brows, 0u, (uint32_t)b[k].ncols};
         if (live) {
             anzr += a[k].nzr;
             annz += a[k].nnz;
@@ -225,17 +235,18 @@ int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a
     if (annz == 0) return CLB_SUCCESS;
     DeviceGuard g(ctl);
     const uint32_t form = tuning ? tuning->form : 0;
-    const Tuning t = to_tuning(tuning);
+    Tuning t = to_tuning(tuning);
 
     // stacked operands
     Temp<PairDesc> dda, ddb;
     Temp<uint64_t> arpt, brpt, rs;
-    Temp<uint32_t> arws, acls, brws, bcls;
+    Temp<uint32_t> arws, acls, brws, bcls, rnc;
     CLB_RETURN_IF(dda.alloc(ctl, count));
     CLB_RETURN_IF(ddb.alloc(ctl, count));
     CLB_RETURN_IF(rs.alloc(ctl, count + 1));
     CLB_RETURN_IF(arpt.alloc(ctl, anzr + 1));
     CLB_RETURN_IF(arws.alloc(ctl, anzr));
+    CLB_RETURN_IF(rnc.alloc(ctl, anzr));
     CLB_RETURN_IF(acls.alloc(ctl, annz));
     CLB_RETURN_IF(brpt.alloc(ctl, bnzr + 1));
     CLB_RETURN_IF(brws.alloc(ctl, bnzr));
@@ -248,18 +259,17 @@ int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a
                  CLB_WRITE_BUFFER_ERROR);
     {
         ProfScope ps(ctl, "batch_stack");
-        stack_kernel<<<dim3(stack_grid_x(ctl, amax, count), count), CAT_NT, 0, ctl->stream>>>(dda.ptr, arpt.ptr,
-                                                                                             arws.ptr, acls.ptr, anzr,
-                                                                                             annz);
-        stack_kernel<<<dim3(stack_grid_x(ctl, bmax, count), count), CAT_NT, 0, ctl->stream>>>(ddb.ptr, brpt.ptr,
-                                                                                             brws.ptr, bcls.ptr, bnzr,
-                                                                                             bnnz);
+        stack_kernel<<<dim3(stack_grid_x(ctl, amax, count), count), CAT_NT, 0, ctl->stream>>>(
+            dda.ptr, arpt.ptr, arws.ptr, acls.ptr, rnc.ptr, anzr, annz);
+        stack_kernel<<<dim3(stack_grid_x(ctl, bmax, count), count), CAT_NT, 0, ctl->stream>>>(
+            ddb.ptr, brpt.ptr, brws.ptr, bcls.ptr, nullptr, bnzr, bnnz);
         CLB_CHECK_LAUNCH();
     }
     const clb_dcsr As{arows, brows, annz, anzr, arpt.ptr, arws.ptr, acls.ptr};
     const clb_dcsr Bs{brows, bcols, bnnz, bnzr, brpt.ptr, brws.ptr, bcls.ptr};
     CLB_RETURN_IF(validate_spgemm(As, Bs));
     clb_dcsr Cs{};
+    t.row_ncols = rnc.ptr;  // each pair's rows use a bitmap as wide as its own product
     CLB_RETURN_IF(spgemm_tuned(ctl, As, Bs, form, t, &Cs, &st));
     const uint32_t inner_launches = st.kernel_launches;
     if (Cs.nnz == 0) {
@@ -339,17 +349,19 @@ int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, co
     DeviceGuard g(ctl);
     std::vector<clb_spgemm_tuning> cand;
     for (uint32_t form : {0u, 1u})
-        for (uint32_t bmin : {4096u, 1024u, 256u})
+        for (uint32_t bmin : {4096u, 1024u})
             for (uint32_t bthr : {1024u, 256u})
-                for (uint32_t wmax : {256u, 64u}) {
-                    clb_spgemm_tuning t;
-                    clb_spgemm_tuning_default(&t);
-                    t.form = form;
-                    t.bitmap_min = bmin;
-                    t.bitmap_threads = bthr;
-                    t.warp_max = wmax;
-                    cand.push_back(t);
-                }
+                for (uint32_t wmax : {256u, 64u})
+                    for (uint32_t small : {8u, 32u}) {
+                        clb_spgemm_tuning t;
+                        clb_spgemm_tuning_default(&t);
+                        t.form = form;
+                        t.bitmap_min = bmin;
+                        t.bitmap_threads = bthr;
+                        t.warp_max = wmax;
+                        t.small_lanes = small;
+                        cand.push_back(t);
+                    }
     cudaEvent_t e0, e1;
     CLB_TRY_CUDA(cudaEventCreate(&e0), CLB_RUN_KERNEL_FAILURE);
     if (cudaEventCreate(&e1) != cudaSuccess) {

@@ -126,17 +126,21 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, scal.ptr + 0));
     CLB_RETURN_IF(launch_binning(ctl, work.ptr, nullptr, n, B.ncols, info.ptr, list.ptr, flags.ptr, t));
     CLB_TRY_CUDA(cudaMemsetAsync(row_nnz.ptr, 0, n * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    // rows per bin: only the bins with rows are launched, sized to them
+    uint32_t hinfo[NUM_BINS];
+    CLB_TRY_CUDA(cudaMemcpyAsync(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost, ctl->stream),
+                 CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
 
     BinLists bl{list.ptr, info.ptr};
     RowOut sym{row_nnz.ptr, nullptr, nullptr, nullptr, nullptr, ctl->d_status};
-    CLB_RETURN_IF(launch_accumulators(ctl, false, bl, a, b, sym, B.ncols, n, t));
+    sym.row_ncols = t.row_ncols;
+    CLB_RETURN_IF(launch_accumulators(ctl, false, bl, a, b, sym, B.ncols, n, t, hinfo));
 
     CLB_RETURN_IF(scan_u32_to_u64(ctl, row_nnz.ptr, off.ptr, n, scal.ptr + 1));
     CLB_RETURN_IF(scan_u32_inplace(ctl, flags.ptr, n, scal.ptr + 2));
     uint64_t h[3];
     CLB_RETURN_IF(read_scalars(ctl, scal.ptr, h, 3));
-    uint32_t hinfo[NUM_BINS];
-    CLB_TRY_CUDA(cudaMemcpy(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost), CLB_READ_BUFFER_ERROR);
     st.products = h[0];
     const uint64_t nnz = h[1], nzr = h[2];
     st.nnz = nnz;
@@ -158,7 +162,8 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     CLB_RETURN_IF(launch_assemble(ctl, work.ptr, flags.ptr, off.ptr, A.rows, n, c_rpt.ptr, c_rows.ptr, nzr, nnz));
 
     RowOut num{nullptr, off.ptr, nullptr, nullptr, c_cols.ptr, ctl->d_status};
-    CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t));
+    num.row_ncols = t.row_ncols;
+    CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t, hinfo));
     CLB_RETURN_IF(check_status(ctl, "matrix_multiplication_hash"));
 
     C.nnz = nnz;

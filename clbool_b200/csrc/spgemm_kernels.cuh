@@ -42,7 +42,9 @@ enum Bin : int {
     BIN_BMP_XL = 9,   // products > 2^20
     BIN_BMP_L = 10,   // products > 2^17
     BIN_BMP = 11,     // the rest
-    NUM_BINS = 12
+    BIN_G8 = 12,      // products <= 8, 8 lanes per row (tuning small_lanes <= 8)
+    BIN_G16 = 13,     // products <= 16, 16 lanes per row (small_lanes <= 16)
+    NUM_BINS = 14
 };
 
 // Rows with at most this many products never reach the bitmap accumulator
@@ -56,17 +58,26 @@ constexpr uint32_t ESC_MAX_PRODUCTS = 4096;
 //                  ESC_MAX_PRODUCTS; lower values pay off when the bitmap is
 //                  narrow, i.e. few columns);
 //   bitmap_threads threads per bitmap row (256, 512 or 1024).
+//   small_lanes    lanes per row for the smallest rows: 8 (rows of <= 8
+//                  products share a warp four ways, <= 16 two ways), 16, or
+//                  32 (a warp per row).
 struct Tuning {
     uint32_t warp_max = 256;
     uint32_t bitmap_min = ESC_MAX_PRODUCTS;
     uint32_t bitmap_threads = 1024;
+    uint32_t small_lanes = 8;
+    // Per A row: columns of that row's product, when they differ by row (a
+    // stacked batch of pairs); null = B.ncols for every row.
+    const uint32_t *row_ncols = nullptr;
 };
 
 // Bin of a row from its product count and its distinct-column bound
 // (min(products, ncols), or a capacity).
 __host__ __device__ __forceinline__ int bin_of(uint64_t products, uint64_t distinct_bound, uint32_t warp_max,
-                                               uint32_t bitmap_min) {
+                                               uint32_t bitmap_min, uint32_t small_lanes) {
     if (products == 0) return BIN_NONE;
+    if (products <= 8 && small_lanes <= 8) return BIN_G8;
+    if (products <= 16 && small_lanes <= 16) return BIN_G16;
     if (products <= warp_max) {
         if (products <= 32) return BIN_W1;
         if (products <= 64) return BIN_W2;
@@ -116,6 +127,7 @@ struct RowOut {
     uint32_t *arena = nullptr;
     unsigned long long *arena_cursor = nullptr;    // entries reserved so far
     uint64_t arena_cap = 0;                        // entries
+    const uint32_t *row_ncols = nullptr;           // columns of row i's product (batched pairs), or all
 };
 
 // ------------------------------------------------------------- warp ESC ----
@@ -234,6 +246,80 @@ __global__ void __launch_bounds__(ESC_WARPS * 32) warp_esc_kernel(BinLists bl, i
                 if (flags & (1u << e)) *dst++ = v[e];
             }
         }
+    }
+}
+
+// G lanes per row (G = 8 or 16), 32 / G rows per warp, for rows of at most
+// G products: each lane gathers the B row of one A entry into the group's
+// slice of a warp-private buffer, the group sorts its G values with a
+// bitonic network over width-G shuffles and drops duplicates.  Loops and
+// shuffles are warp-uniform; groups without a row carry EMPTY.
+template <int G, bool NUMERIC>
+__global__ void __launch_bounds__(ESC_WARPS * 32, 4) group_esc_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o) {
+    constexpr int RPW = 32 / G;  // rows per warp
+    __shared__ uint32_t sbuf[ESC_WARPS][32];
+    const uint32_t lane = lane_id(), lg = lane % G, grp = lane / G;
+    uint32_t *buf = sbuf[warp_id()] + grp * G;
+    const uint32_t gmask = (G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u)) << (grp * G);
+    uint32_t beg, cnt;
+    bin_range(bl, bin, beg, cnt);
+    for (uint32_t w = blockIdx.x * ESC_WARPS + warp_id(); w * RPW < cnt; w += gridDim.x * ESC_WARPS) {
+        const uint32_t item = w * RPW + grp;
+        const bool has = item < cnt;
+        const uint32_t i = has ? bl.list[beg + item] : 0;
+        const uint64_t ja = has ? a.rpt[i] : 0, je = has ? a.rpt[i + 1] : 0;
+        uint32_t fill = 0;
+        for (uint64_t c = 0;; c += G) {
+            const bool more = ja + c < je;
+            if (!__any_sync(0xFFFFFFFFu, more)) break;
+            const uint64_t j = ja + c + lg;
+            uint64_t bb = 0;
+            uint32_t len = 0;
+            if (j < je) len = b_row(b, __ldg(a.cols + j), bb);
+            uint32_t inc = len;
+#pragma unroll
+            for (int d = 1; d < G; d <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, d, G);
+                if ((int)lg >= d) inc += t;
+            }
+            const uint32_t off = fill + inc - len;
+            for (uint32_t t = 0; t < len; ++t)
+                if (off + t < (uint32_t)G) buf[off + t] = __ldg(b.cols + bb + t);
+            fill += __shfl_sync(0xFFFFFFFFu, inc, G - 1, G);
+        }
+        __syncwarp();
+        if (fill > (uint32_t)G) {  // binning guarantees fill <= G
+            if (lg == 0) raise_status(o.status, DEV_BOUNDS);
+            fill = G;
+        }
+        uint32_t v = lg < fill ? buf[lg] : EMPTY;
+        __syncwarp();
+#pragma unroll
+        for (int k = 2; k <= G; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const uint32_t x = __shfl_xor_sync(0xFFFFFFFFu, v, j, G);
+                const bool up = (lg & k) == 0, lower = (lg & j) == 0;
+                v = (up == lower) ? min(v, x) : max(v, x);
+            }
+        }
+        const uint32_t pv = __shfl_up_sync(0xFFFFFFFFu, v, 1, G);
+        const bool f = v != EMPTY && (lg == 0 || v != pv);
+        const uint32_t fm = __ballot_sync(0xFFFFFFFFu, f) & gmask;
+        const uint32_t total = __popc(fm);
+        if (!has) continue;
+        if (!NUMERIC) {
+            if (lg == 0) o.row_nnz[i] = total;
+            continue;
+        }
+        if (o.row_cap) {
+            if (total > o.row_cap[i]) {
+                if (lg == 0) o.overflow[i] = 1;
+                continue;
+            }
+            if (lg == 0) o.row_nnz[i] = total;
+        }
+        if (f) o.cols[o.row_off[i] + __popc(fm & ((1u << lane) - 1u))] = v;
     }
 }
 
@@ -450,7 +536,7 @@ constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (column
 
 // Words of the bitmap for `ncols` columns: a multiple of the emission step,
 // at most BMP_MAX_WORDS.
-inline uint32_t bitmap_words(uint64_t ncols) {
+__host__ __device__ inline uint32_t bitmap_words(uint64_t ncols) {
     uint64_t w = (ncols + 31) / 32;
     w = (w + BMP_STEP_WORDS - 1) / BMP_STEP_WORDS * BMP_STEP_WORDS;
     if (w > BMP_MAX_WORDS) w = BMP_MAX_WORDS;
@@ -702,8 +788,6 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
     for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) bm[w] = 0;
     __syncthreads();
     const uint32_t lane = lane_id(), wi = warp_id();
-    const uint64_t chunk_cols = (uint64_t)W * 32;
-    const uint32_t nsteps = W / BMP_STEP_WORDS;  // <= BMP_MAX_STEPS
     constexpr int TPS = BMP_NT / (int)BMP_MAX_STEPS;  // counting threads per step
     static_assert(TPS >= 1 && TPS <= 32 && (TPS & (TPS - 1)) == 0, "block size");
     uint4 *bm4 = reinterpret_cast<uint4 *>(bm);
@@ -713,10 +797,15 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
         if (item >= cnt) break;
         const uint32_t i = bl.list[beg + item];
         const uint32_t shift = item < nheavy ? 9u : 8u;
+        // this row's columns (a batched pair can be narrower than the batch)
+        const uint64_t rn = o.row_ncols ? (uint64_t)o.row_ncols[i] : ncols;
+        const uint32_t Wr = bitmap_words(rn);
+        const uint64_t chunk_cols = (uint64_t)Wr * 32;
+        const uint32_t nsteps = Wr / BMP_STEP_WORDS;  // <= BMP_MAX_STEPS
         uint64_t total = 0;
         const uint64_t out_base = NUMERIC ? o.row_off[i] : 0;
         bool overflowed = false;
-        for (uint64_t c0 = 0; c0 < (MULTI ? ncols : 1); c0 += chunk_cols) {
+        for (uint64_t c0 = 0; c0 < (MULTI ? rn : 1); c0 += chunk_cols) {
             if (MULTI) {
                 unit_products<BMP_NT, BMP_ECH>(a, b, i, shift, s_beg, s_len, s_upre, scratch,
                                                [&](uint32_t c, bool valid) {
@@ -729,7 +818,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
             }
             if (!NUMERIC || overflowed) {
                 uint32_t mine = 0;
-                for (uint32_t w4 = threadIdx.x; w4 < W / 4; w4 += BMP_NT) {
+                for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) {
                     const uint4 x = bm4[w4];
                     mine += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
                     bm4[w4] = make_uint4(0, 0, 0, 0);
@@ -779,7 +868,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 }
                 if (MULTI || !o.arena || s_spill == ~0ull) {
                     overflowed = true;
-                    for (uint32_t w4 = threadIdx.x; w4 < W / 4; w4 += BMP_NT) bm4[w4] = make_uint4(0, 0, 0, 0);
+                    for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) bm4[w4] = make_uint4(0, 0, 0, 0);
                     total += ctot;
                     __syncthreads();
                     continue;

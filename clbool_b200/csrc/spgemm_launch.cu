@@ -11,7 +11,7 @@ constexpr int BIN_NT = 256;
 
 __global__ void __launch_bounds__(BIN_NT) bin_count_kernel(const uint32_t *__restrict__ work,
                                                            const uint32_t *__restrict__ cap, uint64_t n, uint64_t ncols,
-                                                           uint32_t warp_max, uint32_t bitmap_min,
+                                                           uint32_t warp_max, uint32_t bitmap_min, uint32_t small,
                                                            uint32_t *__restrict__ info, uint32_t *__restrict__ flags) {
     __shared__ uint32_t hist[NUM_BINS];
     if (threadIdx.x < NUM_BINS) hist[threadIdx.x] = 0;
@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(BIN_NT) bin_count_kernel(const uint32_t *__res
     for (uint64_t i = (uint64_t)blockIdx.x * BIN_NT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * BIN_NT) {
         uint32_t p = work[i];
         uint64_t bound = cap ? (uint64_t)cap[i] : (p < ncols ? (uint64_t)p : ncols);
-        int bin = bin_of(p, bound, warp_max, bitmap_min);
+        int bin = bin_of(p, bound, warp_max, bitmap_min, small);
         atomicAdd(&hist[bin], 1u);
         flags[i] = p > 0 ? 1u : 0u;
     }
@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(BIN_NT) bin_count_kernel(const uint32_t *__res
 __global__ void __launch_bounds__(BIN_NT) bin_scatter_kernel(const uint32_t *__restrict__ work,
                                                              const uint32_t *__restrict__ cap, uint64_t n,
                                                              uint64_t ncols, uint32_t warp_max, uint32_t bitmap_min,
-                                                             uint32_t *__restrict__ info,
+                                                             uint32_t small, uint32_t *__restrict__ info,
                                                              uint32_t *__restrict__ list) {
     __shared__ uint32_t boff[NUM_BINS];
     if (threadIdx.x == 0) {
@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(BIN_NT) bin_scatter_kernel(const uint32_t *__r
         if (i < n) {
             uint32_t p = work[i];
             uint64_t bound = cap ? (uint64_t)cap[i] : (p < ncols ? (uint64_t)p : ncols);
-            bin = bin_of(p, bound, warp_max, bitmap_min);
+            bin = bin_of(p, bound, warp_max, bitmap_min, small);
         }
         // warp-aggregated reservation per bin
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
@@ -100,6 +100,18 @@ int launch_esc(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, c
     return CLB_SUCCESS;
 }
 
+template <int G, bool NUM>
+int launch_group_esc(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
+                     uint64_t nmax, const char *name) {
+    static int occ = occupancy(group_esc_kernel<G, NUM>, ESC_WARPS * 32, 0);
+    unsigned grid = persistent_grid(ctl, occ, ceil_div_u(nmax, ESC_WARPS * (32 / G)));
+    ProfScope ps(ctl, name);
+    group_esc_kernel<G, NUM><<<grid, ESC_WARPS * 32, 0, ctl->stream>>>(bl, bin, a, b, o);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
 template <int T, int NT, bool NUM>
 int launch_hash(clb_controls *ctl, const BinLists &bl, int bin, const AView &a, const BRows &b, const RowOut &o,
                 uint64_t nmax, uint32_t *counter, const char *name) {
@@ -145,30 +157,53 @@ int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const B
     return launch_bitmap_nt<NUM, 1024>(ctl, bl, a, b, o, ncols, nmax, counter, name);
 }
 
+// hc (host, may be null): rows per bin, read back after binning; bins
+// without rows are not launched and the grids follow the bins' sizes.
 template <bool NUM>
 int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o, uint64_t ncols,
-               uint64_t nmax, const Tuning &t, bool hash_bins = true) {
+               uint64_t nmax, const Tuning &t, const uint32_t *hc, bool hash_bins = true) {
+    auto rows = [&](int bin) -> uint64_t { return hc ? hc[bin] : nmax; };
     // work counters of the dynamically scheduled launches
     Temp<uint32_t> ctr;
     CLB_RETURN_IF(ctr.alloc(ctl, 8));
     CLB_TRY_CUDA(cudaMemsetAsync(ctr.ptr, 0, 8 * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     // Heavy bins first so the long rows start early.
-    CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, a, b, o, ncols, nmax, ctr.ptr + 0,
-                                     NUM ? "bitmap_numeric" : "bitmap_symbolic", t.bitmap_threads));
+    const uint64_t nbmp = hc ? (uint64_t)hc[BIN_BMP_XL] + hc[BIN_BMP_L] + hc[BIN_BMP] : nmax;
+    if (nbmp)
+        CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, a, b, o, ncols, nbmp, ctr.ptr + 0,
+                                         NUM ? "bitmap_numeric" : "bitmap_symbolic", t.bitmap_threads));
     if (hash_bins) {
-        CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, nmax, ctr.ptr + 1,
-                                                   NUM ? "hash8k_numeric" : "hash8k_symbolic")));
-        CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, nmax, ctr.ptr + 2,
-                                                   NUM ? "hash4k_numeric" : "hash4k_symbolic")));
-        CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, nmax, ctr.ptr + 3,
-                                                   NUM ? "hash2k_numeric" : "hash2k_symbolic")));
-        CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, nmax, ctr.ptr + 4,
-                                                   NUM ? "hash1k_numeric" : "hash1k_symbolic")));
+        if (rows(BIN_H8K))
+            CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, rows(BIN_H8K), ctr.ptr + 1,
+                                                       NUM ? "hash8k_numeric" : "hash8k_symbolic")));
+        if (rows(BIN_H4K))
+            CLB_RETURN_IF((launch_hash<4096, 512, NUM>(ctl, bl, BIN_H4K, a, b, o, rows(BIN_H4K), ctr.ptr + 2,
+                                                       NUM ? "hash4k_numeric" : "hash4k_symbolic")));
+        if (rows(BIN_H2K))
+            CLB_RETURN_IF((launch_hash<2048, 256, NUM>(ctl, bl, BIN_H2K, a, b, o, rows(BIN_H2K), ctr.ptr + 3,
+                                                       NUM ? "hash2k_numeric" : "hash2k_symbolic")));
+        if (rows(BIN_H1K))
+            CLB_RETURN_IF((launch_hash<1024, 256, NUM>(ctl, bl, BIN_H1K, a, b, o, rows(BIN_H1K), ctr.ptr + 4,
+                                                       NUM ? "hash1k_numeric" : "hash1k_symbolic")));
     }
-    CLB_RETURN_IF((launch_esc<8, NUM>(ctl, bl, BIN_W8, a, b, o, nmax, NUM ? "esc256_numeric" : "esc256_symbolic")));
-    CLB_RETURN_IF((launch_esc<4, NUM>(ctl, bl, BIN_W4, a, b, o, nmax, NUM ? "esc128_numeric" : "esc128_symbolic")));
-    CLB_RETURN_IF((launch_esc<2, NUM>(ctl, bl, BIN_W2, a, b, o, nmax, NUM ? "esc64_numeric" : "esc64_symbolic")));
-    CLB_RETURN_IF((launch_esc<1, NUM>(ctl, bl, BIN_W1, a, b, o, nmax, NUM ? "esc32_numeric" : "esc32_symbolic")));
+    if (rows(BIN_W8))
+        CLB_RETURN_IF((launch_esc<8, NUM>(ctl, bl, BIN_W8, a, b, o, rows(BIN_W8),
+                                          NUM ? "esc256_numeric" : "esc256_symbolic")));
+    if (rows(BIN_W4))
+        CLB_RETURN_IF((launch_esc<4, NUM>(ctl, bl, BIN_W4, a, b, o, rows(BIN_W4),
+                                          NUM ? "esc128_numeric" : "esc128_symbolic")));
+    if (rows(BIN_W2))
+        CLB_RETURN_IF((launch_esc<2, NUM>(ctl, bl, BIN_W2, a, b, o, rows(BIN_W2),
+                                          NUM ? "esc64_numeric" : "esc64_symbolic")));
+    if (rows(BIN_W1))
+        CLB_RETURN_IF((launch_esc<1, NUM>(ctl, bl, BIN_W1, a, b, o, rows(BIN_W1),
+                                          NUM ? "esc32_numeric" : "esc32_symbolic")));
+    if (t.small_lanes <= 16 && rows(BIN_G16))
+        CLB_RETURN_IF((launch_group_esc<16, NUM>(ctl, bl, BIN_G16, a, b, o, rows(BIN_G16),
+                                                 NUM ? "esc16_numeric" : "esc16_symbolic")));
+    if (t.small_lanes <= 8 && rows(BIN_G8))
+        CLB_RETURN_IF((launch_group_esc<8, NUM>(ctl, bl, BIN_G8, a, b, o, rows(BIN_G8),
+                                                NUM ? "esc8_numeric" : "esc8_symbolic")));
     return CLB_SUCCESS;
 }
 
@@ -179,22 +214,25 @@ int launch_binning(clb_controls *ctl, const uint32_t *work, const uint32_t *cap,
     CLB_TRY_CUDA(cudaMemsetAsync(info, 0, 2 * NUM_BINS * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     unsigned grid = persistent_grid(ctl, 8, ceil_div_u(n, BIN_NT));
     ProfScope ps(ctl, "binning");
-    bin_count_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, t.warp_max, t.bitmap_min, info, flags);
-    bin_scatter_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, t.warp_max, t.bitmap_min, info, list);
+    bin_count_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, t.warp_max, t.bitmap_min, t.small_lanes,
+                                                       info, flags);
+    bin_scatter_kernel<<<grid, BIN_NT, 0, ctl->stream>>>(work, cap, n, ncols, t.warp_max, t.bitmap_min, t.small_lanes,
+                                                         info, list);
     ctl->launches += 2;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
 }
 
 int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, const AView &a, const BRows &b,
-                        const RowOut &o, uint64_t ncols, uint64_t nmax, const Tuning &t) {
-    return numeric ? launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t)
-                   : launch_all<false>(ctl, bl, a, b, o, ncols, nmax, t);
+                        const RowOut &o, uint64_t ncols, uint64_t nmax, const Tuning &t, const uint32_t *hc) {
+    return numeric ? launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t, hc)
+                   : launch_all<false>(ctl, bl, a, b, o, ncols, nmax, t, hc);
 }
 
 int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
-                               const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins, const Tuning &t) {
-    return launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t, hash_bins);
+                               const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins, const Tuning &t,
+                               const uint32_t *hc) {
+    return launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t, hc, hash_bins);
 }
 
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,

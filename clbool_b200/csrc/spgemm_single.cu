@@ -208,14 +208,23 @@ int launch_upper_bound_caps(clb_controls *ctl, const uint32_t *work, uint64_t n,
 
 // The accumulators of the ESC form for rows of up to 4096 products.
 int launch_esc_accumulators(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
-                            const uint32_t *work, uint64_t nmax) {
+                            const uint32_t *work, uint64_t nmax, const uint32_t *hc) {
     Temp<uint32_t> ctr;
     CLB_RETURN_IF(ctr.alloc(ctl, 4));
     CLB_TRY_CUDA(cudaMemsetAsync(ctr.ptr, 0, 4 * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
-    CLB_RETURN_IF((launch_cta_esc<4096, 512>(ctl, bl, BIN_H8K, a, b, o, work, nmax, ctr.ptr + 0, "cta_esc4096")));
-    CLB_RETURN_IF((launch_cta_esc<2048, 256>(ctl, bl, BIN_H4K, a, b, o, work, nmax, ctr.ptr + 1, "cta_esc2048")));
-    CLB_RETURN_IF((launch_cta_esc<1024, 256>(ctl, bl, BIN_H2K, a, b, o, work, nmax, ctr.ptr + 2, "cta_esc1024")));
-    CLB_RETURN_IF((launch_cta_esc<512, 128>(ctl, bl, BIN_H1K, a, b, o, work, nmax, ctr.ptr + 3, "cta_esc512")));
+    auto rows = [&](int bin) -> uint64_t { return hc ? hc[bin] : nmax; };
+    if (rows(BIN_H8K))
+        CLB_RETURN_IF((launch_cta_esc<4096, 512>(ctl, bl, BIN_H8K, a, b, o, work, rows(BIN_H8K), ctr.ptr + 0,
+                                                 "cta_esc4096")));
+    if (rows(BIN_H4K))
+        CLB_RETURN_IF((launch_cta_esc<2048, 256>(ctl, bl, BIN_H4K, a, b, o, work, rows(BIN_H4K), ctr.ptr + 1,
+                                                 "cta_esc2048")));
+    if (rows(BIN_H2K))
+        CLB_RETURN_IF((launch_cta_esc<1024, 256>(ctl, bl, BIN_H2K, a, b, o, work, rows(BIN_H2K), ctr.ptr + 2,
+                                                 "cta_esc1024")));
+    if (rows(BIN_H1K))
+        CLB_RETURN_IF((launch_cta_esc<512, 128>(ctl, bl, BIN_H1K, a, b, o, work, rows(BIN_H1K), ctr.ptr + 3,
+                                                "cta_esc512")));
     return CLB_SUCCESS;
 }
 
@@ -252,9 +261,11 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     uint64_t h[2];
     CLB_RETURN_IF(read_scalars(ctl, scal.ptr, h, 2));
     const uint64_t nzr = h[0], capacity = h[1];
+    uint32_t hinfo[NUM_BINS];  // rows per bin: only bins with rows are launched
+    CLB_TRY_CUDA(cudaMemcpyAsync(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost, ctl->stream),
+                 CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
     if (st) {
-        uint32_t hinfo[NUM_BINS];
-        CLB_TRY_CUDA(cudaMemcpy(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost), CLB_READ_BUFFER_ERROR);
         for (int k = 0; k < NUM_BINS; ++k) st->rows_per_bin[k] = hinfo[k];
         st->capacity = capacity;
     }
@@ -263,6 +274,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
 
     BinLists bl{list.ptr, info.ptr};
     RowOut num{row_nnz.ptr, slot_off.ptr, cap, ovf.ptr, pre.ptr, ctl->d_status};
+    num.row_ncols = t.row_ncols;
     // spill arena for single-chunk bitmap rows over their capacity
     Temp<uint64_t> spill;
     Temp<uint32_t> arena;
@@ -280,10 +292,10 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     if (esc) {
         // warp ESC and bitmap rows through the shared launcher's bins; rows of
         // the hash bins go to the CTA ESC kernels instead.
-        CLB_RETURN_IF(launch_esc_accumulators(ctl, bl, a, b, num, work, n));
-        CLB_RETURN_IF(launch_accumulators_subset(ctl, bl, a, b, num, B.ncols, n, /*hash_bins=*/false, t));
+        CLB_RETURN_IF(launch_esc_accumulators(ctl, bl, a, b, num, work, n, hinfo));
+        CLB_RETURN_IF(launch_accumulators_subset(ctl, bl, a, b, num, B.ncols, n, /*hash_bins=*/false, t, hinfo));
     } else {
-        CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t));
+        CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t, hinfo));
     }
 
     // the fallback below resets the device status word: check it first
@@ -326,7 +338,9 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
         CLB_CHECK_LAUNCH();
         clb_dcsr subA{A.nrows, A.ncols, sub_nnz, novf, sub_rpt.ptr, sub_rows.ptr, sub_cols.ptr};
         const uint32_t launches = ctl->launches;
-        CLB_RETURN_IF(spgemm_hash_two_pass(ctl, subA, B, &sub_c, nullptr, t));
+        Tuning tf = t;
+        tf.row_ncols = nullptr;  // indexed by the rows of A, not of the gathered A'
+        CLB_RETURN_IF(spgemm_hash_two_pass(ctl, subA, B, &sub_c, nullptr, tf));
         ctl->launches += launches;
         if (sub_c.nzr != novf) {
             clb_dcsr_release(ctl, &sub_c);

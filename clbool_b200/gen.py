@@ -37,6 +37,13 @@ def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c:
     return (key >> np.uint64(32)).astype(np.uint32), (key & np.uint64(0xFFFFFFFF)).astype(np.uint32)
 
 
+def _sorted_unique(a: np.ndarray) -> np.ndarray:
+    a = np.sort(a)
+    if a.size < 2:
+        return a
+    return a[np.concatenate([[True], a[1:] != a[:-1]])]
+
+
 def _rows_without_replacement(lens: np.ndarray, ncols: int, rng: np.random.Generator):
     """Sorted COO with exactly lens[i] distinct columns in row i (uniform
     without replacement), vectorised: draw with replacement, drop duplicate
@@ -49,14 +56,14 @@ def _rows_without_replacement(lens: np.ndarray, ncols: int, rng: np.random.Gener
     sparse = lens.copy()
     sparse[dense] = 0
     rows = np.repeat(np.arange(nrows, dtype=np.int64), sparse)
-    keys = np.unique(rows * ncols + rng.integers(0, ncols, size=rows.size))
+    keys = _sorted_unique(rows * ncols + rng.integers(0, ncols, size=rows.size))
     for _ in range(200):
         have = np.bincount(keys // ncols, minlength=nrows)
         short = sparse - have
         if not short.any():
             break
         extra = np.repeat(np.arange(nrows, dtype=np.int64), short)
-        keys = np.unique(np.concatenate([keys, extra * ncols + rng.integers(0, ncols, size=extra.size)]))
+        keys = _sorted_unique(np.concatenate([keys, extra * ncols + rng.integers(0, ncols, size=extra.size)]))
     else:
         raise RuntimeError("row generation did not converge")
     if dkeys:

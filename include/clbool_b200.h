@@ -267,13 +267,16 @@ CLB_API int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a, const 
  *                   (the rest use the CTA hash / CTA ESC kernels, whose table
  *                   size follows the row's bound: 1K, 2K, 4K or 8K slots)
  *   bitmap_threads  threads per bitmap row: 256, 512 or 1024
+ *   small_lanes     lanes per row for rows of at most 8 / 16 products: 8
+ *                   (four / two rows per warp), 16, or 32 (a warp per row)
  * Zero fields take the defaults (clb_spgemm_tuning_default). */
 typedef struct clb_spgemm_tuning {
     uint32_t form;
     uint32_t warp_max;
     uint32_t bitmap_min;
     uint32_t bitmap_threads;
-    uint32_t reserved[4];
+    uint32_t small_lanes;
+    uint32_t reserved[3];
 } clb_spgemm_tuning;
 CLB_API void clb_spgemm_tuning_default(clb_spgemm_tuning *tuning);
 /* C = A*B with a tuning (NULL = defaults, i.e. clb_dcsr_spgemm_hash). */
@@ -285,8 +288,8 @@ CLB_API int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const cl
  * owns its buffers.  stats (optional) covers the whole batch. */
 CLB_API int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                     clb_dcsr *c, const clb_spgemm_tuning *tuning, clb_spgemm_stats *stats);
-/* Times the batched product under every candidate tuning (24: form x
- * bitmap_min x bitmap_threads x warp_max) on the given pairs and returns the
+/* Times the batched product under every candidate tuning (32: form x
+ * bitmap_min x bitmap_threads x warp_max x small_lanes) on the given pairs and returns the
  * fastest in *best; tried/ms (optional, max_tried entries) receive each
  * candidate and its device time in ms, *n_tried their number. */
 CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,

@@ -48,13 +48,13 @@ def test_batch_of_power_law_pairs(controls):
     assert st["products"] == sum(int(O.workload(a, b).sum()) for a, b in pairs)
 
 
-@pytest.mark.parametrize("form,warp_max,bitmap_min,bitmap_threads", [
-    ("two_pass", 256, 4096, 1024), ("single_pass", 256, 4096, 1024), ("two_pass", 64, 256, 256),
-    ("single_pass", 32, 256, 512), ("two_pass", 128, 1024, 256), ("single_pass", 64, 1024, 1024)])
-def test_every_tuning_gives_the_same_product(controls, form, warp_max, bitmap_min, bitmap_threads):
+@pytest.mark.parametrize("form,warp_max,bitmap_min,bitmap_threads,small_lanes", [
+    ("two_pass", 256, 4096, 1024, 8), ("single_pass", 256, 4096, 1024, 8), ("two_pass", 64, 256, 256, 32),
+    ("single_pass", 32, 256, 512, 16), ("two_pass", 128, 1024, 256, 16), ("single_pass", 64, 1024, 1024, 32)])
+def test_every_tuning_gives_the_same_product(controls, form, warp_max, bitmap_min, bitmap_threads, small_lanes):
     import clbool_b200 as cb
     pairs = batch(6, seed=3) + [(pairs_dcsr(1500, 40), pairs_dcsr(1500, 40))]
-    t = cb.dcsr.tuning(form, warp_max, bitmap_min, bitmap_threads)
+    t = cb.dcsr.tuning(form, warp_max, bitmap_min, bitmap_threads, small_lanes)
     got = run_batched(controls, pairs, tune=t)
     for k, ((a, b), c) in enumerate(zip(pairs, got)):
         assert_dcsr_equal(c, O.spgemm(a, b), f"pair {k} {t.as_dict()}")
@@ -113,7 +113,7 @@ def test_autotune_picks_a_tuning(controls):
     pairs = batch(8, seed=5)
     dev = [(to_device(controls, a), to_device(controls, b)) for a, b in pairs]
     best, tried = cb.dcsr.autotune(controls, dev)
-    assert len(tried) == 24
+    assert len(tried) == 32
     assert all(ms > 0 for _, ms in tried)
     fastest = min(tried, key=lambda t: t[1])
     assert fastest[0] == best.as_dict()
