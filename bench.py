@@ -609,6 +609,79 @@ def run_small(args) -> dict:
                        "nnz_A": int(ra.size), "nnz_B": int(rb.size)}, "calls": out}
 
 
+def run_cfpq(args) -> dict:
+    """Bounded closure C <- C v sum_i C L_i over 3 uniform label matrices
+    (n = 2^18, average degree 3 each, seeds 1-3), each iteration's three
+    products in one batched call; stops at a fixpoint, 64 iterations, or
+    before an iteration of more than 4e9 products."""
+    import torch
+
+    import clbool_b200 as cb
+    from clbool_b200 import cfpq, gen
+    ctl = cb.create_controls(0, 0)
+    n = 1 << 18
+    labels = []
+    for seed in (1, 2, 3):
+        r, c = gen.poisson_rows(n, n, 3.0, seed=seed)
+        labels.append(cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(*gen.to_dcsr(r, c)), n))
+    out = {}
+    # accumulator tuning: autotuned on the second iteration's product C_2 M
+    C2, _ = cfpq.closure(ctl, labels, max_iters=2)
+    M = cfpq.union(ctl, [cfpq.identity(ctl, n)] + labels)
+    best, _ = cb.dcsr.autotune(ctl, [(C2, M)])
+    del C2
+    for method, tune in (("fused", None), ("fused_autotuned", best), ("batched", None)):
+        m = "batched" if method == "batched" else "fused"
+        cfpq.closure(ctl, labels, max_iters=2, method=m, tune=tune)  # warm-up
+        torch.cuda.synchronize()
+        C, hist = cfpq.closure(ctl, labels, max_iters=64, max_products=int(4e9), method=m, tune=tune)
+        out[method] = {"iterations": hist, "final_nnz": C.nnz(), "stop": hist[-1].get("stop"),
+                       "products": sum(h["products"] for h in hist), "ms": sum(h["ms"] for h in hist)}
+        if tune is not None:
+            out[method]["tuning"] = tune.as_dict()
+        del C
+    f = out["fused_autotuned"]
+    return {"metric": METRIC, "workload": "cfpq3_n2^18_deg3", "value": f["products"] / (f["ms"] / 1e3),
+            "unit": UNIT, "n_gpus": 1, "data": "synthetic", "higher_is_better": True,
+            "config": {"workload": "cfpq3_n2^18_deg3", "n": n, "labels": 3, "degree": 3, "max_products": 4e9,
+                       "value_method": "fused (C <- C (I v L1 v L2 v L3)), autotuned on C_2 M"},
+            "methods": out}
+
+
+def run_kron(args) -> dict:
+    """DCSR Kronecker product of two R-MAT scale-11 graphs (seeds 1, 2)."""
+    import torch
+
+    import clbool_b200 as cb
+    from clbool_b200 import gen
+    ctl = cb.create_controls(0, 0)
+    stream = torch.cuda.ExternalStream(ctl.stream, device="cuda:0")
+    mats = []
+    for seed in (1, 2):
+        r, c = gen.rmat(11, seed=seed)
+        mats.append(cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(*gen.to_dcsr(r, c)), 1 << 11))
+    A, B = mats
+    k = cb.dcsr.kronecker_product(ctl, None, A, B)
+    nnz, nzr = k.nnz(), k.nzr()
+    del k
+
+    def f():
+        out = cb.dcsr.kronecker_product(ctl, None, A, B)
+        del out
+    for _ in range(max(3, args.warmup)):
+        f()
+    ms = _event_ms(stream, f, max(5, args.steps))
+    out_bytes = 4 * nnz + 8 * (nzr + 1) + 4 * nzr
+    peak, src = peaks()
+    return {"metric": "Kronecker output entries/s", "workload": "kron_rmat11_x_rmat11", "value": nnz / (ms / 1e3),
+            "unit": "entries/s", "ms_per_step": ms, "n_gpus": 1, "data": "synthetic", "higher_is_better": True,
+            "config": {"workload": "kron_rmat11_x_rmat11", "nnz_A": A.nnz(), "nnz_B": B.nnz(), "nnz_C": nnz,
+                       "nzr_C": nzr},
+            "roofline": {"bound": "hbm", "achieved": out_bytes / (ms / 1e3) / 1e9, "peak": peak, "peak_source": src,
+                         "unit": "GB/s", "frac": out_bytes / (ms / 1e3) / 1e9 / peak,
+                         "alg_bytes": out_bytes}}
+
+
 # --------------------------------------------------------------------- main --
 def main():
     ap = argparse.ArgumentParser()
@@ -626,12 +699,13 @@ def main():
                     help="left operand = this seeded fraction of A's stored rows (profiling captures)")
     ap.add_argument("--ref-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="rmat", choices=["rmat", "batch", "poisson4096"],
+    ap.add_argument("--workload", default="rmat", choices=["rmat", "batch", "poisson4096", "cfpq", "kron"],
                     help="rmat: the headline A*A; batch / poisson4096: secondary workloads (own JSON line)")
     ap.add_argument("--pairs", type=int, default=256)
     args = ap.parse_args()
     if args.workload != "rmat":
-        print(json.dumps(run_batch(args) if args.workload == "batch" else run_small(args)), flush=True)
+        fn = {"batch": run_batch, "poisson4096": run_small, "cfpq": run_cfpq, "kron": run_kron}[args.workload]
+        print(json.dumps(fn(args)), flush=True)
         return
     if args.form is None:
         args.form = "learned" if os.path.exists(args.sizer) else "two_pass"

@@ -417,6 +417,7 @@ int clb_dcsr_row_nnz(clb_controls *ctl, const clb_dcsr *a_, const clb_dcsr *b_, 
     CLB_RETURN_IF(launch_binning(ctl, work.ptr, nullptr, n, B.ncols, info.ptr, list.ptr, flags.ptr));
     BinLists bl{list.ptr, info.ptr};
     RowOut sym{row_nnz, nullptr, nullptr, nullptr, nullptr, ctl->d_status};
+    sym.row_products = work.ptr;
     CLB_RETURN_IF(launch_accumulators(ctl, false, bl, a, b, sym, B.ncols, n));
     return check_status(ctl, "row_nnz");
 }

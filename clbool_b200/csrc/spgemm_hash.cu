@@ -135,6 +135,7 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     BinLists bl{list.ptr, info.ptr};
     RowOut sym{row_nnz.ptr, nullptr, nullptr, nullptr, nullptr, ctl->d_status};
     sym.row_ncols = t.row_ncols;
+    sym.row_products = work.ptr;
     CLB_RETURN_IF(launch_accumulators(ctl, false, bl, a, b, sym, B.ncols, n, t, hinfo));
 
     CLB_RETURN_IF(scan_u32_to_u64(ctl, row_nnz.ptr, off.ptr, n, scal.ptr + 1));
@@ -163,6 +164,7 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
 
     RowOut num{nullptr, off.ptr, nullptr, nullptr, c_cols.ptr, ctl->d_status};
     num.row_ncols = t.row_ncols;
+    num.row_products = work.ptr;
     CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t, hinfo));
     CLB_RETURN_IF(check_status(ctl, "matrix_multiplication_hash"));
 

@@ -128,6 +128,7 @@ struct RowOut {
     unsigned long long *arena_cursor = nullptr;    // entries reserved so far
     uint64_t arena_cap = 0;                        // entries
     const uint32_t *row_ncols = nullptr;           // columns of row i's product (batched pairs), or all
+    const uint32_t *row_products = nullptr;        // products of row i (picks the bitmap insertion path)
 };
 
 // ------------------------------------------------------------- warp ESC ----
@@ -533,6 +534,7 @@ constexpr int BMP_U = 8;                      // B-column loads in flight per la
 constexpr uint32_t BMP_STEP_WORDS = 128;      // emission step: 4 words per lane
 constexpr uint32_t BMP_MAX_STEPS = BMP_MAX_WORDS / BMP_STEP_WORDS;
 constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (columns)
+constexpr uint32_t BMP_SHORT = 64;            // products per A entry below which a row uses the per-product mapping
 
 // Words of the bitmap for `ncols` columns: a multiple of the emission step,
 // at most BMP_MAX_WORDS.
@@ -802,6 +804,10 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
         const uint32_t Wr = bitmap_words(rn);
         const uint64_t chunk_cols = (uint64_t)Wr * 32;
         const uint32_t nsteps = Wr / BMP_STEP_WORDS;  // <= BMP_MAX_STEPS
+        // Rows whose B rows average fewer than BMP_SHORT products would
+        // leave most lanes of a unit idle: they take the per-product mapping.
+        const bool short_b = o.row_products &&
+                             (uint64_t)o.row_products[i] < (uint64_t)BMP_SHORT * (a.rpt[i + 1] - a.rpt[i]);
         uint64_t total = 0;
         const uint64_t out_base = NUMERIC ? o.row_off[i] : 0;
         bool overflowed = false;
@@ -811,6 +817,12 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                                                [&](uint32_t c, bool valid) {
                     const uint64_t r = (uint64_t)c - c0;  // wraps for columns below c0
                     if (valid && r < chunk_cols) atomicOr(bm + (r >> 5), 1u << (r & 31));
+                });
+            } else if (short_b) {
+                // many short B rows: per-product mapping over the whole row
+                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_upre, s_beg, scratch,
+                                                      [&](uint32_t c, bool valid, uint32_t) {
+                    if (valid && c < (uint32_t)chunk_cols) atomicOr(bm + (c >> 5), 1u << (c & 31));
                 });
             } else {
                 bitmap_insert_row<BMP_NT, BMP_ECH>(a, b, i, shift, (uint32_t)(chunk_cols - 1), bm, s_beg, s_len,

@@ -275,6 +275,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     BinLists bl{list.ptr, info.ptr};
     RowOut num{row_nnz.ptr, slot_off.ptr, cap, ovf.ptr, pre.ptr, ctl->d_status};
     num.row_ncols = t.row_ncols;
+    num.row_products = work;
     // spill arena for single-chunk bitmap rows over their capacity
     Temp<uint64_t> spill;
     Temp<uint32_t> arena;

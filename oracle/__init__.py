@@ -317,6 +317,36 @@ def transpose(a: Dcsr) -> Dcsr:
     return _from_orc(sc)
 
 
+def union(mats) -> Dcsr:
+    """Boolean sum of DCSR matrices of one shape (restates
+    coo_utils::matrix_addition_cpu, coo_utils.cpp:315-324, folded)."""
+    m0 = mats[0]
+    rows, cols = [], []
+    for m in mats:
+        if len(m.cols):
+            rows.append(np.repeat(np.asarray(m.rows, np.uint32), np.diff(np.asarray(m.rpt, np.int64))))
+            cols.append(np.asarray(m.cols, np.uint32))
+    if not rows:
+        return coo_to_dcsr(Coo(m0.nrows, m0.ncols, np.zeros(0, np.uint32), np.zeros(0, np.uint32)))
+    r, c = unique_pairs(*sort_pairs(np.concatenate(rows), np.concatenate(cols)))
+    return coo_to_dcsr(Coo(m0.nrows, m0.ncols, r, c))
+
+
+def closure(labels, max_iters: int = 64):
+    """Bounded fixpoint C_{t+1} = C_t v sum_i C_t L_i from C_0 = v_i L_i;
+    returns (C, nnz per iteration).  Not in the reference."""
+    C = union(labels)
+    hist = [len(C.cols)]
+    for _ in range(max_iters):
+        Cn = union([C] + [spgemm(C, L) for L in labels])
+        hist.append(len(Cn.cols))
+        stable = len(Cn.cols) == len(C.cols)
+        C = Cn
+        if stable:
+            break
+    return C, hist
+
+
 def row_features(a: Dcsr, b: Dcsr) -> np.ndarray:
     """Six features of every A row of A*B (float64, shape [nzr_A, 6]), the
     inputs of the row-size predictor: log2(1+|A_i|), log2(1+P_i),

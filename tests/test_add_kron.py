@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from util import coo_digest, csr_digest, dcsr_digest, from_device, golden, pairs_dcsr, to_device
+from util import assert_dcsr_equal, coo_digest, csr_digest, dcsr_digest, from_device, golden, pairs_dcsr, to_device
 
 pytestmark = pytest.mark.gpu
 G = golden()
@@ -122,3 +122,43 @@ def test_transpose(controls, size, k):
     a = pairs_dcsr(size, k)
     t = cb.dcsr.transpose(controls, None, to_device(controls, a))
     assert dcsr_digest(from_device(controls, t)) == dcsr_digest(O.transpose(a))
+
+
+# ------------------------------------------------------------ closure (CFPQ) --
+def _labels(n, deg, count, seed):
+    from clbool_b200 import gen
+    out = []
+    for k in range(count):
+        r, c = gen.poisson_rows(n, n, float(deg), seed=seed + k)
+        out.append(O.coo_to_dcsr(O.Coo(n, n, r, c)))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["fused", "batched"])
+def test_closure_fixpoint_matches_oracle(controls, method):
+    """Three uniform label matrices (n = 2^9, average degree 0.6 so the
+    closure stays sparse): every iteration's nnz and the fixpoint equal the
+    oracle's, by both iteration methods."""
+    from clbool_b200 import cfpq
+    labels = _labels(1 << 9, 0.6, 3, seed=11)
+    want, want_hist = O.closure(labels)
+    C, hist = cfpq.closure(controls, [to_device(controls, L) for L in labels], method=method)
+    assert [h["nnz"] for h in hist] == want_hist
+    assert hist[-1]["stop"] == "fixpoint"
+    assert_dcsr_equal(from_device(controls, C), want, "closure")
+
+
+@pytest.mark.gpu
+def test_closure_bounds(controls):
+    """Degree 3 per label: the closure grows fast; the iteration cap and the
+    products guard stop it, and the iterations done match the oracle's."""
+    from clbool_b200 import cfpq
+    labels = _labels(1 << 10, 3, 3, seed=21)
+    C, hist = cfpq.closure(controls, [to_device(controls, L) for L in labels], max_iters=2, method="batched")
+    assert hist[-1]["stop"] == "max_iters" and len(hist) == 3
+    want, want_hist = O.closure(labels, max_iters=2)
+    assert [h["nnz"] for h in hist] == want_hist
+    assert_dcsr_equal(from_device(controls, C), want, "closure, 2 iterations")
+    C2, hist2 = cfpq.closure(controls, [to_device(controls, L) for L in labels], max_products=1)
+    assert hist2[-1]["stop"] == "max_products" and len(hist2) == 1
