@@ -100,6 +100,16 @@ int main() {
         matrix_dcsr C2;
         dcsr::matrix_multiplication(controls, C2, A, B);
         EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, C2)) == product(pa, pb));
+        // additions without a reference counterpart: learned and batched forms
+        dcsr::RowSizer sizer(controls, seed);
+        matrix_dcsr C3;
+        dcsr::matrix_multiplication_learned(controls, C3, A, B, sizer);
+        EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, C3)) == product(pa, pb));
+        auto batch = dcsr::matrix_multiplication_batched(controls, {{A, B}, {B, A}, {A, A}});
+        EXPECT(batch.size() == 3);
+        EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, batch[0])) == product(pa, pb));
+        EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, batch[1])) == product(pb, pa));
+        EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, batch[2])) == product(pa, pa));
 
         std::vector<uint32_t> ar, ac, br, bc;
         for (auto &p : pa) { ar.push_back(p.first); ac.push_back(p.second); }

@@ -53,12 +53,20 @@ __global__ void __launch_bounds__(KR_NT) kron_cols_kernel(const uint64_t *__rest
                 for (uint64_t jb = lane; jb < lb; jb += 32)
                     dst[ja * lb + jb] = (uint32_t)(base + __ldg(bcols + b0 + jb));
             }
-        } else {
-            // short B rows: flatten (ja, jb) so all lanes stay busy
+        } else if (lb) {
+            // short B rows: flatten (ja, jb) so all lanes stay busy; each lane
+            // steps its (ja, jb) by 32 positions without dividing
             const uint64_t n = la * lb;
+            const uint32_t l = (uint32_t)lb, da = 32u / l, db = 32u % l;
+            uint32_t ja = lane / l, jb = lane % l;
             for (uint64_t q = lane; q < n; q += 32) {
-                const uint64_t ja = q / lb, jb = q - ja * lb;
                 dst[q] = (uint32_t)((uint64_t)__ldg(acols + a0 + ja) * bncols + __ldg(bcols + b0 + jb));
+                ja += da;
+                jb += db;
+                if (jb >= l) {
+                    jb -= l;
+                    ++ja;
+                }
             }
         }
     }

@@ -21,6 +21,7 @@
 #include <cstdint>
 #include <iostream>
 #include <memory>
+#include <utility>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -383,6 +384,55 @@ inline void transpose(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &m
     clb_dcsr v = matrix_in.view(), out{};
     details::check(clb_dcsr_transpose(c.get(), &v, &out));
     matrix_out = matrix_dcsr::adopt(c, out);
+}
+
+// ---- additions without a counterpart in the reference ------------------
+// Row-size predictor of the learned single-pass SpGEMM (owns device weights).
+class RowSizer {
+public:
+    explicit RowSizer(Controls &c, uint64_t seed = 1) {
+        clb_sizer *s = nullptr;
+        details::check(clb_sizer_create(c.get(), seed, &s));
+        handle_.reset(s, [](clb_sizer *p) { clb_sizer_destroy(p); });
+    }
+    RowSizer(Controls &c, const std::vector<float> &params) : RowSizer(c) { set_params(params); }
+    std::vector<float> params() const {
+        std::vector<float> p((size_t)clb_sizer_num_params());
+        details::check(clb_sizer_get_params(handle_.get(), p.data(), p.size()));
+        return p;
+    }
+    void set_params(const std::vector<float> &p) {
+        details::check(clb_sizer_set_params(handle_.get(), p.data(), p.size()));
+    }
+    clb_sizer *get() const { return handle_.get(); }
+
+private:
+    std::shared_ptr<clb_sizer> handle_;
+};
+
+// C = A*B in one numeric pass sized by the predictor; exact for any predictor.
+inline void matrix_multiplication_learned(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &a,
+                                          const matrix_dcsr &b, const RowSizer &sizer, float margin_log2 = 0.25f,
+                                          float slack = 8.0f, clb_spgemm_stats *stats = nullptr) {
+    clb_dcsr va = a.view(), vb = b.view(), out{};
+    details::check(clb_dcsr_spgemm_learned(c.get(), &va, &vb, sizer.get(), margin_log2, slack, &out, stats));
+    matrix_out = matrix_dcsr::adopt(c, out);
+}
+
+// out[k] = pairs[k].first * pairs[k].second, all pairs in one pass.
+inline std::vector<matrix_dcsr> matrix_multiplication_batched(
+    Controls &c, const std::vector<std::pair<matrix_dcsr, matrix_dcsr>> &pairs,
+    const clb_spgemm_tuning *tuning = nullptr, clb_spgemm_stats *stats = nullptr) {
+    std::vector<clb_dcsr> va, vb, vc(pairs.size());
+    for (const auto &p : pairs) {
+        va.push_back(p.first.view());
+        vb.push_back(p.second.view());
+    }
+    details::check(clb_dcsr_spgemm_batched(c.get(), (uint32_t)pairs.size(), va.data(), vb.data(), vc.data(), tuning,
+                                           stats));
+    std::vector<matrix_dcsr> out;
+    for (auto &m : vc) out.push_back(matrix_dcsr::adopt(c, m));
+    return out;
 }
 }  // namespace dcsr
 
