@@ -100,6 +100,8 @@ _SIGS = {
     "clb_csr_add": (C.c_int, [vp, P(clb_csr), P(clb_csr), P(clb_csr)]),
     "clb_dcsr_kronecker": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr)]),
     "clb_dcsr_transpose": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr)]),
+    "clb_dcsr_submatrix": (C.c_int, [vp, P(clb_dcsr), C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, P(clb_dcsr)]),
+    "clb_dcsr_reduce": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr)]),
     # learned sizing
     "clb_sizer_num_params": (C.c_int, []),
     "clb_sizer_create": (C.c_int, [vp, C.c_uint64, P(vp)]),

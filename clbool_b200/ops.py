@@ -226,5 +226,25 @@ def transpose(controls: Controls, matrix_out: matrix_dcsr | None, matrix_in: mat
     return res if matrix_out is None else matrix_out._assign(res)
 
 
+def submatrix(controls: Controls, matrix_out: matrix_dcsr | None, matrix_in: matrix_dcsr, i: int, j: int, nrows: int,
+              ncols: int) -> matrix_dcsr:
+    """dcsr::submatrix: rows [i, i+nrows), columns [j, j+ncols), re-indexed."""
+    out = clb_dcsr()
+    s = matrix_in.c_struct()
+    check(lib.clb_dcsr_submatrix(controls.handle, C.byref(s), int(i), int(j), int(nrows), int(ncols), C.byref(out)),
+          "dcsr::submatrix")
+    res = matrix_dcsr.adopt(controls, out)
+    return res if matrix_out is None else matrix_out._assign(res)
+
+
+def reduce(controls: Controls, matrix_out: matrix_dcsr | None, matrix_in: matrix_dcsr) -> matrix_dcsr:
+    """dcsr::reduce: row-wise OR as an nrows x 1 matrix."""
+    out = clb_dcsr()
+    s = matrix_in.c_struct()
+    check(lib.clb_dcsr_reduce(controls.handle, C.byref(s), C.byref(out)), "dcsr::reduce")
+    res = matrix_dcsr.adopt(controls, out)
+    return res if matrix_out is None else matrix_out._assign(res)
+
+
 def sort_arrays(controls: Controls, rows_gpu: DeviceBuffer, cols_gpu: DeviceBuffer, n: int) -> None:
     _coo_sort(controls, rows_gpu, cols_gpu, n)

@@ -386,6 +386,19 @@ inline void transpose(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &m
     matrix_out = matrix_dcsr::adopt(c, out);
 }
 
+inline void submatrix(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &matrix_in, uint32_t i, uint32_t j,
+                      uint32_t nrows, uint32_t ncols) {
+    clb_dcsr v = matrix_in.view(), out{};
+    details::check(clb_dcsr_submatrix(c.get(), &v, i, j, nrows, ncols, &out));
+    matrix_out = matrix_dcsr::adopt(c, out);
+}
+
+inline void reduce(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &matrix_in) {
+    clb_dcsr v = matrix_in.view(), out{};
+    details::check(clb_dcsr_reduce(c.get(), &v, &out));
+    matrix_out = matrix_dcsr::adopt(c, out);
+}
+
 // ---- additions without a counterpart in the reference ------------------
 // Row-size predictor of the learned single-pass SpGEMM (owns device weights).
 class RowSizer {

@@ -218,6 +218,15 @@ CLB_API int clb_dcsr_kronecker(clb_controls *ctl, const clb_dcsr *a, const clb_d
 /* dcsr::transpose (src/dcsr/dcsr.hpp:17-19, dcsr_transpose.cpp:5-16). */
 CLB_API int clb_dcsr_transpose(clb_controls *ctl, const clb_dcsr *in, clb_dcsr *out);
 
+/* dcsr::submatrix (src/dcsr/dcsr.hpp:12-16, dcsr_submatrix.cpp:98-155): rows
+ * [i, i+nrows) and columns [j, j+ncols) of `in`, re-indexed to start at 0,
+ * empty rows dropped; `out` is nrows x ncols (also when it has no entries). */
+CLB_API int clb_dcsr_submatrix(clb_controls *ctl, const clb_dcsr *in, uint64_t i, uint64_t j, uint64_t nrows,
+                               uint64_t ncols, clb_dcsr *out);
+/* dcsr::reduce (src/dcsr/dcsr.hpp:22-24, dcsr_reduce.cpp:5-31): the row-wise
+ * OR of `in` as an nrows x 1 matrix, one entry (column 0) per stored row. */
+CLB_API int clb_dcsr_reduce(clb_controls *ctl, const clb_dcsr *in, clb_dcsr *out);
+
 /* dcsr::matrix_multiplication (src/dcsr/dcsr.hpp:27-30,
  * dcsr_matrix_multiplication.cpp:26-97): the ESC/merge form -- every row gets
  * its upper bound of slots, one expand-sort-compress (or bitmap) pass fills

@@ -102,6 +102,9 @@ def lib():
         L.orc_csr_add.restype = C.c_uint64
         L.orc_kronecker.argtypes = [C.POINTER(_OrcDcsr), C.POINTER(_OrcDcsr), C.POINTER(_OrcDcsr)]
         L.orc_transpose.argtypes = [C.POINTER(_OrcDcsr), C.POINTER(_OrcDcsr)]
+        L.orc_submatrix.argtypes = [C.POINTER(_OrcDcsr), C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                                    C.POINTER(_OrcDcsr)]
+        L.orc_reduce.argtypes = [C.POINTER(_OrcDcsr), C.POINTER(_OrcDcsr)]
         L.orc_mlp_num_params.restype = C.c_int
         f32p = C.POINTER(C.c_float)
         f64p = C.POINTER(C.c_double)
@@ -317,6 +320,25 @@ def transpose(a: Dcsr) -> Dcsr:
     return _from_orc(sc)
 
 
+def submatrix(a: Dcsr, i: int, j: int, nrows: int, ncols: int) -> Dcsr:
+    """Rows [i, i+nrows), columns [j, j+ncols) of A, re-indexed (empty rows
+    dropped); cpu_matrix_operations.cpp:6-52."""
+    keep = []
+    sa = _to_orc(a, keep)
+    sc = _OrcDcsr()
+    lib().orc_submatrix(C.byref(sa), i, j, nrows, ncols, C.byref(sc))
+    return _from_orc(sc)
+
+
+def reduce(a: Dcsr) -> Dcsr:
+    """Row-wise OR: one entry (column 0) per stored row; dcsr_reduce.cpp:5-31."""
+    keep = []
+    sa = _to_orc(a, keep)
+    sc = _OrcDcsr()
+    lib().orc_reduce(C.byref(sa), C.byref(sc))
+    return _from_orc(sc)
+
+
 def union(mats) -> Dcsr:
     """Boolean sum of DCSR matrices of one shape (restates
     coo_utils::matrix_addition_cpu, coo_utils.cpp:315-324, folded)."""
@@ -427,6 +449,13 @@ class Ref:
         L.ref_kronecker_pairs.argtypes = [u32p, u32p, C.c_uint32, u32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.POINTER(u32p), C.POINTER(u32p)]
         L.ref_kronecker_pairs.restype = C.c_uint64
+        L.ref_submatrix.argtypes = [u32p, u32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.c_uint32, C.POINTER(u32p), C.POINTER(u32p), C.POINTER(u32p),
+                                    C.POINTER(C.c_uint32)]
+        L.ref_submatrix.restype = C.c_uint32
+        L.ref_reduce.argtypes = [u32p, u32p, u32p, C.c_uint32, C.c_uint32, C.POINTER(u32p), C.POINTER(u32p),
+                                 C.POINTER(u32p)]
+        L.ref_reduce.restype = C.c_uint32
         L.ref_random_matrices.argtypes = [C.c_int, C.c_uint32, C.c_uint32] + \
             [C.POINTER(u32p)] * 3 + [u32p] + [C.POINTER(u32p)] * 3 + [u32p]
         self.L = L
@@ -522,6 +551,24 @@ class Ref:
         A = Dcsr(max_size, max_size, a[0].astype(np.uint64), a[1], a[2])
         B = Dcsr(max_size, max_size, b[0].astype(np.uint64), b[1], b[2])
         return A, B
+
+    def submatrix(self, a: Dcsr, i, j, nrows, ncols) -> Dcsr:
+        keep = [self._arr(a.rows), self._arr(a.cols)]
+        ra = self._arr(np.asarray(a.rpt, dtype=np.uint64).astype(np.uint32))
+        rp, rr, cc, nzr = u32p(), u32p(), u32p(), C.c_uint32()
+        nnz = self.L.ref_submatrix(_p32(ra), _p32(keep[0]), _p32(keep[1]), len(a.rows), len(a.cols), i, j, nrows,
+                                   ncols, C.byref(rp), C.byref(rr), C.byref(cc), C.byref(nzr))
+        # an empty result comes back without row pointers
+        rpt = self._take(rp, nzr.value + 1).astype(np.uint64) if nnz else np.zeros(1, np.uint64)
+        return Dcsr(nrows, ncols, rpt, self._take(rr, nzr.value), self._take(cc, nnz))
+
+    def reduce(self, a: Dcsr) -> Dcsr:
+        keep = [self._arr(a.rows), self._arr(a.cols)]
+        ra = self._arr(np.asarray(a.rpt, dtype=np.uint64).astype(np.uint32))
+        rp, rr, cc = u32p(), u32p(), u32p()
+        n = self.L.ref_reduce(_p32(ra), _p32(keep[0]), _p32(keep[1]), len(a.rows), len(a.cols), C.byref(rp),
+                              C.byref(rr), C.byref(cc))
+        return Dcsr(a.nrows, 1, self._take(rp, n + 1).astype(np.uint64), self._take(rr, n), self._take(cc, n))
 
     def kronecker_pairs(self, a: Coo, b: Coo, b_nrows, b_ncols) -> Coo:
         r, c = u32p(), u32p()

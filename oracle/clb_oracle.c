@@ -640,3 +640,69 @@ void orc_mlp_grad(const float *params, const float *feat, const float *target, u
     }
     *loss = L;
 }
+
+
+/* ------------------------------------------------------------------------ */
+/* dcsr::submatrix (src/dcsr/dcsr_submatrix.cpp:98-155, CPU form            */
+/* src/common/cpu_matrix_operations.cpp:6-52): rows [i, i+nrows) and columns */
+/* [j, j+ncols) of A, re-indexed to start at 0; empty rows dropped.          */
+/* ------------------------------------------------------------------------ */
+static uint64_t lb_u32(const uint32_t *a, uint64_t n, uint64_t key) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint64_t m = lo + (hi - lo) / 2;
+        if ((uint64_t)a[m] < key) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
+void orc_submatrix(const orc_dcsr *a, uint64_t i, uint64_t j, uint64_t nrows, uint64_t ncols, orc_dcsr *out) {
+    memset(out, 0, sizeof(*out));
+    out->nrows = nrows;
+    out->ncols = ncols;
+    if (a->nnz == 0) return;
+    uint64_t r0 = lb_u32(a->rows, a->nzr, i), r1 = lb_u32(a->rows, a->nzr, i + nrows);
+    uint64_t n = r1 > r0 ? r1 - r0 : 0;
+    uint64_t *beg = (uint64_t *)malloc((n ? n : 1) * 8), *len = (uint64_t *)malloc((n ? n : 1) * 8);
+    uint64_t nnz = 0, nzr = 0;
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint64_t s = a->rpt[r0 + k], e = a->rpt[r0 + k + 1];
+        const uint64_t b = s + lb_u32(a->cols + s, e - s, j), f = s + lb_u32(a->cols + s, e - s, j + ncols);
+        beg[k] = b;
+        len[k] = f - b;
+        nnz += len[k];
+        nzr += len[k] > 0;
+    }
+    out->nnz = nnz;
+    out->nzr = nzr;
+    out->rpt = (uint64_t *)malloc((nzr + 1) * 8);
+    out->rows = (uint32_t *)malloc((nzr ? nzr : 1) * 4);
+    out->cols = (uint32_t *)malloc((nnz ? nnz : 1) * 4);
+    uint64_t o = 0, q = 0;
+    for (uint64_t k = 0; k < n; ++k) {
+        if (!len[k]) continue;
+        out->rpt[q] = o;
+        out->rows[q] = (uint32_t)(a->rows[r0 + k] - i);
+        for (uint64_t t = 0; t < len[k]; ++t) out->cols[o + t] = (uint32_t)(a->cols[beg[k] + t] - j);
+        o += len[k];
+        ++q;
+    }
+    out->rpt[nzr] = nnz;
+    free(beg);
+    free(len);
+}
+
+/* dcsr::reduce (src/dcsr/dcsr_reduce.cpp:5-31, cpu_matrix_operations.cpp:63-75):
+ * the row-wise OR, a column vector with one entry (column 0) per stored row. */
+void orc_reduce(const orc_dcsr *a, orc_dcsr *out) {
+    memset(out, 0, sizeof(*out));
+    out->nrows = a->nrows;
+    out->ncols = 1;
+    if (a->nnz == 0) return;
+    out->nnz = out->nzr = a->nzr;
+    out->rpt = (uint64_t *)malloc((a->nzr + 1) * 8);
+    out->rows = (uint32_t *)malloc(a->nzr * 4);
+    out->cols = (uint32_t *)calloc(a->nzr, 4);
+    for (uint64_t k = 0; k <= a->nzr; ++k) out->rpt[k] = k;
+    memcpy(out->rows, a->rows, a->nzr * 4);
+}

@@ -17,6 +17,7 @@
 //   utils::fill_random_buffer              src/common/utils.cpp:208-217
 //   coo_utils::fill_random_matrix          src/coo/coo_utils.cpp:135-151
 //   coo_utils::generate_random_matrices_large / _esc   src/coo/coo_utils.cpp:13-132
+//   submatrix_cpu, reduce                  src/common/cpu_matrix_operations.cpp:6-75
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -163,6 +164,30 @@ void ref_random_matrices(int which, uint32_t max_size, uint32_t seed,
     b_sizes[0] = ab.second.rpt().size();
     b_sizes[1] = ab.second.rows().size();
     b_sizes[2] = ab.second.cols().size();
+}
+
+uint32_t ref_submatrix(const uint32_t *rpt, const uint32_t *rows, const uint32_t *cols, uint32_t nzr, uint32_t nnz,
+                       uint32_t i, uint32_t j, uint32_t nrows, uint32_t ncols, uint32_t **orpt, uint32_t **orows,
+                       uint32_t **ocols, uint32_t *onzr) {
+    matrix_dcsr_cpu a = to_dcsr(rpt, rows, cols, nzr, nnz);
+    matrix_dcsr_cpu c;
+    utils::submatrix_cpu(c, a, i, j, nrows, ncols);
+    *orpt = dup_vec(c.rpt());
+    *orows = dup_vec(c.rows());
+    *ocols = dup_vec(c.cols());
+    *onzr = (uint32_t)c.rows().size();
+    return (uint32_t)c.cols().size();
+}
+
+uint32_t ref_reduce(const uint32_t *rpt, const uint32_t *rows, const uint32_t *cols, uint32_t nzr, uint32_t nnz,
+                    uint32_t **orpt, uint32_t **orows, uint32_t **ocols) {
+    matrix_dcsr_cpu a = to_dcsr(rpt, rows, cols, nzr, nnz);
+    matrix_dcsr_cpu c;
+    utils::reduce(c, a);
+    *orpt = dup_vec(c.rpt());
+    *orows = dup_vec(c.rows());
+    *ocols = dup_vec(c.cols());
+    return (uint32_t)c.rows().size();
 }
 
 }  // extern "C"

@@ -170,6 +170,29 @@ def main():
                      "cols": sha((key & np.uint64(0xFFFFFFFF)).astype(np.uint32), np.uint32)})
     cases["bitonic_sort"] = grid
 
+    # reduce / submatrix: the README example (test_operations.cpp:309-310) and
+    # the reference's submatrix / reduce test shapes (test_operations.cpp:52-106,
+    # operations.cpp:84-166) with seeded ranges (the reference draws them from
+    # std::random_device).
+    Ar = R.pairs_to_dcsr(a_rows, a_cols, 5, 5)
+    rr = R.reduce(Ar)
+    rs = R.submatrix(Ar, 0, 2, 3, 2)
+    cases["readme"]["reduce"] = {"rpt": rr.rpt.tolist(), "rows": rr.rows.tolist(), "cols": rr.cols.tolist()}
+    cases["readme"]["submatrix_0_2_3_2"] = {"rpt": rs.rpt.tolist(), "rows": rs.rows.tolist(),
+                                            "cols": rs.cols.tolist()}
+    rng = np.random.default_rng(2024)
+    grid = []
+    for size, k in ((5, 3), (400, 7), (995, 19), (1800, 30), (5000, 45)):
+        r, c = R.generate_coo_pairs(size * k, size)
+        a = R.pairs_to_dcsr(r, c, size, size)
+        i1, i2, i3, i4 = (int(x) for x in rng.integers(0, size + 1, 4))
+        i, nr, j, nc = min(i1, i2), abs(i1 - i2), min(i3, i4), abs(i3 - i4)
+        sub = R.submatrix(a, i, j, nr, nc)
+        red = R.reduce(a)
+        grid.append({"size": size, "k": k, "i": i, "j": j, "nrows": nr, "ncols": nc,
+                     "submatrix": dcsr_digest(sub), "reduce": dcsr_digest(red)})
+    cases["submatrix_reduce"] = grid
+
     with open(OUT, "w") as f:
         json.dump(g, f, indent=1, sort_keys=True)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")

@@ -130,3 +130,20 @@ def test_rowwise_nnz_matches_product():
     nnz = O.spgemm_row_nnz(a, a)
     assert int(nnz.sum()) == len(c.cols)
     assert np.array_equal(nnz[nnz > 0], np.diff(c.rpt))
+
+
+def test_submatrix_reduce_golden():
+    """README example (test_operations.cpp:309-310) and seeded ranges of the
+    reference's submatrix / reduce tests, recorded from the reference."""
+    g = G["readme"]
+    a = O.coo_to_dcsr(O.Coo(5, 5, np.array(g["a"]["rows"], np.uint32), np.array(g["a"]["cols"], np.uint32)))
+    r = O.reduce(a)
+    assert r.rpt.tolist() == g["reduce"]["rpt"] and r.rows.tolist() == g["reduce"]["rows"]
+    assert r.cols.tolist() == g["reduce"]["cols"]
+    s = O.submatrix(a, 0, 2, 3, 2)
+    assert s.rpt.tolist() == g["submatrix_0_2_3_2"]["rpt"] and s.rows.tolist() == g["submatrix_0_2_3_2"]["rows"]
+    assert s.cols.tolist() == g["submatrix_0_2_3_2"]["cols"]
+    for case in G["submatrix_reduce"]:
+        a = pairs_dcsr(case["size"], case["k"])
+        assert dcsr_digest(O.submatrix(a, case["i"], case["j"], case["nrows"], case["ncols"])) == case["submatrix"]
+        assert dcsr_digest(O.reduce(a)) == case["reduce"]
