@@ -269,3 +269,23 @@ def test_packaged_checkpoint_rmat16(controls):
     assert_dcsr_equal(got, want, "rmat16 packaged predictor")
     assert st["fallback_rows"] <= max(2, len(want.rows) // 1000)
     assert st["capacity"] < 1.5 * len(want.cols)
+
+
+@pytest.mark.gpu
+def test_learned_fallback_on_wide_rows(controls):
+    """Columns past one bitmap chunk (2^21 + 5): bitmap rows over their slot
+    cannot spill (their count is only known after the last chunk), so they
+    take the exact two-pass fallback; C is still the oracle's product."""
+    from clbool_b200 import sizing
+    n = (1 << 21) + 5
+    rng = np.random.default_rng(12)
+    ra = np.repeat(np.arange(64, dtype=np.uint32), 40)
+    ca = rng.integers(0, 3000, ra.size).astype(np.uint32)
+    a = O.coo_to_dcsr(O.Coo(64, 3000, *O.unique_pairs(*O.sort_pairs(ra, ca))))
+    rb = np.repeat(np.arange(3000, dtype=np.uint32), 200)
+    cbb = rng.integers(0, n, rb.size).astype(np.uint32)
+    b = O.coo_to_dcsr(O.Coo(3000, n, *O.unique_pairs(*O.sort_pairs(rb, cbb))))
+    s = sizing.RowSizer(controls, seed=4)
+    got, st = _learned(controls, a, b, s, margin=-1000.0, slack=0.0)
+    assert_dcsr_equal(got, O.spgemm(a, b), "wide learned")
+    assert st["fallback_rows"] > 0 and st["spilled_rows"] == 0
