@@ -682,6 +682,49 @@ def run_kron(args) -> dict:
                          "alg_bytes": out_bytes}}
 
 
+def run_rmat21(args) -> dict:
+    """Learned-form A*A at R-MAT scale 21 (seed 21, the scale the predictor is
+    evaluated on; never trained on): C (2.65e10 entries, 106 GB) does not fit
+    beside its slots, so A's rows run in blocks balanced by products and each
+    block's C is discarded after its nnz is read.  Reports products/s, the
+    slots over nnz, spilled and fallback rows."""
+    import torch
+
+    import clbool_b200 as cb
+    from clbool_b200 import gen, sizing
+    ctl = cb.create_controls(0, 0)
+    stream = torch.cuda.ExternalStream(ctl.stream, device="cuda:0")
+    scale = 21
+    n = 1 << scale
+    r, c = gen.rmat(scale, seed=scale)
+    rpt, rows, cols = gen.to_dcsr(r, c)
+    del r, c
+    A_full = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(rpt, rows, cols), n)
+    work = cb.dcsr.workload(ctl, A_full, A_full)[0].to_host(rows.size).astype(np.int64)
+    sizer = sizing.RowSizer.load(ctl, args.sizer)
+    blocks = max(1, args.blocks)
+    tot = {"products": 0, "nnz": 0, "capacity": 0, "spilled_rows": 0, "fallback_rows": 0, "ms": 0.0}
+    for k in range(blocks):
+        lo, hi = shard_rows(work, blocks, k)
+        if hi <= lo:
+            continue
+        srpt = (rpt[lo:hi + 1] - rpt[lo]).astype(np.uint64)
+        A = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(srpt, rows[lo:hi], cols[int(rpt[lo]):int(rpt[hi])]), n)
+        st = {}
+        ms = _event_ms(stream, lambda: sizing.matrix_multiplication_learned(ctl, None, A, A_full, sizer, stats=st), 1)
+        for key in ("products", "nnz", "capacity", "spilled_rows", "fallback_rows"):
+            tot[key] += int(st.get(key, 0))
+        tot["ms"] += ms
+        del A
+    return {"metric": METRIC, "workload": "rmat_s21_AxA_learned_row_blocks", "value": tot["products"] / (tot["ms"] / 1e3),
+            "unit": UNIT, "n_gpus": 1, "data": "synthetic", "higher_is_better": True,
+            "config": {"workload": "rmat_s21_AxA_learned_row_blocks", "scale": scale, "seed": scale,
+                       "row_blocks": blocks, "nnz_A": int(cols.size)},
+            "ms": tot["ms"], "products": tot["products"], "nnz_C": tot["nnz"],
+            "slots_over_nnz": tot["capacity"] / max(tot["nnz"], 1), "spilled_rows": tot["spilled_rows"],
+            "fallback_rows": tot["fallback_rows"], "rows": int(rows.size)}
+
+
 # --------------------------------------------------------------------- main --
 def main():
     ap = argparse.ArgumentParser()
@@ -699,12 +742,15 @@ def main():
                     help="left operand = this seeded fraction of A's stored rows (profiling captures)")
     ap.add_argument("--ref-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="rmat", choices=["rmat", "batch", "poisson4096", "cfpq", "kron"],
+    ap.add_argument("--workload", default="rmat",
+                    choices=["rmat", "batch", "poisson4096", "cfpq", "kron", "rmat21"],
                     help="rmat: the headline A*A; batch / poisson4096: secondary workloads (own JSON line)")
     ap.add_argument("--pairs", type=int, default=256)
+    ap.add_argument("--blocks", type=int, default=4, help="row blocks of the scale-21 run")
     args = ap.parse_args()
     if args.workload != "rmat":
-        fn = {"batch": run_batch, "poisson4096": run_small, "cfpq": run_cfpq, "kron": run_kron}[args.workload]
+        fn = {"batch": run_batch, "poisson4096": run_small, "cfpq": run_cfpq, "kron": run_kron,
+              "rmat21": run_rmat21}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
     if args.form is None:
