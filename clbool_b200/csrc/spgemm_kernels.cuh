@@ -15,6 +15,8 @@
 //     per-word counts emits the columns already sorted (no sort pass).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace clb {
@@ -374,7 +376,8 @@ __device__ __forceinline__ void block_bitonic_sort(uint32_t *s, uint32_t M) {
 // idx is the product's index in the row's flattened product list.
 template <int NT, int ECH, int U, class F>
 __device__ __forceinline__ void balanced_products(const AView &a, const BRows &b, uint32_t i, uint32_t *s_pre,
-                                                  uint32_t *s_beg, uint32_t *scratch, F &&f) {
+                                                  uint32_t *s_beg, uint32_t *scratch, F &&f, uint32_t part = 0,
+                                                  uint32_t nparts = 1) {
     constexpr int EPT = ECH / NT;
     constexpr int NW = NT / 32;
     constexpr uint32_t WCH = 32u * U;
@@ -409,7 +412,8 @@ __device__ __forceinline__ void balanced_products(const AView &a, const BRows &b
         if (threadIdx.x == 0) s_pre[n] = total;
         __syncthreads();
         uint32_t e = 0;  // lane's entry cursor, carried from chunk to chunk
-        for (uint32_t base = w * WCH; base < total; base += NW * WCH) {
+        // the CTAs of a cluster (part of nparts) interleave the warp chunks
+        for (uint32_t base = (part * NW + w) * WCH; base < total; base += nparts * NW * WCH) {
             const uint32_t p = base + lane;
             {   // largest e in [e, n) with s_pre[e] <= p: short linear walk,
                 // binary search when the cursor is more than 8 entries behind
@@ -655,7 +659,8 @@ __device__ __forceinline__ void unit_products(const AView &a, const BRows &b, ui
     }
 }
 
-// Single-chunk insertion (all columns fit the bitmap).  Units are the
+// Single-chunk insertion (all columns fit the bitmap, or the cluster's
+// bitmaps: `set_bit(c)` sets column c wherever it lives).  Units are the
 // intersections of a B row with ALIGNED windows of 2^shift positions of
 // B.cols, so all but a row's first and last unit are whole windows.  A warp
 // sweeps 256 positions at a time; lane l takes the 8 consecutive positions
@@ -667,10 +672,11 @@ __device__ __forceinline__ void unit_products(const AView &a, const BRows &b, ui
 // covers a valid position, so it never leaves the 16-byte block of a valid
 // column.  Columns are clamped to the bitmap (memory safety on malformed
 // input).  Requires B.nnz <= 2^32 - 4096.
-template <int NT, int ECH>
+template <int NT, int ECH, class SetBit>
 __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b, uint32_t i, uint32_t shift,
-                                                  uint32_t maxcol, uint32_t *bm, uint32_t *s_beg, uint32_t *s_len,
-                                                  uint32_t *s_upre, uint32_t *scratch) {
+                                                  uint32_t maxcol, SetBit &&set_bit, uint32_t *s_beg, uint32_t *s_len,
+                                                  uint32_t *s_upre, uint32_t *scratch, uint32_t part = 0,
+                                                  uint32_t nparts = 1) {
     static_assert(ECH % NT == 0, "entry chunk must be a multiple of the block");
     constexpr int EPT = ECH / NT;
     constexpr int NW = NT / 32;
@@ -705,7 +711,7 @@ __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b
         if (threadIdx.x == 0) s_upre[n] = total;
         __syncthreads();
         uint32_t e = 0;  // warp-uniform entry cursor
-        for (uint32_t u = w; u < total; u += NW) {
+        for (uint32_t u = part * NW + w; u < total; u += nparts * NW) {
             for (;;) {
                 const uint32_t idx = e + 1 + lane;
                 const bool le = idx <= n && s_upre[idx] <= u;
@@ -737,8 +743,7 @@ __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b
                 for (int j = 0; j < 8; ++j) {
                     const uint32_t q = p0 + (uint32_t)j;
                     if (q >= vlo && q < vhi) {
-                        const uint32_t c = min(v[j], maxcol);
-                        atomicOr(bm + (c >> 5), 1u << (c & 31));
+                        set_bit(min(v[j], maxcol));
                     }
                 }
             }
@@ -747,6 +752,139 @@ __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b
     }
 }
 
+// ---- chunk counting and emission, shared by the bitmap kernels ----------
+
+// Pop-counts and clears `words` words of the bitmap; returns the block's sum.
+template <int BMP_NT>
+__device__ __forceinline__ uint32_t bitmap_count_clear(uint4 *bm4, uint32_t words, uint32_t *scratch) {
+    uint32_t mine = 0;
+    for (uint32_t w4 = threadIdx.x; w4 < words / 4; w4 += BMP_NT) {
+        const uint4 x = bm4[w4];
+        mine += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+        bm4[w4] = make_uint4(0, 0, 0, 0);
+    }
+    return block_sum<uint32_t, BMP_NT>(mine, scratch);
+}
+
+// Counts the set bits of the `nsteps` 128-word steps and lists the non-empty
+// ones: s_list[g] = step, s_soff[g] = its first output, s_soff[nlist] =
+// total.  TPS threads count one step (32 uint4); thread TPS*s ends up holding
+// step s; one block scan of (count << 11 | nonempty) gives both offsets
+// (counts <= 4096 per step, <= 2^20 per chunk; flags <= 256 < 2^11).
+// Resets *s_next and ends with a block barrier.
+template <int BMP_NT>
+__device__ __forceinline__ uint32_t bitmap_list_steps(const uint4 *bm4, uint32_t nsteps, uint32_t *s_list,
+                                                      uint32_t *s_soff, uint32_t *s_next, uint32_t *scratch,
+                                                      uint32_t &nlist) {
+    constexpr int TPS = BMP_NT / (int)BMP_MAX_STEPS;
+    static_assert(TPS >= 1 && TPS <= 32 && (TPS & (TPS - 1)) == 0, "block size");
+    uint32_t scnt = 0;
+    if (threadIdx.x / TPS < nsteps) {
+        const uint4 *p4 = bm4 + (threadIdx.x / TPS) * 32 + (threadIdx.x % TPS) * (32 / TPS);
+#pragma unroll 8
+        for (int k = 0; k < 32 / TPS; ++k) {
+            const uint4 x = p4[k];
+            scnt += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+        }
+    }
+#pragma unroll
+    for (int d = 1; d < TPS; d <<= 1) scnt += __shfl_xor_sync(0xFFFFFFFFu, scnt, d);
+    if ((threadIdx.x % TPS) != 0) scnt = 0;
+    uint32_t ptot;
+    const uint32_t ex = block_exclusive_scan<uint32_t, BMP_NT>((scnt << 11) | (scnt ? 1u : 0u), scratch, &ptot);
+    const uint32_t ctot = ptot >> 11;
+    nlist = ptot & 0x7FFu;
+    if (scnt) {
+        s_list[ex & 0x7FFu] = threadIdx.x / TPS;
+        s_soff[ex & 0x7FFu] = ex >> 11;
+    }
+    if (threadIdx.x == 0) {
+        s_soff[nlist] = ctot;
+        *s_next = 0;
+    }
+    __syncthreads();
+    return ctot;
+}
+
+// Emits the listed steps as sorted columns colbase + bit index to out[],
+// clearing the bitmap.  Warps take steps dynamically; for a step, lane l
+// holds words 4l..4l+3 and a warp scan of their counts places them; the
+// step's outputs are produced in windows of up to BMP_STAGE: the window's
+// outputs are split evenly over the lanes, each lane finds the word and bit
+// of its first output (shuffle search over the scan, then nth_set_bit) and
+// walks the bitmap from there into the warp's staging buffer, which the warp
+// copies out with coalesced stores.  Cost follows the non-empty steps and the
+// output, not the bitmap width.  The caller synchronises the block after.
+__device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t nlist, const uint32_t *s_list,
+                                            const uint32_t *s_soff, uint32_t *s_next, uint32_t *stage, uint32_t *out,
+                                            uint32_t colbase) {
+    const uint32_t lane = lane_id();
+    for (;;) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(s_next, 1u);
+        g = __shfl_sync(0xFFFFFFFFu, g, 0);
+        if (g >= nlist) break;
+        const uint32_t st = s_list[g];
+        const uint32_t pos = s_soff[g];
+        const uint32_t T = s_soff[g + 1] - pos;
+        const uint32_t q4 = st * 32u + lane;  // lane's uint4 of the step
+        const uint4 x = bm4[q4];
+        const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+        const uint32_t inc = warp_inclusive_scan(pc);
+        for (uint32_t w0 = 0; w0 < T; w0 += BMP_STAGE) {
+            const uint32_t m = min(BMP_STAGE, T - w0);
+            const uint32_t per = (m + 31) >> 5;  // outputs per lane
+            const uint32_t k = w0 + lane * per;
+            const uint32_t kend = min(k + per, w0 + m);
+            const uint32_t key = min(k, T - 1);
+            // L = first lane whose inclusive count exceeds key
+            uint32_t L = 0;
+#pragma unroll
+            for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
+                const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, L + sft - 1);
+                if (v <= key) L += sft;
+            }
+            const uint32_t exL = __shfl_sync(0xFFFFFFFFu, inc - pc, L);
+            if (k < kend) {
+                const uint4 y = bm4[st * 32u + L];
+                uint32_t r = key - exL, wv = y.x, widx = (st * 32u + L) * 4u, c;
+                c = __popc(y.x);
+                if (r >= c) {
+                    r -= c; wv = y.y; ++widx; c = __popc(y.y);
+                    if (r >= c) {
+                        r -= c; wv = y.z; ++widx; c = __popc(y.z);
+                        if (r >= c) { r -= c; wv = y.w; ++widx; }
+                    }
+                }
+                uint32_t cur = wv & (0xFFFFFFFFu << nth_set_bit(wv, r));
+                for (uint32_t kk = k; kk < kend; ++kk) {
+                    while (!cur) cur = bm[++widx];  // the step holds more outputs
+                    stage[kk - w0] = colbase + widx * 32u + (uint32_t)(__ffs(cur) - 1);
+                    cur &= cur - 1;
+                }
+            }
+            __syncwarp();
+            for (uint32_t t = lane; t < m; t += 32) out[pos + w0 + t] = stage[t];
+            __syncwarp();
+        }
+        if (pc) bm4[q4] = make_uint4(0, 0, 0, 0);
+    }
+}
+
+// Shared-memory layout of the bitmap kernels (32-bit words, bitmap of W).
+struct BitmapSmem {
+    uint32_t *bm, *s_beg, *s_len, *s_upre, *s_list, *s_soff, *s_stage;
+    __device__ __forceinline__ BitmapSmem(uint32_t *smem, uint32_t W) {
+        bm = smem;
+        s_beg = smem + W;
+        s_len = s_beg + BMP_ECH;
+        s_upre = s_len + BMP_ECH;             // BMP_ECH + 1
+        s_list = s_upre + BMP_ECH + 1;        // BMP_MAX_STEPS
+        s_soff = s_list + BMP_MAX_STEPS;      // BMP_MAX_STEPS + 1
+        s_stage = s_soff + BMP_MAX_STEPS + 1; // (threads / 32) * BMP_STAGE
+    }
+};
+
 // Rows of bins [bin_lo, bin_hi] (contiguous in the list, heaviest first),
 // one row per CTA at a time, taken from `counter`.  MULTI: the columns do
 // not fit one bitmap chunk, so every chunk re-walks the row's products.
@@ -754,31 +892,15 @@ __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b
 // the 32 warps of a lighter row still get several units each).  Plain
 // shared atomics: B rows are mostly sparse over 2^20 columns, and warp-level
 // aggregation of same-word bits cost more instructions than the conflicts
-// it saved (measured on R-MAT scale 20).
-//
-// Emission of a chunk, in steps of 128 words (4096 columns): groups of four
-// threads count one step; one block scan of (count << 11 | nonempty) gives
-// every non-empty step a slot in a compact list and its output offset.
-// Warps take list entries dynamically.  For a step, lane l holds words
-// 4l..4l+3 and a warp scan of their counts places them; the step's outputs
-// are then produced in windows of up to BMP_STAGE: the window's outputs are
-// split evenly over the lanes, each lane finds the word and bit of its first
-// output (shuffle search over the scan, then nth_set_bit) and walks the
-// bitmap from there, writing into the warp's staging buffer, which the warp
-// copies to C with coalesced stores.  Cost follows the non-empty steps and
-// the output, not the bitmap width, and is even across lanes.
+// it saved (measured on R-MAT scale 20).  Emission in 128-word steps
+// (bitmap_list_steps, bitmap_emit).
 template <bool NUMERIC, bool MULTI, int BMP_NT>
 __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLists bl, int bin_lo, int bin_hi, AView a, BRows b,
                                                                RowOut o, uint64_t ncols, uint32_t W,
                                                                uint32_t *counter) {
     extern __shared__ __align__(16) uint32_t smem[];
-    uint32_t *bm = smem;
-    uint32_t *s_beg = smem + W;
-    uint32_t *s_len = s_beg + BMP_ECH;
-    uint32_t *s_upre = s_len + BMP_ECH;             // BMP_ECH + 1
-    uint32_t *s_list = s_upre + BMP_ECH + 1;        // BMP_MAX_STEPS
-    uint32_t *s_soff = s_list + BMP_MAX_STEPS;      // BMP_MAX_STEPS + 1
-    uint32_t *s_stage = s_soff + BMP_MAX_STEPS + 1; // (BMP_NT / 32) * BMP_STAGE
+    const BitmapSmem S(smem, W);
+    uint32_t *const bm = S.bm;
     __shared__ uint32_t scratch[33];
     __shared__ uint32_t s_slot, s_next;
     __shared__ unsigned long long s_spill;
@@ -789,11 +911,8 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
     const uint32_t nheavy = bin_hi > bin_lo ? cnt - bl.info[bin_hi] : 0;
     for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) bm[w] = 0;
     __syncthreads();
-    const uint32_t lane = lane_id(), wi = warp_id();
-    constexpr int TPS = BMP_NT / (int)BMP_MAX_STEPS;  // counting threads per step
-    static_assert(TPS >= 1 && TPS <= 32 && (TPS & (TPS - 1)) == 0, "block size");
     uint4 *bm4 = reinterpret_cast<uint4 *>(bm);
-    uint32_t *const stage = s_stage + wi * BMP_STAGE;
+    uint32_t *const stage = S.s_stage + warp_id() * BMP_STAGE;
     for (;;) {
         const uint32_t item = next_item(counter, &s_slot);
         if (item >= cnt) break;
@@ -813,58 +932,28 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
         bool overflowed = false;
         for (uint64_t c0 = 0; c0 < (MULTI ? rn : 1); c0 += chunk_cols) {
             if (MULTI) {
-                unit_products<BMP_NT, BMP_ECH>(a, b, i, shift, s_beg, s_len, s_upre, scratch,
+                unit_products<BMP_NT, BMP_ECH>(a, b, i, shift, S.s_beg, S.s_len, S.s_upre, scratch,
                                                [&](uint32_t c, bool valid) {
                     const uint64_t r = (uint64_t)c - c0;  // wraps for columns below c0
                     if (valid && r < chunk_cols) atomicOr(bm + (r >> 5), 1u << (r & 31));
                 });
             } else if (short_b) {
                 // many short B rows: per-product mapping over the whole row
-                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, s_upre, s_beg, scratch,
+                balanced_products<BMP_NT, BMP_ECH, 4>(a, b, i, S.s_upre, S.s_beg, scratch,
                                                       [&](uint32_t c, bool valid, uint32_t) {
                     if (valid && c < (uint32_t)chunk_cols) atomicOr(bm + (c >> 5), 1u << (c & 31));
                 });
             } else {
-                bitmap_insert_row<BMP_NT, BMP_ECH>(a, b, i, shift, (uint32_t)(chunk_cols - 1), bm, s_beg, s_len,
-                                                   s_upre, scratch);
+                bitmap_insert_row<BMP_NT, BMP_ECH>(a, b, i, shift, (uint32_t)(chunk_cols - 1),
+                                                   [&](uint32_t c) { atomicOr(bm + (c >> 5), 1u << (c & 31)); },
+                                                   S.s_beg, S.s_len, S.s_upre, scratch);
             }
             if (!NUMERIC || overflowed) {
-                uint32_t mine = 0;
-                for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) {
-                    const uint4 x = bm4[w4];
-                    mine += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
-                    bm4[w4] = make_uint4(0, 0, 0, 0);
-                }
-                total += block_sum<uint32_t, BMP_NT>(mine, scratch);
+                total += bitmap_count_clear<BMP_NT>(bm4, Wr, scratch);
                 continue;
             }
-            // TPS threads count one 128-word step (32 uint4), thread TPS*s
-            // ends up holding step s
-            uint32_t scnt = 0;
-            if (threadIdx.x / TPS < nsteps) {
-                const uint4 *p4 = bm4 + (threadIdx.x / TPS) * 32 + (threadIdx.x % TPS) * (32 / TPS);
-#pragma unroll 8
-                for (int k = 0; k < 32 / TPS; ++k) {
-                    const uint4 x = p4[k];
-                    scnt += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
-                }
-            }
-#pragma unroll
-            for (int d = 1; d < TPS; d <<= 1) scnt += __shfl_xor_sync(0xFFFFFFFFu, scnt, d);
-            if ((threadIdx.x % TPS) != 0) scnt = 0;
-            // counts <= 4096 per step, <= 2^20 per chunk; flags <= 256 < 2^11
-            uint32_t ptot;
-            const uint32_t ex = block_exclusive_scan<uint32_t, BMP_NT>((scnt << 11) | (scnt ? 1u : 0u), scratch, &ptot);
-            const uint32_t ctot = ptot >> 11, nlist = ptot & 0x7FFu;
-            if (scnt) {
-                s_list[ex & 0x7FFu] = threadIdx.x / TPS;
-                s_soff[ex & 0x7FFu] = ex >> 11;
-            }
-            if (threadIdx.x == 0) {
-                s_soff[nlist] = ctot;
-                s_next = 0;
-            }
-            __syncthreads();
+            uint32_t nlist;
+            const uint32_t ctot = bitmap_list_steps<BMP_NT>(bm4, nsteps, S.s_list, S.s_soff, &s_next, scratch, nlist);
             uint32_t *out = o.cols + out_base + total;
             if (o.row_cap && total + ctot > o.row_cap[i]) {
                 // single-pass forms: the row does not fit its slot.  A
@@ -888,57 +977,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 out = o.arena + s_spill;
                 if (threadIdx.x == 0) o.spill[i] = s_spill;
             }
-            for (;;) {
-                uint32_t g = 0;
-                if (lane == 0) g = atomicAdd(&s_next, 1u);
-                g = __shfl_sync(0xFFFFFFFFu, g, 0);
-                if (g >= nlist) break;
-                const uint32_t st = s_list[g];
-                const uint32_t pos = s_soff[g];
-                const uint32_t T = s_soff[g + 1] - pos;
-                const uint32_t q4 = st * 32u + lane;  // lane's uint4 of the step
-                const uint4 x = bm4[q4];
-                const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
-                const uint32_t inc = warp_inclusive_scan(pc);
-                const uint32_t colbase = (uint32_t)c0;
-                for (uint32_t w0 = 0; w0 < T; w0 += BMP_STAGE) {
-                    const uint32_t m = min(BMP_STAGE, T - w0);
-                    const uint32_t per = (m + 31) >> 5;  // outputs per lane
-                    const uint32_t k = w0 + lane * per;
-                    const uint32_t kend = min(k + per, w0 + m);
-                    const uint32_t key = min(k, T - 1);
-                    // L = first lane whose inclusive count exceeds key
-                    uint32_t L = 0;
-#pragma unroll
-                    for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
-                        const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, L + sft - 1);
-                        if (v <= key) L += sft;
-                    }
-                    const uint32_t exL = __shfl_sync(0xFFFFFFFFu, inc - pc, L);
-                    if (k < kend) {
-                        const uint4 y = bm4[st * 32u + L];
-                        uint32_t r = key - exL, wv = y.x, widx = (st * 32u + L) * 4u, c;
-                        c = __popc(y.x);
-                        if (r >= c) {
-                            r -= c; wv = y.y; ++widx; c = __popc(y.y);
-                            if (r >= c) {
-                                r -= c; wv = y.z; ++widx; c = __popc(y.z);
-                                if (r >= c) { r -= c; wv = y.w; ++widx; }
-                            }
-                        }
-                        uint32_t cur = wv & (0xFFFFFFFFu << nth_set_bit(wv, r));
-                        for (uint32_t kk = k; kk < kend; ++kk) {
-                            while (!cur) cur = bm[++widx];  // the step holds more outputs
-                            stage[kk - w0] = colbase + widx * 32u + (uint32_t)(__ffs(cur) - 1);
-                            cur &= cur - 1;
-                        }
-                    }
-                    __syncwarp();
-                    for (uint32_t t = lane; t < m; t += 32) out[pos + w0 + t] = stage[t];
-                    __syncwarp();
-                }
-                if (pc) bm4[q4] = make_uint4(0, 0, 0, 0);
-            }
+            bitmap_emit(bm, bm4, nlist, S.s_list, S.s_soff, &s_next, stage, out, (uint32_t)c0);
             total += ctot;
             __syncthreads();
         }
@@ -950,6 +989,129 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 else o.row_nnz[i] = (uint32_t)total;
             }
         }
+    }
+}
+
+// Columns per CTA of the cluster bitmap kernel.
+constexpr uint32_t CLB_CHUNK_SHIFT = 20;
+
+// Rows with 2^20 < ncols <= CL * 2^20: the CL CTAs of a thread-block cluster
+// hold one 2^20-column slice of the row's bitmap each, in their own shared
+// memory, and work on ONE row together.  Every CTA stages the row's A
+// entries and takes its share of the insertion units; each product sets its
+// bit in the owning CTA's slice through distributed shared memory (atomicOr
+// on the mapped address).  After a cluster barrier every CTA counts its
+// slice, the counts are exchanged through distributed shared memory, and
+// each CTA emits its slice at its offset (the columns of lower slices come
+// first).  One pass over the products instead of one per 2^20-column chunk.
+// All control flow that reaches a cluster barrier is cluster-uniform: the
+// row index is fetched by rank 0 and broadcast, and every decision after it
+// depends only on values all CTAs share.
+template <bool NUMERIC, int CL>
+__global__ void __launch_bounds__(1024, 1) bitmap_cluster_kernel(BinLists bl, int bin_lo, int bin_hi, AView a, BRows b,
+                                                                 RowOut o, uint64_t ncols, uint32_t *counter) {
+    constexpr int NT = 1024;
+    constexpr uint32_t W = 1u << (CLB_CHUNK_SHIFT - 5);  // words per CTA
+    extern __shared__ __align__(16) uint32_t smem[];
+    const BitmapSmem S(smem, W);
+    uint32_t *const bm = S.bm;
+    __shared__ uint32_t scratch[33];
+    __shared__ uint32_t s_item, s_next;
+    __shared__ uint32_t s_counts[CL];
+    __shared__ unsigned long long s_spill;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const uint32_t rank = cluster.block_rank();
+    uint32_t *slices[CL];
+#pragma unroll
+    for (int q = 0; q < CL; ++q) slices[q] = cluster.map_shared_rank(bm, q);
+    uint32_t beg, cnt = 0, tmp;
+    bin_range(bl, bin_lo, beg, tmp);
+    for (int q = bin_lo; q <= bin_hi; ++q) cnt += bl.info[q];
+    const uint32_t nheavy = bin_hi > bin_lo ? cnt - bl.info[bin_hi] : 0;
+    for (uint32_t w = threadIdx.x; w < W; w += NT) bm[w] = 0;
+    uint4 *bm4 = reinterpret_cast<uint4 *>(bm);
+    uint32_t *const stage = S.s_stage + warp_id() * BMP_STAGE;
+    const uint32_t maxcol = (uint32_t)min(ncols, (uint64_t)CL << CLB_CHUNK_SHIFT) - 1;
+    for (;;) {
+        // every slice is clear and every CTA done with the previous row
+        cluster.sync();
+        if (rank == 0 && threadIdx.x == 0) {
+            const uint32_t it = atomicAdd(counter, 1u);
+#pragma unroll
+            for (int q = 0; q < CL; ++q) *cluster.map_shared_rank(&s_item, q) = it;
+        }
+        cluster.sync();
+        const uint32_t item = s_item;
+        if (item >= cnt) break;  // cluster-uniform
+        const uint32_t i = bl.list[beg + item];
+        const uint32_t shift = item < nheavy ? 9u : 8u;
+        const bool short_b = o.row_products &&
+                             (uint64_t)o.row_products[i] < (uint64_t)BMP_SHORT * (a.rpt[i + 1] - a.rpt[i]);
+        auto set_bit = [&](uint32_t c) {
+            const uint32_t q = c >> CLB_CHUNK_SHIFT;
+            uint32_t *sl = slices[0];  // select, not an indexed (local-memory) load
+#pragma unroll
+            for (int k = 1; k < CL; ++k)
+                if (q == (uint32_t)k) sl = slices[k];
+            atomicOr(sl + ((c & ((1u << CLB_CHUNK_SHIFT) - 1)) >> 5), 1u << (c & 31));
+        };
+        if (short_b) {
+            balanced_products<NT, BMP_ECH, 4>(a, b, i, S.s_upre, S.s_beg, scratch,
+                                              [&](uint32_t c, bool valid, uint32_t) {
+                if (valid) set_bit(min(c, maxcol));
+            }, rank, CL);
+        } else {
+            bitmap_insert_row<NT, BMP_ECH>(a, b, i, shift, maxcol, set_bit, S.s_beg, S.s_len, S.s_upre, scratch, rank,
+                                           CL);
+        }
+        cluster.sync();  // every product's bit is set, in every slice
+        uint32_t nlist = 0, ctot;
+        if (NUMERIC)
+            ctot = bitmap_list_steps<NT>(bm4, W / BMP_STEP_WORDS, S.s_list, S.s_soff, &s_next, scratch, nlist);
+        else
+            ctot = bitmap_count_clear<NT>(bm4, W, scratch);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int q = 0; q < CL; ++q) cluster.map_shared_rank(s_counts, q)[rank] = ctot;
+        }
+        cluster.sync();
+        uint64_t before = 0, total = 0;
+#pragma unroll
+        for (int q = 0; q < CL; ++q) {
+            before += (uint32_t)q < rank ? s_counts[q] : 0u;
+            total += s_counts[q];
+        }
+        if (!NUMERIC) {
+            if (rank == 0 && threadIdx.x == 0) o.row_nnz[i] = (uint32_t)total;
+            continue;
+        }
+        uint32_t *out = o.cols + o.row_off[i];
+        if (o.row_cap && total > o.row_cap[i]) {
+            // over the slot: rank 0 reserves the whole row in the spill
+            // arena and broadcasts the offset (~0: no room -> exact rerun)
+            if (rank == 0 && threadIdx.x == 0) {
+                unsigned long long at = ~0ull;
+                if (o.arena) {
+                    at = atomicAdd(o.arena_cursor, (unsigned long long)total);
+                    if (at + total > o.arena_cap) at = ~0ull;
+                }
+#pragma unroll
+                for (int q = 0; q < CL; ++q) *cluster.map_shared_rank(&s_spill, q) = at;
+                if (o.spill) o.spill[i] = at;
+                if (at == ~0ull) o.overflow[i] = 1;
+            }
+            cluster.sync();
+            if (s_spill == ~0ull) {
+                for (uint32_t w4 = threadIdx.x; w4 < W / 4; w4 += NT) bm4[w4] = make_uint4(0, 0, 0, 0);
+                __syncthreads();
+                continue;
+            }
+            out = o.arena + s_spill;
+        }
+        bitmap_emit(bm, bm4, nlist, S.s_list, S.s_soff, &s_next, stage, out + before, rank << CLB_CHUNK_SHIFT);
+        if (o.row_cap && rank == 0 && threadIdx.x == 0) o.row_nnz[i] = (uint32_t)total;
+        __syncthreads();
     }
 }
 

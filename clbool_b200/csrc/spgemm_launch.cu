@@ -149,9 +149,51 @@ int launch_bitmap_nt(clb_controls *ctl, const BinLists &bl, const AView &a, cons
                  : launch_bitmap_t<NUM, false, NT>(ctl, bl, a, b, o, ncols, nmax, counter, name);
 }
 
+// Rows wider than one bitmap chunk (2^20 < ncols <= CL * 2^20): one row per
+// thread-block cluster of CL CTAs, each holding a 2^20-column slice.
+template <bool NUM, int CL>
+int launch_bitmap_cluster(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
+                          uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name) {
+    const size_t smem = bitmap_smem_bytes(1u << (CLB_CHUNK_SHIFT - 5), 1024);
+    auto kern = bitmap_cluster_kernel<NUM, CL>;
+    CLB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 CLB_RUN_KERNEL_FAILURE);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CL);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctl->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        clusters = 1;
+    }
+    if ((uint64_t)clusters > nmax) clusters = (int)(nmax ? nmax : 1);
+    cfg.gridDim = dim3((unsigned)(clusters * CL));
+    ProfScope ps(ctl, name);
+    CLB_TRY_CUDA(cudaLaunchKernelEx(&cfg, kern, bl, (int)BIN_BMP_XL, (int)BIN_BMP, a, b, o, ncols, counter),
+                 CLB_RUN_KERNEL_FAILURE);
+    ctl->launches += 1;
+    return CLB_SUCCESS;
+}
+
 template <bool NUM>
 int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
                   uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name, uint32_t threads) {
+    // wider than one chunk, uniform width: a cluster holds the whole row
+    if (!o.row_ncols && ncols > (1ull << CLB_CHUNK_SHIFT)) {
+        if (ncols <= (2ull << CLB_CHUNK_SHIFT))
+            return launch_bitmap_cluster<NUM, 2>(ctl, bl, a, b, o, ncols, nmax, counter, name);
+        if (ncols <= (4ull << CLB_CHUNK_SHIFT))
+            return launch_bitmap_cluster<NUM, 4>(ctl, bl, a, b, o, ncols, nmax, counter, name);
+    }
     if (threads <= 256) return launch_bitmap_nt<NUM, 256>(ctl, bl, a, b, o, ncols, nmax, counter, name);
     if (threads <= 512) return launch_bitmap_nt<NUM, 512>(ctl, bl, a, b, o, ncols, nmax, counter, name);
     return launch_bitmap_nt<NUM, 1024>(ctl, bl, a, b, o, ncols, nmax, counter, name);

@@ -271,13 +271,38 @@ def test_packaged_checkpoint_rmat16(controls):
     assert st["capacity"] < 1.5 * len(want.cols)
 
 
+def _wide_pair(n, seed):
+    rng = np.random.default_rng(seed)
+    ra = np.repeat(np.arange(64, dtype=np.uint32), 40)
+    ca = rng.integers(0, 3000, ra.size).astype(np.uint32)
+    a = O.coo_to_dcsr(O.Coo(64, 3000, *O.unique_pairs(*O.sort_pairs(ra, ca))))
+    rb = np.repeat(np.arange(3000, dtype=np.uint32), 200)
+    cbb = rng.integers(0, n, rb.size).astype(np.uint32)
+    b = O.coo_to_dcsr(O.Coo(3000, n, *O.unique_pairs(*O.sort_pairs(rb, cbb))))
+    return a, b
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [(1 << 20) + 3, (1 << 21) + 5, (3 << 20) + 9])
+def test_learned_spill_on_cluster_rows(controls, n):
+    """Columns past one bitmap chunk but within four: a thread-block cluster
+    holds the row, knows its exact count after insertion, and spills rows
+    over their slot in the same pass; C is the oracle's product."""
+    from clbool_b200 import sizing
+    a, b = _wide_pair(n, 13)
+    s = sizing.RowSizer(controls, seed=4)
+    got, st = _learned(controls, a, b, s, margin=-1000.0, slack=0.0)
+    assert_dcsr_equal(got, O.spgemm(a, b), f"cluster learned n={n}")
+    assert st["spilled_rows"] > 0 and st["fallback_rows"] == 0
+
+
 @pytest.mark.gpu
 def test_learned_fallback_on_wide_rows(controls):
-    """Columns past one bitmap chunk (2^21 + 5): bitmap rows over their slot
+    """Columns past four bitmap chunks (2^22 + 5): bitmap rows over their slot
     cannot spill (their count is only known after the last chunk), so they
     take the exact two-pass fallback; C is still the oracle's product."""
     from clbool_b200 import sizing
-    n = (1 << 21) + 5
+    n = (1 << 22) + 5
     rng = np.random.default_rng(12)
     ra = np.repeat(np.arange(64, dtype=np.uint32), 40)
     ca = rng.integers(0, 3000, ra.size).astype(np.uint32)
