@@ -47,12 +47,13 @@ class clb_spgemm_stats(C.Structure):
 
 class clb_spgemm_tuning(C.Structure):
     _fields_ = [("form", C.c_uint32), ("warp_max", C.c_uint32), ("bitmap_min", C.c_uint32),
-                ("bitmap_threads", C.c_uint32), ("small_lanes", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("bitmap_threads", C.c_uint32), ("small_lanes", C.c_uint32), ("wide_rows", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
     def as_dict(self) -> dict:
         return {"form": "two_pass" if self.form == 0 else "single_pass", "warp_max": self.warp_max,
                 "bitmap_min": self.bitmap_min, "bitmap_threads": self.bitmap_threads,
-                "small_lanes": self.small_lanes}
+                "small_lanes": self.small_lanes, "wide_rows": {1: "cluster", 2: "chunks"}.get(self.wide_rows, "chunks")}
 
 
 P = C.POINTER
@@ -114,8 +115,8 @@ _SIGS = {
     "clb_sizer_gradients": (C.c_int, [vp, vp, vp, C.c_uint64, vp, P(C.c_float)]),
     "clb_sizer_train": (C.c_int, [vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64,
                                   P(C.c_float)]),
-    "clb_dcsr_spgemm_learned": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, C.c_float, C.c_float, P(clb_dcsr),
-                                          P(clb_spgemm_stats)]),
+    "clb_dcsr_spgemm_learned": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, C.c_float, C.c_float,
+                                          P(clb_spgemm_tuning), P(clb_dcsr), P(clb_spgemm_stats)]),
     # tuning and batching
     "clb_spgemm_tuning_default": (None, [P(clb_spgemm_tuning)]),
     "clb_dcsr_spgemm_tuned": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_tuning), P(clb_dcsr),

@@ -15,7 +15,7 @@ from .core import ClBoolException, Controls, check, matrix_dcsr
 
 
 def tuning(form: str | int = "two_pass", warp_max: int = 0, bitmap_min: int = 0, bitmap_threads: int = 0,
-           small_lanes: int = 0) -> clb_spgemm_tuning:
+           small_lanes: int = 0, wide_rows: str = "") -> clb_spgemm_tuning:
     """A tuning; zero fields take the library defaults."""
     t = clb_spgemm_tuning()
     lib.clb_spgemm_tuning_default(C.byref(t))
@@ -28,6 +28,8 @@ def tuning(form: str | int = "two_pass", warp_max: int = 0, bitmap_min: int = 0,
         t.bitmap_threads = bitmap_threads
     if small_lanes:
         t.small_lanes = small_lanes
+    if wide_rows:
+        t.wide_rows = {"cluster": 1, "chunks": 2}[wide_rows]
     return t
 
 

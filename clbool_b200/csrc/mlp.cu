@@ -526,8 +526,11 @@ int clb_sizer_train(clb_sizer *s, const float *features, const float *targets, u
 }
 
 int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a_, const clb_dcsr *b_, const clb_sizer *sizer,
-                            float margin_log2, float slack, clb_dcsr *c, clb_spgemm_stats *stats) {
+                            float margin_log2, float slack, const clb_spgemm_tuning *tuning, clb_dcsr *c,
+                            clb_spgemm_stats *stats) {
     if (!ctl || !a_ || !b_ || !c || !sizer) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    CLB_RETURN_IF(check_tuning(tuning));
+    const Tuning t = to_tuning(tuning);
     const clb_dcsr A = *a_, B = *b_;
     CLB_RETURN_IF(validate_spgemm(A, B));
     DeviceGuard g(ctl);
@@ -559,7 +562,7 @@ int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a_, const clb_dcs
         ProfScope ps(ctl, "predict");
         predict_kernel<<<grid_for(ctl, n, MLP_NT, 4), MLP_NT, 0, ctl->stream>>>(sizer->params, feat.ptr, n, pred.ptr);
         capacity_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(pred.ptr, work.ptr, n, B.ncols, margin_log2, slack,
-                                                                  ESC_MAX_PRODUCTS, cap.ptr);
+                                                                  t.bitmap_min, cap.ptr);
         ctl->launches += 2;
         CLB_CHECK_LAUNCH();
     }
@@ -571,7 +574,7 @@ int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a_, const clb_dcs
     CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &products, 1));
     // ESC accumulators for the rows up to ESC_MAX_PRODUCTS products, learned
     // capacities and the spill arena (1/16 of the slots) for the bitmap rows
-    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st, 16);
+    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st, 16, t);
     st.kernel_launches = ctl->launches;
     if (stats) *stats = st;
     return rc;

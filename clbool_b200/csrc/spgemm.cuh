@@ -34,6 +34,9 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
                        clb_spgemm_stats *st, uint64_t arena_div, const Tuning &t = Tuning());
 // cap[i] = min(work[i], ncols): the exact upper bound of a row's count.
 int launch_upper_bound_caps(clb_controls *ctl, const uint32_t *work, uint64_t n, uint64_t ncols, uint32_t *cap);
+// Public tuning struct -> internal tuning (zero fields: defaults), and its check.
+Tuning to_tuning(const clb_spgemm_tuning *t);
+int check_tuning(const clb_spgemm_tuning *t);
 int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
                          clb_spgemm_stats *stats, const Tuning &t = Tuning());
 

@@ -103,30 +103,6 @@ unsigned stack_grid_x(const clb_controls *ctl, uint64_t largest, uint32_t count)
     return (unsigned)std::min<uint64_t>(std::max<uint64_t>(gx, 1), 65535);
 }
 
-Tuning to_tuning(const clb_spgemm_tuning *t) {
-    Tuning r;
-    if (!t) return r;
-    if (t->warp_max) r.warp_max = t->warp_max;
-    if (t->bitmap_min) r.bitmap_min = t->bitmap_min;
-    if (t->bitmap_threads) r.bitmap_threads = t->bitmap_threads;
-    if (t->small_lanes) r.small_lanes = t->small_lanes;
-    return r;
-}
-
-int check_tuning(const clb_spgemm_tuning *t) {
-    if (!t) return CLB_SUCCESS;
-    if (t->form > 1) return fail(CLB_INVALID_VALUE, "tuning.form must be 0 (two-pass) or 1 (single pass)");
-    if (t->warp_max && t->warp_max != 32 && t->warp_max != 64 && t->warp_max != 128 && t->warp_max != 256)
-        return fail(CLB_INVALID_VALUE, "tuning.warp_max must be 32, 64, 128 or 256");
-    if (t->bitmap_min && (t->bitmap_min < 256 || t->bitmap_min > ESC_MAX_PRODUCTS))
-        return fail(CLB_INVALID_VALUE, "tuning.bitmap_min must be in [256, 4096]");
-    if (t->bitmap_threads && t->bitmap_threads != 256 && t->bitmap_threads != 512 && t->bitmap_threads != 1024)
-        return fail(CLB_INVALID_VALUE, "tuning.bitmap_threads must be 256, 512 or 1024");
-    if (t->small_lanes && t->small_lanes != 8 && t->small_lanes != 16 && t->small_lanes != 32)
-        return fail(CLB_INVALID_VALUE, "tuning.small_lanes must be 8, 16 or 32");
-    return CLB_SUCCESS;
-}
-
 // One product with a tuning: the exact two-pass form or the single pass into
 // upper-bound slots (ESC accumulators for the rows below bitmap_min).
 int spgemm_tuned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, uint32_t form, const Tuning &t,
@@ -164,6 +140,32 @@ int spgemm_tuned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, uint32
 
 }  // namespace
 
+Tuning to_tuning(const clb_spgemm_tuning *t) {
+    Tuning r;
+    if (!t) return r;
+    if (t->warp_max) r.warp_max = t->warp_max;
+    if (t->bitmap_min) r.bitmap_min = t->bitmap_min;
+    if (t->bitmap_threads) r.bitmap_threads = t->bitmap_threads;
+    if (t->small_lanes) r.small_lanes = t->small_lanes;
+    if (t->wide_rows) r.wide_cluster = t->wide_rows == 1;
+    return r;
+}
+
+int check_tuning(const clb_spgemm_tuning *t) {
+    if (!t) return CLB_SUCCESS;
+    if (t->form > 1) return fail(CLB_INVALID_VALUE, "tuning.form must be 0 (two-pass) or 1 (single pass)");
+    if (t->warp_max && t->warp_max != 32 && t->warp_max != 64 && t->warp_max != 128 && t->warp_max != 256)
+        return fail(CLB_INVALID_VALUE, "tuning.warp_max must be 32, 64, 128 or 256");
+    if (t->bitmap_min && (t->bitmap_min < 256 || t->bitmap_min > ESC_MAX_PRODUCTS))
+        return fail(CLB_INVALID_VALUE, "tuning.bitmap_min must be in [256, 4096]");
+    if (t->bitmap_threads && t->bitmap_threads != 256 && t->bitmap_threads != 512 && t->bitmap_threads != 1024)
+        return fail(CLB_INVALID_VALUE, "tuning.bitmap_threads must be 256, 512 or 1024");
+    if (t->small_lanes && t->small_lanes != 8 && t->small_lanes != 16 && t->small_lanes != 32)
+        return fail(CLB_INVALID_VALUE, "tuning.small_lanes must be 8, 16 or 32");
+    if (t->wide_rows > 2) return fail(CLB_INVALID_VALUE, "tuning.wide_rows must be 1 (cluster) or 2 (chunks)");
+    return CLB_SUCCESS;
+}
+
 }  // namespace clb
 
 using namespace clb;
@@ -179,6 +181,7 @@ void clb_spgemm_tuning_default(clb_spgemm_tuning *t) {
     t->bitmap_min = d.bitmap_min;
     t->bitmap_threads = d.bitmap_threads;
     t->small_lanes = d.small_lanes;
+    t->wide_rows = d.wide_cluster ? 1 : 2;
 }
 
 int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_spgemm_tuning *tuning,
@@ -348,6 +351,11 @@ int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, co
     if (!ctl || !best) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
     DeviceGuard g(ctl);
     std::vector<clb_spgemm_tuning> cand;
+    uint64_t widest = 0;
+    for (uint32_t k = 0; k < count; ++k) widest = std::max(widest, b[k].ncols);
+    const std::vector<uint32_t> wides = widest > (1ull << CLB_CHUNK_SHIFT) ? std::vector<uint32_t>{2u, 1u}
+                                                                            : std::vector<uint32_t>{2u};
+    for (uint32_t wide : wides)
     for (uint32_t form : {0u, 1u})
         for (uint32_t bmin : {4096u, 1024u})
             for (uint32_t bthr : {1024u, 256u})
@@ -360,6 +368,7 @@ int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, co
                         t.bitmap_threads = bthr;
                         t.warp_max = wmax;
                         t.small_lanes = small;
+                        t.wide_rows = wide;
                         cand.push_back(t);
                     }
     cudaEvent_t e0, e1;

@@ -62,12 +62,18 @@ constexpr uint32_t ESC_MAX_PRODUCTS = 4096;
 //   bitmap_threads threads per bitmap row (256, 512 or 1024).
 //   small_lanes    lanes per row for the smallest rows: 8 (rows of <= 8
 //                  products share a warp four ways, <= 16 two ways), 16, or
-//                  32 (a warp per row).
+//                  32 (a warp per row);
+//   wide_cluster   rows wider than one bitmap chunk (2^20 < ncols <= 2^22):
+//                  false = one CTA walks the products once per chunk, true =
+//                  a cluster of 2 or 4 CTAs holds the whole row (one pass,
+//                  distributed shared memory; slower on R-MAT scale 21, but
+//                  such rows can spill in the learned form).
 struct Tuning {
     uint32_t warp_max = 256;
     uint32_t bitmap_min = ESC_MAX_PRODUCTS;
     uint32_t bitmap_threads = 1024;
     uint32_t small_lanes = 8;
+    bool wide_cluster = false;
     // Per A row: columns of that row's product, when they differ by row (a
     // stacked batch of pairs); null = B.ncols for every row.
     const uint32_t *row_ncols = nullptr;

@@ -186,9 +186,10 @@ int launch_bitmap_cluster(clb_controls *ctl, const BinLists &bl, const AView &a,
 
 template <bool NUM>
 int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o,
-                  uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name, uint32_t threads) {
-    // wider than one chunk, uniform width: a cluster holds the whole row
-    if (!o.row_ncols && ncols > (1ull << CLB_CHUNK_SHIFT)) {
+                  uint64_t ncols, uint64_t nmax, uint32_t *counter, const char *name, uint32_t threads,
+                  bool wide_cluster) {
+    // wider than one chunk, uniform width: a cluster can hold the whole row
+    if (wide_cluster && !o.row_ncols && ncols > (1ull << CLB_CHUNK_SHIFT)) {
         if (ncols <= (2ull << CLB_CHUNK_SHIFT))
             return launch_bitmap_cluster<NUM, 2>(ctl, bl, a, b, o, ncols, nmax, counter, name);
         if (ncols <= (4ull << CLB_CHUNK_SHIFT))
@@ -213,7 +214,8 @@ int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRow
     const uint64_t nbmp = hc ? (uint64_t)hc[BIN_BMP_XL] + hc[BIN_BMP_L] + hc[BIN_BMP] : nmax;
     if (nbmp)
         CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, a, b, o, ncols, nbmp, ctr.ptr + 0,
-                                         NUM ? "bitmap_numeric" : "bitmap_symbolic", t.bitmap_threads));
+                                         NUM ? "bitmap_numeric" : "bitmap_symbolic", t.bitmap_threads,
+                                         t.wide_cluster));
     if (hash_bins) {
         if (rows(BIN_H8K))
             CLB_RETURN_IF((launch_hash<8192, 512, NUM>(ctl, bl, BIN_H8K, a, b, o, rows(BIN_H8K), ctr.ptr + 1,

@@ -6,8 +6,10 @@ log2(1 + nnz(C row)) / 16.  Training (forward, backward, Adam) and inference
 run in the library's CUDA kernels; this module only moves arrays and files.
 
 ``matrix_multiplication_learned`` is C = A*B with one numeric pass into
-predicted capacities; rows that overflow are recomputed by the exact two-pass
-form, so the result is always identical to ``dcsr.matrix_multiplication_hash``.
+predicted capacities; a row over its slot goes to a spill arena in the same
+pass (or, where its count comes too late, is recomputed by the exact
+two-pass form), so the result is always identical to
+``dcsr.matrix_multiplication_hash``.
 """
 from __future__ import annotations
 
@@ -131,13 +133,16 @@ class RowSizer:
 
 def matrix_multiplication_learned(controls: Controls, matrix_out: matrix_dcsr | None, a: matrix_dcsr,
                                   b: matrix_dcsr, sizer: RowSizer, margin_log2: float = DEFAULT_MARGIN_LOG2,
-                                  slack: float = DEFAULT_SLACK, stats: dict | None = None) -> matrix_dcsr:
-    """C = A*B (boolean) in one numeric pass sized by `sizer`; exact."""
+                                  slack: float = DEFAULT_SLACK, stats: dict | None = None,
+                                  tune=None) -> matrix_dcsr:
+    """C = A*B (boolean) in one numeric pass sized by `sizer`; exact.
+    `tune` (optional, batched.tuning(...)) sets the accumulators."""
     out = clb_dcsr()
     st = clb_spgemm_stats()
     sa, sb = a.c_struct(), b.c_struct()
     check(lib.clb_dcsr_spgemm_learned(controls.handle, C.byref(sa), C.byref(sb), sizer.handle, float(margin_log2),
-                                      float(slack), C.byref(out), C.byref(st)), "matrix_multiplication_learned")
+                                      float(slack), C.byref(tune) if tune is not None else None, C.byref(out),
+                                      C.byref(st)), "matrix_multiplication_learned")
     res = matrix_dcsr.adopt(controls, out)
     if stats is not None:
         stats.update(st.as_dict())

@@ -426,9 +426,11 @@ private:
 // C = A*B in one numeric pass sized by the predictor; exact for any predictor.
 inline void matrix_multiplication_learned(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &a,
                                           const matrix_dcsr &b, const RowSizer &sizer, float margin_log2 = 0.25f,
-                                          float slack = 8.0f, clb_spgemm_stats *stats = nullptr) {
+                                          float slack = 8.0f, clb_spgemm_stats *stats = nullptr,
+                                          const clb_spgemm_tuning *tuning = nullptr) {
     clb_dcsr va = a.view(), vb = b.view(), out{};
-    details::check(clb_dcsr_spgemm_learned(c.get(), &va, &vb, sizer.get(), margin_log2, slack, &out, stats));
+    details::check(
+        clb_dcsr_spgemm_learned(c.get(), &va, &vb, sizer.get(), margin_log2, slack, tuning, &out, stats));
     matrix_out = matrix_dcsr::adopt(c, out);
 }
 

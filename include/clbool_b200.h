@@ -263,8 +263,10 @@ CLB_API int clb_sizer_gradients(clb_sizer *sizer, const float *features, const f
 /* Adam training over n rows (device arrays; targets = log2(1 + nnz) / 16). */
 CLB_API int clb_sizer_train(clb_sizer *sizer, const float *features, const float *targets, uint64_t n,
                             uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float *final_loss);
+/* tuning: accumulator tuning (NULL = defaults; `form` is ignored). */
 CLB_API int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_sizer *sizer,
-                                    float margin_log2, float slack, clb_dcsr *c, clb_spgemm_stats *stats);
+                                    float margin_log2, float slack, const struct clb_spgemm_tuning *tuning,
+                                    clb_dcsr *c, clb_spgemm_stats *stats);
 
 /* ------------------------------------------------- tuning and batching -- */
 /* Not in the reference.  Accumulator tuning; every setting gives the same C.
@@ -278,6 +280,9 @@ CLB_API int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a, const 
  *   bitmap_threads  threads per bitmap row: 256, 512 or 1024
  *   small_lanes     lanes per row for rows of at most 8 / 16 products: 8
  *                   (four / two rows per warp), 16, or 32 (a warp per row)
+ *   wide_rows       rows with 2^20 < ncols <= 2^22: 1 = one thread-block
+ *                   cluster (2 or 4 CTAs) per row, 2 = one CTA per row that
+ *                   walks the products once per 2^20-column chunk (default)
  * Zero fields take the defaults (clb_spgemm_tuning_default). */
 typedef struct clb_spgemm_tuning {
     uint32_t form;
@@ -285,7 +290,8 @@ typedef struct clb_spgemm_tuning {
     uint32_t bitmap_min;
     uint32_t bitmap_threads;
     uint32_t small_lanes;
-    uint32_t reserved[3];
+    uint32_t wide_rows;
+    uint32_t reserved[2];
 } clb_spgemm_tuning;
 CLB_API void clb_spgemm_tuning_default(clb_spgemm_tuning *tuning);
 /* C = A*B with a tuning (NULL = defaults, i.e. clb_dcsr_spgemm_hash). */
@@ -298,7 +304,9 @@ CLB_API int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const cl
 CLB_API int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                     clb_dcsr *c, const clb_spgemm_tuning *tuning, clb_spgemm_stats *stats);
 /* Times the batched product under every candidate tuning (32: form x
- * bitmap_min x bitmap_threads x warp_max x small_lanes) on the given pairs and returns the
+ * bitmap_min x bitmap_threads x warp_max x small_lanes; twice that with both
+ * wide_rows settings when a pair has more than 2^20 columns) on the given
+ * pairs and returns the
  * fastest in *best; tried/ms (optional, max_tried entries) receive each
  * candidate and its device time in ms, *n_tried their number. */
 CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,

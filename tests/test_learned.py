@@ -146,10 +146,10 @@ def test_training_reduces_loss(controls):
     assert abs(l2 - l1) <= 1e-5 * l1
 
 
-def _learned(ctl, a, b, sizer, margin=None, slack=None):
+def _learned(ctl, a, b, sizer, margin=None, slack=None, tune=None):
     import clbool_b200 as cb
     from clbool_b200 import sizing
-    kw = {}
+    kw = {"tune": tune}
     if margin is not None:
         kw["margin_log2"] = margin
     if slack is not None:
@@ -284,16 +284,22 @@ def _wide_pair(n, seed):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [(1 << 20) + 3, (1 << 21) + 5, (3 << 20) + 9])
-def test_learned_spill_on_cluster_rows(controls, n):
-    """Columns past one bitmap chunk but within four: a thread-block cluster
-    holds the row, knows its exact count after insertion, and spills rows
-    over their slot in the same pass; C is the oracle's product."""
-    from clbool_b200 import sizing
+@pytest.mark.parametrize("wide", ["cluster", "chunks"])
+def test_learned_wide_rows(controls, n, wide):
+    """Columns past one bitmap chunk but within four.  With a thread-block
+    cluster per row the row's exact count is known after its one insertion
+    pass, so rows over their slot spill in the same pass; walking the chunks
+    one after another they can only be recomputed (fallback).  Either way C
+    is the oracle's product."""
+    from clbool_b200 import batched, sizing
     a, b = _wide_pair(n, 13)
     s = sizing.RowSizer(controls, seed=4)
-    got, st = _learned(controls, a, b, s, margin=-1000.0, slack=0.0)
-    assert_dcsr_equal(got, O.spgemm(a, b), f"cluster learned n={n}")
-    assert st["spilled_rows"] > 0 and st["fallback_rows"] == 0
+    got, st = _learned(controls, a, b, s, margin=-1000.0, slack=0.0, tune=batched.tuning(wide_rows=wide))
+    assert_dcsr_equal(got, O.spgemm(a, b), f"learned n={n} {wide}")
+    if wide == "cluster":
+        assert st["spilled_rows"] > 0 and st["fallback_rows"] == 0
+    else:
+        assert st["fallback_rows"] > 0 and st["spilled_rows"] == 0
 
 
 @pytest.mark.gpu
