@@ -58,7 +58,7 @@ static matrix_coo_cpu_pairs pairs_of(const matrix_dcsr_cpu &m) {
     return p;
 }
 
-int main() {
+int main(int argc, char **argv) {
     Controls controls = create_controls();
     show_devices();
 
@@ -124,6 +124,19 @@ int main() {
         matrix_coo_cpu_pairs got;
         for (size_t i = 0; i < hs.rows.size(); ++i) got.push_back({hs.rows[i], hs.cols[i]});
         EXPECT(got == matrix_coo_cpu_pairs(u.begin(), u.end()));
+    }
+
+    // ---- binary DCSR files: written here, read back here and (with argv[1])
+    // left for the Python reader to check the shared format ----
+    {
+        const std::string path = argc > 1 ? argv[1] : "/tmp/clbool_b200_check.dcsr";
+        matrix_dcsr_cpu h = matrix_dcsr_from_gpu(controls, a_dcsr);
+        io::save_dcsr(path, 5, 5, h);
+        uint64_t nr = 0, nc = 0;
+        matrix_dcsr_cpu back = io::load_dcsr(path, nr, nc);
+        EXPECT(nr == 5 && nc == 5 && back.rpt == h.rpt && back.rows == h.rows && back.cols == h.cols);
+        matrix_dcsr dev = matrix_dcsr_from_cpu(controls, back, 5);
+        EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, dev)) == pairs_of(h));
     }
 
     // ---- errors surface as clbool::Exception with the reference's Status ----

@@ -19,6 +19,8 @@
 #include <clbool_b200.h>
 
 #include <cstdint>
+#include <cstring>
+#include <fstream>
 #include <iostream>
 #include <memory>
 #include <utility>
@@ -470,5 +472,126 @@ inline void matrix_addition(Controls &c, matrix_csr &out, const matrix_csr &a, c
     out = matrix_csr::adopt(c, o);
 }
 }  // namespace csr
+
+
+// ---- binary DCSR files with a checksum (same format as clbool_b200/io.py) --
+// magic "CLBDCSR1" | nrows, ncols, nnz, nzr (u64) | rpt u64[nzr+1] | rows u32[nzr]
+// | cols u32[nnz] | SHA-256 of everything before it.  Little-endian hosts.
+namespace io {
+namespace details {
+// SHA-256 (FIPS 180-4).
+class Sha256 {
+public:
+    Sha256() { reset(); }
+    void update(const uint8_t *p, size_t n) {
+        for (size_t i = 0; i < n; ++i) {
+            buf_[len_++ % 64] = p[i];
+            if (len_ % 64 == 0) block(buf_);
+        }
+    }
+    void digest(uint8_t out[32]) {
+        const uint64_t bits = len_ * 8;
+        uint8_t one = 0x80, zero = 0;
+        update(&one, 1);
+        while (len_ % 64 != 56) update(&zero, 1);
+        for (int i = 7; i >= 0; --i) {
+            uint8_t b = (uint8_t)(bits >> (8 * i));
+            update(&b, 1);
+        }
+        for (int i = 0; i < 8; ++i)
+            for (int j = 0; j < 4; ++j) out[4 * i + j] = (uint8_t)(h_[i] >> (24 - 8 * j));
+    }
+
+private:
+    static uint32_t rotr(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+    void reset() {
+        static const uint32_t h0[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                                       0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+        std::memcpy(h_, h0, sizeof(h_));
+        len_ = 0;
+    }
+    void block(const uint8_t *b) {
+        static const uint32_t k[64] = {
+            0x428a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4, 0xab1c5ed5,
+            0xd807aa98, 0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe, 0x9bdc06a7, 0xc19bf174,
+            0xe49b69c1, 0xefbe4786, 0x0fc19dc6, 0x240ca1cc, 0x2de92c6f, 0x4a7484aa, 0x5cb0a9dc, 0x76f988da,
+            0x983e5152, 0xa831c66d, 0xb00327c8, 0xbf597fc7, 0xc6e00bf3, 0xd5a79147, 0x06ca6351, 0x14292967,
+            0x27b70a85, 0x2e1b2138, 0x4d2c6dfc, 0x53380d13, 0x650a7354, 0x766a0abb, 0x81c2c92e, 0x92722c85,
+            0xa2bfe8a1, 0xa81a664b, 0xc24b8b70, 0xc76c51a3, 0xd192e819, 0xd6990624, 0xf40e3585, 0x106aa070,
+            0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
+            0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
+        uint32_t w[64];
+        for (int i = 0; i < 16; ++i)
+            w[i] = (uint32_t)b[4 * i] << 24 | (uint32_t)b[4 * i + 1] << 16 | (uint32_t)b[4 * i + 2] << 8 | b[4 * i + 3];
+        for (int i = 16; i < 64; ++i) {
+            const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
+            const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
+            w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+        }
+        uint32_t a = h_[0], bb = h_[1], c = h_[2], d = h_[3], e = h_[4], f = h_[5], g = h_[6], h = h_[7];
+        for (int i = 0; i < 64; ++i) {
+            const uint32_t t1 = h + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + k[i] + w[i];
+            const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & bb) ^ (a & c) ^ (bb & c));
+            h = g; g = f; f = e; e = d + t1; d = c; c = bb; bb = a; a = t1 + t2;
+        }
+        h_[0] += a; h_[1] += bb; h_[2] += c; h_[3] += d; h_[4] += e; h_[5] += f; h_[6] += g; h_[7] += h;
+    }
+    uint32_t h_[8];
+    uint8_t buf_[64];
+    uint64_t len_;
+};
+}  // namespace details
+
+inline void save_dcsr(const std::string &path, uint64_t nrows, uint64_t ncols, const matrix_dcsr_cpu &m) {
+    const uint64_t nnz = m.cols.size(), nzr = nnz ? m.rows.size() : 0;
+    std::string body("CLBDCSR1");
+    auto put = [&](const void *p, size_t n) { body.append((const char *)p, n); };
+    const uint64_t hdr[4] = {nrows, ncols, nnz, nzr};
+    put(hdr, sizeof(hdr));
+    if (nnz) {
+        put(m.rpt.data(), 8 * (nzr + 1));
+        put(m.rows.data(), 4 * nzr);
+        put(m.cols.data(), 4 * nnz);
+    }
+    uint8_t dg[32];
+    details::Sha256 sh;
+    sh.update((const uint8_t *)body.data(), body.size());
+    sh.digest(dg);
+    std::ofstream f(path, std::ios::binary);
+    f.write(body.data(), (std::streamsize)body.size());
+    f.write((const char *)dg, 32);
+    if (!f) throw Exception(path + ": write failed", CLBOOL_INVALID_VALUE);
+}
+
+inline matrix_dcsr_cpu load_dcsr(const std::string &path, uint64_t &nrows, uint64_t &ncols) {
+    std::ifstream f(path, std::ios::binary);
+    std::string data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    if (data.size() < 8 + 32 + 32 || data.compare(0, 8, "CLBDCSR1") != 0)
+        throw Exception(path + ": not a DCSR file", CLBOOL_INVALID_VALUE);
+    uint8_t dg[32];
+    details::Sha256 sh;
+    sh.update((const uint8_t *)data.data(), data.size() - 32);
+    sh.digest(dg);
+    if (std::memcmp(dg, data.data() + data.size() - 32, 32) != 0)
+        throw Exception(path + ": checksum mismatch", CLBOOL_INVALID_VALUE);
+    uint64_t hdr[4];
+    std::memcpy(hdr, data.data() + 8, sizeof(hdr));
+    nrows = hdr[0];
+    ncols = hdr[1];
+    const uint64_t nnz = hdr[2], nzr = hdr[3];
+    matrix_dcsr_cpu m;
+    if (!nnz) return m;
+    if (data.size() != 40 + 8 * (nzr + 1) + 4 * nzr + 4 * nnz + 32)
+        throw Exception(path + ": truncated", CLBOOL_INVALID_VALUE);
+    const char *p = data.data() + 40;
+    m.rpt.resize(nzr + 1);
+    m.rows.resize(nzr);
+    m.cols.resize(nnz);
+    std::memcpy(m.rpt.data(), p, 8 * (nzr + 1));
+    std::memcpy(m.rows.data(), p + 8 * (nzr + 1), 4 * nzr);
+    std::memcpy(m.cols.data(), p + 8 * (nzr + 1) + 4 * nzr, 4 * nnz);
+    return m;
+}
+}  // namespace io
 
 }  // namespace clbool

@@ -128,3 +128,4 @@ def test_workload_matches_oracle(controls):
     want = O.workload(a, a)
     assert total == int(want.sum())
     assert np.array_equal(buf.to_host(len(a.rows)).astype(np.uint64), want)
+
