@@ -372,6 +372,82 @@ __device__ __forceinline__ void block_bitonic_sort(uint32_t *s, uint32_t M) {
     }
 }
 
+// One bitonic compare-exchange stage (k, j) over a warp's register chunk:
+// lane l holds elements base + l*E + e; partners closer than E are in the
+// same thread, farther ones (up to 32E) in lane l ^ (j / E).
+template <int E>
+__device__ __forceinline__ void warp_stage(uint32_t (&v)[E], uint32_t base, uint32_t k, uint32_t j) {
+    const uint32_t lane = lane_id();
+    if (j >= (uint32_t)E) {
+        const int lx = (int)(j / E);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const uint32_t idx = base + lane * E + e;
+            const uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, v[e], lx);
+            const bool up = (idx & k) == 0, lower = (idx & j) == 0;
+            v[e] = (up == lower) ? min(v[e], o) : max(v[e], o);
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            if ((e & j) == 0) {
+                const int e2 = e | (int)j;
+                const bool up = ((base + lane * E + e) & k) == 0;
+                const uint32_t x = v[e], y = v[e2];
+                if ((x > y) == up) {
+                    v[e] = y;
+                    v[e2] = x;
+                }
+            }
+        }
+    }
+}
+
+// Ascending sort of exactly NT*E keys in shared memory.  Bitonic network with
+// every stage whose partners are less than 32E apart done in registers by
+// the warp owning that 32E-element chunk (shuffles, no barrier); only the
+// farther stages go through shared memory with a block barrier each: for
+// 4096 keys on 512 threads, 10 barrier stages instead of 78.
+template <int NT, int E>
+__device__ __forceinline__ void block_sort_hybrid(uint32_t *s) {
+    constexpr uint32_t M = NT * E, WCH = 32u * E;
+    const uint32_t base = warp_id() * WCH, lane = lane_id();
+    uint32_t v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = s[base + lane * E + e];
+    // every chunk sorted, in the direction its position in the network asks
+#pragma unroll
+    for (uint32_t k = 2; k <= WCH; k <<= 1)
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) warp_stage<E>(v, base, k, j);
+    for (uint32_t k = 2 * WCH; k <= M; k <<= 1) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) s[base + lane * E + e] = v[e];
+        __syncthreads();
+        for (uint32_t j = k >> 1; j >= WCH; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < (M >> 1); t += NT) {
+                const uint32_t lo = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                const uint32_t hi = lo | j;
+                const bool up = (lo & k) == 0;
+                const uint32_t x = s[lo], y = s[hi];
+                if ((x > y) == up) {
+                    s[lo] = y;
+                    s[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = s[base + lane * E + e];
+#pragma unroll
+        for (uint32_t j = WCH >> 1; j > 0; j >>= 1) warp_stage<E>(v, base, k, j);
+    }
+    __syncthreads();  // every thread done reading s before it is overwritten
+#pragma unroll
+    for (int e = 0; e < E; ++e) s[base + lane * E + e] = v[e];
+    __syncthreads();
+}
+
 // Products of A row i, balanced over a whole CTA.  A entries are staged in
 // chunks of ECH: B-row starts and the exclusive prefix of B-row lengths go to
 // shared memory; then every warp takes 32*U consecutive products of the
@@ -525,11 +601,10 @@ __global__ void __launch_bounds__(NT) hash_cta_kernel(BinLists bl, int bin, AVie
         for (int s = 0; s < SPT; ++s)
             if (keys[s] != EMPTY) table[w++] = keys[s];
         __syncthreads();
-        uint32_t M = 1;
-        while (M < nnz) M <<= 1;
-        for (uint32_t s = nnz + threadIdx.x; s < M; s += NT) table[s] = EMPTY;
+        // the compacted keys (nnz <= T/2) padded to T/2 and sorted
+        for (uint32_t s = nnz + threadIdx.x; s < (uint32_t)(T / 2); s += NT) table[s] = EMPTY;
         __syncthreads();
-        block_bitonic_sort<NT>(table, M);
+        block_sort_hybrid<NT, T / 2 / NT>(table);
         uint32_t *dst = o.cols + o.row_off[i];
         for (uint32_t s = threadIdx.x; s < nnz; s += NT) dst[s] = table[s];
         if (o.row_cap && threadIdx.x == 0) o.row_nnz[i] = nnz;

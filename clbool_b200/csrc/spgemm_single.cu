@@ -51,12 +51,10 @@ __global__ void __launch_bounds__(NT) cta_esc_kernel(BinLists bl, int bin, AView
         balanced_products<NT, HASH_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t idx) {
             if (valid && idx < (uint32_t)NP) keys[idx] = c;
         });
-        uint32_t M = 1;
-        while (M < P) M <<= 1;
-        for (uint32_t s = P + threadIdx.x; s < M; s += NT) keys[s] = EMPTY;
+        for (uint32_t s = P + threadIdx.x; s < (uint32_t)NP; s += NT) keys[s] = EMPTY;
         __syncthreads();
-        // sort
-        block_bitonic_sort<NT>(keys, M);
+        // sort (register-resident bitonic stages, few block barriers)
+        block_sort_hybrid<NT, NP / NT>(keys);
         // compress: keep the first of every run (thread-contiguous segments)
         uint32_t v[SPT], flags = 0, mine = 0;
 #pragma unroll
