@@ -1043,7 +1043,9 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 // and flag the row for the exact recomputation.
                 if (!MULTI && o.arena) {
                     if (threadIdx.x == 0) {
-                        const unsigned long long at = atomicAdd(o.arena_cursor, (unsigned long long)ctot);
+                        // reservations keep 16-byte alignment (vector compaction)
+                        const unsigned long long at =
+                            atomicAdd(o.arena_cursor, (unsigned long long)((ctot + 3u) & ~3u));
                         s_spill = at + ctot <= o.arena_cap ? at : ~0ull;
                     }
                     __syncthreads();
@@ -1174,7 +1176,7 @@ __global__ void __launch_bounds__(1024, 1) bitmap_cluster_kernel(BinLists bl, in
             if (rank == 0 && threadIdx.x == 0) {
                 unsigned long long at = ~0ull;
                 if (o.arena) {
-                    at = atomicAdd(o.arena_cursor, (unsigned long long)total);
+                    at = atomicAdd(o.arena_cursor, (unsigned long long)((total + 3u) & ~3ull));
                     if (at + total > o.arena_cap) at = ~0ull;
                 }
 #pragma unroll

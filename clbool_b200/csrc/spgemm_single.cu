@@ -124,8 +124,65 @@ __global__ void fallback_counts_kernel(const uint32_t *__restrict__ ovf, const u
         if (ovf[i]) row_nnz[i] = (uint32_t)(sub_crpt[pos[i] + 1] - sub_crpt[pos[i]]);
 }
 
-// C.cols <- every row from its slot (or from C' for overflowed rows).  One
-// warp per row, 4 independent 32-bit copies per lane in flight.
+// Slot sizes: capacities rounded up to whole 16-byte groups, so every slot
+// (and every spill reservation) starts 16-byte aligned; *sum = sum of the
+// unrounded capacities.
+__global__ void slot_sizes_kernel(const uint32_t *__restrict__ cap, uint64_t n, uint32_t *__restrict__ capp,
+                                  unsigned long long *__restrict__ sum) {
+    unsigned long long mine = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = cap[i];
+        capp[i] = (c + 3u) & ~3u;
+        mine += c;
+    }
+    mine = warp_sum(mine);
+    if (lane_id() == 0 && mine) atomicAdd(sum, mine);
+}
+
+// Copies len words from a 16-byte aligned src to dst (any alignment), one
+// warp: scalar head up to dst's 16-byte boundary, then 16-byte stores whose
+// four words come from two aligned 16-byte loads joined at the head's offset,
+// then a scalar tail.  Reads may run up to 3 words past src[len - 1] (inside
+// the slot padding / the buffers' slack).
+template <int SH>
+__device__ __forceinline__ uint32_t join4(const uint4 &a, const uint4 &b, uint32_t k) {
+    // words SH+k of the 8-word sequence a.x..a.w, b.x..b.w (k = 0..3)
+    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    return w[SH + k];
+}
+
+template <int SH>
+__device__ __forceinline__ void copy_body(const uint4 *__restrict__ s4, uint4 *__restrict__ d4, uint64_t nq) {
+    // d4[q] = words 4q+SH .. 4q+SH+3 of the aligned source
+    const uint32_t lane = lane_id();
+    for (uint64_t q = lane; q < nq; q += 32) {
+        const uint4 a = __ldg(s4 + q);
+        const uint4 b = SH ? __ldg(s4 + q + 1) : a;
+        d4[q] = make_uint4(join4<SH>(a, b, 0), join4<SH>(a, b, 1), join4<SH>(a, b, 2), join4<SH>(a, b, 3));
+    }
+}
+
+__device__ __forceinline__ void warp_copy_aligned_src(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
+                                                      uint64_t len) {
+    const uint32_t lane = lane_id();
+    const uint32_t head = (uint32_t)(((16u - (reinterpret_cast<uintptr_t>(dst) & 15u)) & 15u) >> 2);
+    const uint64_t h = head < len ? head : len;
+    if (lane < h) dst[lane] = src[lane];
+    const uint64_t rest = len - h, nq = rest >> 2;
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst + h);
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(src);  // words from h on are s4 words h, h+1, ...
+    switch (h & 3) {  // warp-uniform
+        case 0: copy_body<0>(s4 + (h >> 2), d4, nq); break;
+        case 1: copy_body<1>(s4, d4, nq); break;
+        case 2: copy_body<2>(s4, d4, nq); break;
+        default: copy_body<3>(s4, d4, nq); break;
+    }
+    for (uint64_t t = h + (nq << 2) + lane; t < len; t += 32) dst[t] = src[t];
+}
+
+// C.cols <- every row from its slot (or the spill arena, both 16-byte
+// aligned: vector copy), or from C' for recomputed rows (scalar copy).  One
+// warp per row.
 __global__ void compact_rows_kernel(const uint32_t *__restrict__ row_nnz, const uint64_t *__restrict__ slot_off,
                                     const uint64_t *__restrict__ off, const uint32_t *__restrict__ pre,
                                     const uint32_t *__restrict__ ovf, const uint32_t *__restrict__ pos,
@@ -137,20 +194,14 @@ __global__ void compact_rows_kernel(const uint32_t *__restrict__ row_nnz, const 
     for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); i < n; i += nw) {
         const uint32_t len = row_nnz[i];
         if (!len) continue;
-        const uint64_t sp = spill ? spill[i] : ~0ull;
-        const uint32_t *src = (ovf && ovf[i]) ? sub_ccols + sub_crpt[pos[i]]
-                                               : (sp != ~0ull ? arena + sp : pre + slot_off[i]);
         uint32_t *dst = ccols + off[i];
-        uint32_t t = lane;
-        for (; t + 96 < len; t += 128) {
-            const uint32_t x0 = __ldg(src + t), x1 = __ldg(src + t + 32), x2 = __ldg(src + t + 64),
-                           x3 = __ldg(src + t + 96);
-            dst[t] = x0;
-            dst[t + 32] = x1;
-            dst[t + 64] = x2;
-            dst[t + 96] = x3;
+        if (ovf && ovf[i]) {
+            const uint32_t *src = sub_ccols + sub_crpt[pos[i]];
+            for (uint32_t t = lane; t < len; t += 32) dst[t] = __ldg(src + t);
+            continue;
         }
-        for (; t < len; t += 32) dst[t] = __ldg(src + t);
+        const uint64_t sp = spill ? spill[i] : ~0ull;
+        warp_copy_aligned_src(sp != ~0ull ? arena + sp : pre + slot_off[i], dst, len);
     }
 }
 
@@ -255,10 +306,18 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     // bins: ESC by products (CTA ESC up to 4096), learned by capacity
     CLB_RETURN_IF(launch_binning(ctl, work, esc ? work : cap, n, B.ncols, info.ptr, list.ptr, flags.ptr, t));
     CLB_RETURN_IF(scan_u32_inplace(ctl, flags.ptr, n, scal.ptr + 0));        // C row positions, nzr
-    CLB_RETURN_IF(scan_u32_to_u64(ctl, cap, slot_off.ptr, n, scal.ptr + 1));  // slots, capacity
-    uint64_t h[2];
+    // slots: capacities rounded up to 16-byte groups (aligned slot starts)
+    Temp<uint32_t> capp;
+    CLB_RETURN_IF(capp.alloc(ctl, n));
+    slot_sizes_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(cap, n, capp.ptr,
+                                                                 (unsigned long long *)(scal.ptr + 7));
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, capp.ptr, slot_off.ptr, n, scal.ptr + 1));  // slot offsets, slots
+    uint64_t h[2], capacity = 0;
     CLB_RETURN_IF(read_scalars(ctl, scal.ptr, h, 2));
-    const uint64_t nzr = h[0], capacity = h[1];
+    CLB_RETURN_IF(read_scalars(ctl, scal.ptr + 7, &capacity, 1));
+    const uint64_t nzr = h[0], slots = h[1];
     uint32_t hinfo[NUM_BINS];  // rows per bin: only bins with rows are launched
     CLB_TRY_CUDA(cudaMemcpyAsync(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost, ctl->stream),
                  CLB_READ_BUFFER_ERROR);
@@ -267,8 +326,8 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
         for (int k = 0; k < NUM_BINS; ++k) st->rows_per_bin[k] = hinfo[k];
         st->capacity = capacity;
     }
-    Temp<uint32_t> pre;
-    CLB_RETURN_IF(pre.alloc(ctl, capacity ? capacity : 1));
+    Temp<uint32_t> pre;  // + 4 words: the vector copy may read up to 3 words past a slot
+    CLB_RETURN_IF(pre.alloc(ctl, slots + 4));
 
     BinLists bl{list.ptr, info.ptr};
     RowOut num{row_nnz.ptr, slot_off.ptr, cap, ovf.ptr, pre.ptr, ctl->d_status};
@@ -281,7 +340,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
         uint64_t acap = capacity / arena_div;
         if (acap < (1ull << 24)) acap = 1ull << 24;
         CLB_RETURN_IF(spill.alloc(ctl, n));
-        CLB_RETURN_IF(arena.alloc(ctl, acap));
+        CLB_RETURN_IF(arena.alloc(ctl, acap + 4));
         CLB_TRY_CUDA(cudaMemsetAsync(spill.ptr, 0xFF, n * 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
         num.spill = spill.ptr;
         num.arena = arena.ptr;
@@ -320,7 +379,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
         CLB_RETURN_IF(sub_off.alloc(ctl, n));
         CLB_TRY_CUDA(cudaMemcpyAsync(opos.ptr, ovf.ptr, n * 4, cudaMemcpyDeviceToDevice, ctl->stream),
                      CLB_COPY_BUFFER_ERROR);
-        CLB_RETURN_IF(scan_u32_inplace(ctl, opos.ptr, n, scal.ptr + 7));
+        CLB_RETURN_IF(scan_u32_inplace(ctl, opos.ptr, n, scal.ptr + 3));
         gather_rows_lengths_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, A.rpt, n, sub_len.ptr);
         ctl->launches += 1;
         CLB_CHECK_LAUNCH();
