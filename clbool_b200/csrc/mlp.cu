@@ -209,14 +209,37 @@ __global__ void adam_kernel(float *__restrict__ params, float *__restrict__ m, f
 //   |B_k| > 0; 0 if none), A.rows[i] / A.nrows, log2(B.nrows * B.ncols / nnz(B));
 // the log2 features are scaled by 1/16.
 constexpr int FT_NT = 256, FT_GROUP = 8;
+constexpr uint32_t FT_LONG = 256;  // rows with more A entries: one CTA each
 
+__device__ __forceinline__ void write_features(float *__restrict__ feat, uint32_t *__restrict__ work, uint64_t row,
+                                               uint64_t len, uint32_t s, uint32_t mx, uint32_t mn, float rowpos,
+                                               float density_term) {
+    if (mn == 0xFFFFFFFFu) mn = 0;
+    float *f = feat + row * F;
+    f[0] = log2f(1.0f + (float)len) * FEAT_SCALE;
+    f[1] = log2f(1.0f + (float)s) * FEAT_SCALE;
+    f[2] = log2f(1.0f + (float)mx) * FEAT_SCALE;
+    f[3] = log2f(1.0f + (float)mn) * FEAT_SCALE;
+    f[4] = rowpos;
+    f[5] = density_term;
+    if (work) work[row] = s;
+}
+
+// A group of 8 lanes per A row; rows over FT_LONG entries are listed for
+// features_long_kernel (hub rows would keep 8 lanes busy long after the rest).
 __global__ void __launch_bounds__(FT_NT) features_kernel(AView a, BRows b, uint64_t a_nrows, float density_term,
-                                                         float *__restrict__ feat, uint32_t *__restrict__ work) {
+                                                         float *__restrict__ feat, uint32_t *__restrict__ work,
+                                                         uint32_t *__restrict__ long_rows,
+                                                         uint32_t *__restrict__ n_long) {
     const uint32_t gl = threadIdx.x & (FT_GROUP - 1);
     const uint32_t gmask = 0xFFu << (lane_id() & 24u);
     for (uint64_t row = ((uint64_t)blockIdx.x * FT_NT + threadIdx.x) / FT_GROUP; row < a.nzr;
          row += (uint64_t)gridDim.x * (FT_NT / FT_GROUP)) {
         const uint64_t ja = a.rpt[row], je = a.rpt[row + 1];
+        if (je - ja > FT_LONG) {  // the whole group takes this branch
+            if (gl == 0) long_rows[atomicAdd(n_long, 1u)] = (uint32_t)row;
+            continue;
+        }
         uint32_t s = 0, mx = 0, mn = 0xFFFFFFFFu;
         for (uint64_t j = ja + gl; j < je; j += FT_GROUP) {
             uint64_t bb;
@@ -231,17 +254,53 @@ __global__ void __launch_bounds__(FT_NT) features_kernel(AView a, BRows b, uint6
             mx = max(mx, __shfl_xor_sync(gmask, mx, d));
             mn = min(mn, __shfl_xor_sync(gmask, mn, d));
         }
-        if (gl == 0) {
-            if (mn == 0xFFFFFFFFu) mn = 0;
-            float *f = feat + row * F;
-            f[0] = log2f(1.0f + (float)(je - ja)) * FEAT_SCALE;
-            f[1] = log2f(1.0f + (float)s) * FEAT_SCALE;
-            f[2] = log2f(1.0f + (float)mx) * FEAT_SCALE;
-            f[3] = log2f(1.0f + (float)mn) * FEAT_SCALE;
-            f[4] = a_nrows ? (float)((double)a.rows[row] / (double)a_nrows) : 0.0f;
-            f[5] = density_term;
-            if (work) work[row] = s;
+        if (gl == 0)
+            write_features(feat, work, row, je - ja, s, mx, mn,
+                           a_nrows ? (float)((double)a.rows[row] / (double)a_nrows) : 0.0f, density_term);
+    }
+}
+
+// The listed long rows, one CTA per row.
+__global__ void __launch_bounds__(FT_NT) features_long_kernel(AView a, BRows b, uint64_t a_nrows, float density_term,
+                                                              const uint32_t *__restrict__ long_rows,
+                                                              const uint32_t *__restrict__ n_long,
+                                                              float *__restrict__ feat, uint32_t *__restrict__ work) {
+    __shared__ uint32_t red[3][FT_NT / 32];
+    const uint32_t n = *n_long;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const uint32_t row = long_rows[i];
+        const uint64_t ja = a.rpt[row], je = a.rpt[row + 1];
+        uint32_t s = 0, mx = 0, mn = 0xFFFFFFFFu;
+#pragma unroll 4
+        for (uint64_t j = ja + threadIdx.x; j < je; j += FT_NT) {
+            uint64_t bb;
+            const uint32_t len = b_row(b, __ldg(a.cols + j), bb);
+            s += len;
+            mx = max(mx, len);
+            if (len) mn = min(mn, len);
         }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            s += __shfl_xor_sync(0xFFFFFFFFu, s, d);
+            mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, d));
+            mn = min(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, d));
+        }
+        if (lane_id() == 0) {
+            red[0][warp_id()] = s;
+            red[1][warp_id()] = mx;
+            red[2][warp_id()] = mn;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < FT_NT / 32; ++w) {
+                s += red[0][w];
+                mx = max(mx, red[1][w]);
+                mn = min(mn, red[2][w]);
+            }
+            write_features(feat, work, row, je - ja, s, mx, mn,
+                           a_nrows ? (float)((double)a.rows[row] / (double)a_nrows) : 0.0f, density_term);
+        }
+        __syncthreads();
     }
 }
 
@@ -287,10 +346,17 @@ uint64_t splitmix(uint64_t &s) {
 
 int features_launch(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                     float *feat, uint32_t *work) {
+    Temp<uint32_t> long_rows, n_long;
+    CLB_RETURN_IF(n_long.alloc(ctl, 1));
+    CLB_RETURN_IF(long_rows.alloc(ctl, A.nzr ? A.nzr : 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(n_long.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
     ProfScope ps(ctl, "features");
-    features_kernel<<<grid_for(ctl, A.nzr * FT_GROUP), FT_NT, 0, ctl->stream>>>(a, b, A.nrows, density_term(B), feat,
-                                                                              work);
-    ctl->launches += 1;
+    const float dt = density_term(B);
+    features_kernel<<<grid_for(ctl, A.nzr * FT_GROUP), FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, feat, work,
+                                                                              long_rows.ptr, n_long.ptr);
+    features_long_kernel<<<ctl->sm_count * 4, FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, long_rows.ptr, n_long.ptr,
+                                                                       feat, work);
+    ctl->launches += 2;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
 }

@@ -21,10 +21,16 @@ namespace clb {
 namespace {
 
 constexpr int WL_NT = 256;
-constexpr int WL_GROUP = 8;  // lanes per A row in the workload kernel
+constexpr int WL_GROUP = 8;        // lanes per A row in the workload kernel
+constexpr uint32_t WL_LONG = 256;  // rows with more A entries: one CTA each
 
+// Products of every A row: a group of 8 lanes per row; rows over WL_LONG
+// entries are listed for workload_long_kernel (R-MAT hub rows hold tens of
+// thousands of entries, which 8 lanes would walk long after the rest).
 __global__ void __launch_bounds__(WL_NT) workload_kernel(AView a, BRows b, uint32_t *__restrict__ work,
-                                                         unsigned long long *__restrict__ total) {
+                                                         unsigned long long *__restrict__ total,
+                                                         uint32_t *__restrict__ long_rows,
+                                                         uint32_t *__restrict__ n_long) {
     __shared__ unsigned long long ptot;
     if (threadIdx.x == 0) ptot = 0;
     __syncthreads();
@@ -34,6 +40,10 @@ __global__ void __launch_bounds__(WL_NT) workload_kernel(AView a, BRows b, uint3
     for (uint64_t row = ((uint64_t)blockIdx.x * WL_NT + threadIdx.x) / WL_GROUP; row < a.nzr;
          row += (uint64_t)gridDim.x * (WL_NT / WL_GROUP)) {
         const uint64_t ja = a.rpt[row], je = a.rpt[row + 1];
+        if (je - ja > WL_LONG) {  // the whole group takes this branch
+            if (gl == 0) long_rows[atomicAdd(n_long, 1u)] = (uint32_t)row;
+            continue;
+        }
         uint32_t s = 0;
         for (uint64_t j = ja + gl; j < je; j += WL_GROUP) {
             uint64_t bb;
@@ -51,13 +61,44 @@ __global__ void __launch_bounds__(WL_NT) workload_kernel(AView a, BRows b, uint3
     if (threadIdx.x == 0 && ptot) atomicAdd(total, ptot);
 }
 
+// The listed long rows, one CTA per row.
+__global__ void __launch_bounds__(WL_NT) workload_long_kernel(AView a, BRows b, const uint32_t *__restrict__ long_rows,
+                                                              const uint32_t *__restrict__ n_long,
+                                                              uint32_t *__restrict__ work,
+                                                              unsigned long long *__restrict__ total) {
+    __shared__ uint32_t scratch[33];
+    const uint32_t n = *n_long;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const uint32_t row = long_rows[i];
+        const uint64_t ja = a.rpt[row], je = a.rpt[row + 1];
+        uint32_t s = 0;
+#pragma unroll 4
+        for (uint64_t j = ja + threadIdx.x; j < je; j += WL_NT) {
+            uint64_t bb;
+            s += b_row(b, __ldg(a.cols + j), bb);
+        }
+        s = block_sum<uint32_t, WL_NT>(s, scratch);
+        if (threadIdx.x == 0) {
+            work[row] = s;
+            atomicAdd(total, (unsigned long long)s);
+        }
+    }
+}
+
 }  // namespace
 
 int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t *work, uint64_t *d_total) {
+    Temp<uint32_t> long_rows, n_long;
+    CLB_RETURN_IF(n_long.alloc(ctl, 1));
+    CLB_RETURN_IF(long_rows.alloc(ctl, a.nzr ? a.nzr : 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(n_long.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
     unsigned grid = persistent_grid(ctl, 8, ceil_div_u(a.nzr, WL_NT / WL_GROUP));
     ProfScope ps(ctl, "workload");
-    workload_kernel<<<grid, WL_NT, 0, ctl->stream>>>(a, b, work, (unsigned long long *)d_total);
-    ctl->launches += 1;
+    workload_kernel<<<grid, WL_NT, 0, ctl->stream>>>(a, b, work, (unsigned long long *)d_total, long_rows.ptr,
+                                                     n_long.ptr);
+    workload_long_kernel<<<ctl->sm_count * 4, WL_NT, 0, ctl->stream>>>(a, b, long_rows.ptr, n_long.ptr, work,
+                                                                       (unsigned long long *)d_total);
+    ctl->launches += 2;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
 }

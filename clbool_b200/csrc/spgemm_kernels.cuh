@@ -945,7 +945,10 @@ __device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t n
                 }
             }
             __syncwarp();
-            for (uint32_t t = lane; t < m; t += 32) out[pos + w0 + t] = stage[t];
+            uint32_t *const o2 = out + pos + w0 + lane;
+#pragma unroll
+            for (uint32_t u = 0; u < BMP_STAGE / 32; ++u)
+                if (lane + 32 * u < m) o2[32 * u] = stage[lane + 32 * u];
             __syncwarp();
         }
         if (pc) bm4[q4] = make_uint4(0, 0, 0, 0);
