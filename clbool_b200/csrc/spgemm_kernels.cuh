@@ -619,6 +619,7 @@ constexpr int BMP_U = 8;                      // B-column loads in flight per la
 constexpr uint32_t BMP_STEP_WORDS = 128;      // emission step: 4 words per lane
 constexpr uint32_t BMP_MAX_STEPS = BMP_MAX_WORDS / BMP_STEP_WORDS;
 constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (columns)
+constexpr uint32_t BMP_FEW = 16;  // steps with at most this many outputs skip the balanced windows
 constexpr uint32_t BMP_SHORT = 64;            // products per A entry below which a row uses the per-product mapping
 
 // Words of the bitmap for `ncols` columns: a multiple of the emission step,
@@ -894,8 +895,10 @@ __device__ __forceinline__ uint32_t bitmap_list_steps(const uint4 *bm4, uint32_t
 // outputs are split evenly over the lanes, each lane finds the word and bit
 // of its first output (shuffle search over the scan, then nth_set_bit) and
 // walks the bitmap from there into the warp's staging buffer, which the warp
-// copies out with coalesced stores.  Cost follows the non-empty steps and the
-// output, not the bitmap width.  The caller synchronises the block after.
+// copies out with coalesced stores.  A step with at most BMP_FEW outputs
+// skips the windows: each lane writes its own bits at its scan offset.  Cost
+// follows the non-empty steps and the output, not the bitmap width.  The
+// caller synchronises the block after.
 __device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t nlist, const uint32_t *s_list,
                                             const uint32_t *s_soff, uint32_t *s_next, uint32_t *stage, uint32_t *out,
                                             uint32_t colbase) {
@@ -912,6 +915,23 @@ __device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t n
         const uint4 x = bm4[q4];
         const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
         const uint32_t inc = warp_inclusive_scan(pc);
+        if (T <= BMP_FEW) {
+            // few outputs (a quarter of the steps of R-MAT rows hold <= 8):
+            // every lane writes its own bits in place, no search, no staging
+            uint32_t *o = out + pos + inc - pc;
+            const uint32_t wb = colbase + q4 * 128u;
+            uint32_t cur = x.x, j = 0;
+            for (uint32_t t = 0; t < pc; ++t) {
+                while (!cur) {
+                    ++j;
+                    cur = j == 1 ? x.y : (j == 2 ? x.z : x.w);
+                }
+                o[t] = wb + j * 32u + (uint32_t)(__ffs(cur) - 1);
+                cur &= cur - 1;
+            }
+            if (pc) bm4[q4] = make_uint4(0, 0, 0, 0);
+            continue;
+        }
         for (uint32_t w0 = 0; w0 < T; w0 += BMP_STAGE) {
             const uint32_t m = min(BMP_STAGE, T - w0);
             const uint32_t per = (m + 31) >> 5;  // outputs per lane
