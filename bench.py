@@ -604,6 +604,21 @@ def run_small(args) -> dict:
         if name != "coo_add":
             out[name]["products_per_s"] = products / (ms / 1e3)
     out["autotuned"]["tuning"] = best.as_dict()
+    # the host-sync-free form recorded once into a CUDA graph and replayed
+    from clbool_b200 import batched
+    cap = batched.CapturedBatch(ctl, [(A, B)], tune=best)
+    graph = batched.Graph(ctl, cap.enqueue)
+    for _ in range(max(3, args.warmup)):
+        graph.launch()
+    got = cap.result()[0]
+    want = cb.matrix_dcsr_from_gpu(ctl, cb.dcsr.matrix_multiplication_hash(ctl, None, A, B))
+    exact = bool(np.array_equal(got[0], want.rpt) and np.array_equal(got[1], want.rows)
+                 and np.array_equal(got[2], want.cols))
+    ms = _event_ms(stream, graph.launch, max(20, args.steps))
+    out["graph_replay"] = {"us": ms * 1e3, "products_per_s": products / (ms / 1e3), "bit_exact_vs_two_pass": exact}
+    ms = _event_ms(stream, cap.enqueue, max(20, args.steps))
+    out["capture_form_direct"] = {"us": ms * 1e3, "products_per_s": products / (ms / 1e3)}
+    graph.close()
     return {"metric": METRIC, "workload": "poisson4096", "unit": UNIT, "n_gpus": 1, "data": "synthetic",
             "config": {"workload": "poisson4096_AxB", "n": n, "lambda": 8, "products": int(products),
                        "nnz_A": int(ra.size), "nnz_B": int(rb.size)}, "calls": out}

@@ -125,6 +125,14 @@ _SIGS = {
                                           P(clb_spgemm_tuning), P(clb_spgemm_stats)]),
     "clb_spgemm_autotune": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_tuning),
                                       P(clb_spgemm_tuning), P(C.c_double), C.c_uint32, P(C.c_uint32)]),
+    # host-sync-free batched product and CUDA graphs
+    "clb_spgemm_batched_plan": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(C.c_uint64), P(C.c_uint64)]),
+    "clb_dcsr_spgemm_batched_capture": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_tuning),
+                                                  C.c_uint64, vp, vp, vp, C.c_uint64, vp, vp]),
+    "clb_graph_begin": (C.c_int, [vp]),
+    "clb_graph_end": (C.c_int, [vp, P(vp)]),
+    "clb_graph_launch": (C.c_int, [vp, vp]),
+    "clb_graph_destroy": (C.c_int, [vp]),
 }
 
 def _load():

@@ -5,13 +5,21 @@ a list of independent pairs in one pass: the library stacks the pairs
 block-diagonally, runs one set of accumulator launches over all of them, and
 splits the product per pair.  ``autotune`` times the accumulator tunings on a
 batch and returns the fastest; every tuning gives the same C.
+
+``CapturedBatch`` is the same product with caller-sized buffers and no read
+back to the host, so it can be recorded once into a CUDA graph (``Graph``) and
+replayed while the pairs' device arrays keep their sizes and change their
+contents -- the repeated small products of a fixpoint, say, without the
+per-call host round trips.
 """
 from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
+
 from ._capi import clb_dcsr, clb_spgemm_stats, clb_spgemm_tuning, lib
-from .core import ClBoolException, Controls, check, matrix_dcsr
+from .core import ClBoolException, Controls, DeviceBuffer, check, matrix_dcsr
 
 
 def tuning(form: str | int = "two_pass", warp_max: int = 0, bitmap_min: int = 0, bitmap_threads: int = 0,
@@ -84,3 +92,94 @@ def autotune(controls: Controls, pairs, max_tried: int = 64):
     check(lib.clb_spgemm_autotune(controls.handle, n, A, B, C.byref(best), tried, ms, max_tried, C.byref(nt)),
           "autotune")
     return best, [(tried[k].as_dict(), ms[k]) for k in range(min(nt.value, max_tried))]
+
+
+class Graph:
+    """A CUDA graph recorded from the controls' stream (clb_graph_begin / end)."""
+
+    def __init__(self, controls: Controls, fn):
+        self.controls = controls
+        self.handle = None
+        check(lib.clb_graph_begin(controls.handle), "graph_begin")
+        try:
+            fn()
+        finally:
+            h = C.c_void_p()
+            rc = lib.clb_graph_end(controls.handle, C.byref(h))
+        check(rc, "graph_end")
+        self.handle = h
+
+    def launch(self) -> None:
+        """Replays the graph on the controls' stream (no synchronisation)."""
+        check(lib.clb_graph_launch(self.controls.handle, self.handle), "graph_launch")
+
+    def close(self) -> None:
+        if self.handle:
+            lib.clb_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batched_plan(controls: Controls, pairs):
+    """(rows_need, slots_need) of CapturedBatch for the pairs' current contents."""
+    n, A, B, _keep = _arrays(list(pairs))
+    rows, slots = C.c_uint64(), C.c_uint64()
+    check(lib.clb_spgemm_batched_plan(controls.handle, n, A, B, C.byref(rows), C.byref(slots)), "batched_plan")
+    return int(rows.value), int(slots.value)
+
+
+class CapturedBatch:
+    """C_k = A_k * B_k for fixed pairs, into buffers sized once: ``enqueue()``
+    issues the product without any host read (so it may run inside
+    ``Graph(controls, batch.enqueue)``); ``result()`` synchronises and returns
+    the per-pair host arrays, raising when a capacity was too small."""
+
+    FLAG_NAMES = {1: "slot capacity", 2: "column capacity", 4: "device check"}
+
+    def __init__(self, controls: Controls, pairs, slot_capacity: int | None = None,
+                 cols_capacity: int | None = None, tune: clb_spgemm_tuning | None = None):
+        self.controls = controls
+        self.pairs = list(pairs)
+        self.count, self._A, self._B, _ = _arrays(self.pairs)
+        if self.count == 0:
+            raise ClBoolException(12, "CapturedBatch needs at least one pair")
+        rows, slots = batched_plan(controls, self.pairs)
+        self.slot_capacity = int(slots if slot_capacity is None else slot_capacity)
+        self.cols_capacity = int(slots if cols_capacity is None else cols_capacity)
+        self.rows_capacity = rows
+        self.tune = tune
+        self.rpt = DeviceBuffer.empty(controls, rows + 1, np.uint64)
+        self.rows = DeviceBuffer.empty(controls, max(rows, 1), np.uint32)
+        self.cols = DeviceBuffer.empty(controls, max(self.cols_capacity, 1), np.uint32)
+        self.res = DeviceBuffer.empty(controls, 2 + 2 * (self.count + 1), np.uint64)
+        self.flags = DeviceBuffer.empty(controls, 1, np.uint32)
+
+    def enqueue(self) -> None:
+        check(lib.clb_dcsr_spgemm_batched_capture(
+            self.controls.handle, self.count, self._A, self._B, C.byref(self.tune) if self.tune else None,
+            self.slot_capacity, C.c_void_p(self.rpt.ptr), C.c_void_p(self.rows.ptr), C.c_void_p(self.cols.ptr),
+            self.cols_capacity, C.c_void_p(self.res.ptr), C.c_void_p(self.flags.ptr)), "batched_capture")
+
+    def result(self):
+        """[(rpt u64, rows u32, cols u32) per pair] on the host."""
+        self.controls.sync()
+        flags = int(self.flags.to_host(1)[0])
+        if flags:
+            what = ", ".join(v for k, v in self.FLAG_NAMES.items() if flags & k)
+            raise ClBoolException(5, f"captured batch incomplete ({what} exceeded or failed)")
+        r = self.res.to_host()
+        nzr, nnz, k = int(r[0]), int(r[1]), self.count
+        rpt = self.rpt.to_host(nzr + 1).astype(np.uint64)
+        rows = self.rows.to_host(nzr) if nzr else np.zeros(0, np.uint32)
+        cols = self.cols.to_host(nnz) if nnz else np.zeros(0, np.uint32)
+        out = []
+        for i in range(k):
+            r0, r1 = int(r[2 + i]), int(r[3 + i])
+            j0, j1 = int(r[3 + k + i]), int(r[4 + k + i])
+            out.append((rpt[r0:r1 + 1] - np.uint64(j0), rows[r0:r1], cols[j0:j1]))
+        return out

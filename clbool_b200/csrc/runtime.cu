@@ -255,6 +255,42 @@ int clb_controls_sync(clb_controls *ctl) {
     return CLB_SUCCESS;
 }
 
+int clb_graph_begin(clb_controls *ctl) {
+    if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaStreamBeginCapture(ctl->stream, cudaStreamCaptureModeThreadLocal), CLB_RUN_KERNEL_FAILURE);
+    return CLB_SUCCESS;
+}
+
+int clb_graph_end(clb_controls *ctl, void **graph) {
+    if (!ctl || !graph) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    *graph = nullptr;
+    cudaGraph_t gr = nullptr;
+    CLB_TRY_CUDA(cudaStreamEndCapture(ctl->stream, &gr), CLB_RUN_KERNEL_FAILURE);
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CLB_RUN_KERNEL_FAILURE, std::string("graph instantiation: ") + cudaGetErrorString(e));
+    }
+    *graph = ex;
+    return CLB_SUCCESS;
+}
+
+int clb_graph_launch(clb_controls *ctl, void *graph) {
+    if (!ctl || !graph) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(graph), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    return CLB_SUCCESS;
+}
+
+int clb_graph_destroy(void *graph) {
+    if (graph) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph));
+    return CLB_SUCCESS;
+}
+
 int clb_profile_enable(clb_controls *ctl, int on) {
     if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
     DeviceGuard g(ctl);

@@ -32,6 +32,20 @@ int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AVie
 int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                        const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
                        clb_spgemm_stats *st, uint64_t arena_div, const Tuning &t = Tuning());
+// Flags of the host-sync-free form (bits of its device flag word).
+constexpr uint32_t CAPTURE_SLOTS_FULL = 1u;    // slot capacity too small: rows left empty
+constexpr uint32_t CAPTURE_COLS_FULL = 2u;     // column capacity too small: rows not written
+constexpr uint32_t CAPTURE_DEVICE_CHECK = 4u;  // an accumulator's device check failed
+// The ESC single pass with every size from the caller and no host read:
+// slots (slot_capacity entries) and the stream-ordered temporaries are
+// allocated on ctl's stream, C goes to the caller's arrays (rpt: A.nzr + 1,
+// rows: A.nzr, cols: cols_capacity), d_result[0..1] = nzr, nnz and
+// d_result[2..] = per-pair row and column bounds (first[k] = first stacked
+// row of pair k, row_base[k] = its row-id offset, both on the device).
+int spgemm_esc_capture(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const Tuning &t,
+                       uint64_t slot_capacity, const uint64_t *first, const uint32_t *row_base, uint32_t count,
+                       uint64_t *c_rpt, uint32_t *c_rows, uint32_t *c_cols, uint64_t cols_capacity,
+                       uint64_t *d_result, uint32_t *d_flags);
 // cap[i] = min(work[i], ncols): the exact upper bound of a row's count.
 int launch_upper_bound_caps(clb_controls *ctl, const uint32_t *work, uint64_t n, uint64_t ncols, uint32_t *cap);
 // Public tuning struct -> internal tuning (zero fields: defaults), and its check.

@@ -138,6 +138,70 @@ int spgemm_tuned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, uint32
     return rc;
 }
 
+// Pair descriptors reach the device as kernel parameters (by value), so no
+// host memory is read when the launch is replayed from a CUDA graph.
+constexpr uint32_t DESC_CHUNK = 24;
+struct DescChunk {
+    PairDesc a[DESC_CHUNK], b[DESC_CHUNK];
+};
+
+__global__ void store_descs_kernel(DescChunk c, uint32_t k0, uint32_t n, PairDesc *__restrict__ da,
+                                   PairDesc *__restrict__ db, uint64_t *__restrict__ first,
+                                   uint32_t *__restrict__ row_base) {
+    const uint32_t j = threadIdx.x;
+    if (j < n) {
+        da[k0 + j] = c.a[j];
+        db[k0 + j] = c.b[j];
+        first[k0 + j] = c.a[j].nzr_off;
+        row_base[k0 + j] = c.a[j].row_add;
+    }
+}
+
+// *need += sum over rows of round4(min(work, ncols)): the slots of the
+// host-sync-free form (16-byte aligned upper-bound slots).
+__global__ void slot_need_kernel(const uint32_t *__restrict__ work, uint64_t n, uint64_t ncols,
+                                 unsigned long long *__restrict__ need) {
+    unsigned long long mine = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = min((uint64_t)work[i], ncols);
+        mine += (c + 3) & ~3ull;
+    }
+    mine = warp_sum(mine);
+    if (lane_id() == 0 && mine) atomicAdd(need, mine);
+}
+
+// Host-side checks and stacking offsets shared by the batched entry points.
+int pair_descs(uint32_t count, const clb_dcsr *a, const clb_dcsr *b, std::vector<PairDesc> &da,
+               std::vector<PairDesc> &db, uint64_t &arows, uint64_t &brows, uint64_t &anzr, uint64_t &annz,
+               uint64_t &bnzr, uint64_t &bnnz, uint64_t &bcols, uint64_t &amax, uint64_t &bmax) {
+    da.resize(count);
+    db.resize(count);
+    arows = brows = anzr = annz = bnzr = bnnz = bcols = amax = bmax = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const int rc = validate_spgemm(a[k], b[k]);
+        if (rc != CLB_SUCCESS) return fail(rc, "pair " + std::to_string(k) + ": " + clb_last_error());
+        const bool live = a[k].nnz && b[k].nnz;
+        da[k] = PairDesc{a[k].rpt, a[k].rows, a[k].cols, live ? a[k].nzr : 0, live ? a[k].nnz : 0, anzr, annz,
+                         (uint32_t)arows, (uint32_t)brows, (uint32_t)b[k].ncols};
+        db[k] = PairDesc{b[k].rpt, b[k].rows, b[k].cols, live ? b[k].nzr : 0, live ? b[k].nnz : 0, bnzr, bnnz,
+                         (uint32_t)brows, 0u, (uint32_t)b[k].ncols};
+        if (live) {
+            anzr += a[k].nzr;
+            annz += a[k].nnz;
+            bnzr += b[k].nzr;
+            bnnz += b[k].nnz;
+            amax = std::max(amax, std::max(a[k].nnz, a[k].nzr + 1));
+            bmax = std::max(bmax, std::max(b[k].nnz, b[k].nzr + 1));
+        }
+        arows += a[k].nrows;
+        brows += b[k].nrows;
+        bcols = std::max(bcols, b[k].ncols);
+        if (arows > 0xFFFFFFFFull || brows > 0xFFFFFFFFull)
+            return fail(CLB_NOT_SUPPORTED, "the stacked batch exceeds 2^32 - 1 rows");
+    }
+    return CLB_SUCCESS;
+}
+
 }  // namespace
 
 Tuning to_tuning(const clb_spgemm_tuning *t) {
@@ -343,6 +407,101 @@ int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a
     st.kernel_launches = inner_launches + 4;
     if (stats) *stats = st;
     return CLB_SUCCESS;
+}
+
+int clb_spgemm_batched_plan(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                            uint64_t *rows_need, uint64_t *slots_need) {
+    if (!ctl || (count && (!a || !b)) || !rows_need || !slots_need) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    if (count > 65535) return fail(CLB_NOT_SUPPORTED, "at most 65535 pairs per batch");
+    std::vector<PairDesc> da, db;
+    uint64_t arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax;
+    CLB_RETURN_IF(pair_descs(count, a, b, da, db, arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax));
+    *rows_need = anzr;
+    *slots_need = 0;
+    if (annz == 0) return CLB_SUCCESS;
+    DeviceGuard g(ctl);
+    Temp<uint64_t> need;
+    CLB_RETURN_IF(need.alloc(ctl, 2));
+    CLB_TRY_CUDA(cudaMemsetAsync(need.ptr, 0, 16, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    for (uint32_t k = 0; k < count; ++k) {
+        if (!da[k].nnz) continue;
+        const AView av{a[k].rpt, a[k].rows, a[k].cols, a[k].nzr};
+        BRows bv;
+        Temp<uint64_t> dense;
+        Temp<uint32_t> work;
+        CLB_RETURN_IF(prepare_b(ctl, b[k], dense, bv));
+        CLB_RETURN_IF(work.alloc(ctl, a[k].nzr));
+        CLB_RETURN_IF(launch_workload(ctl, av, bv, work.ptr, need.ptr + 1));
+        slot_need_kernel<<<std::max<unsigned>(1, std::min<uint64_t>((a[k].nzr + 255) / 256, ctl->sm_count * 8)), 256,
+                           0, ctl->stream>>>(work.ptr, a[k].nzr, b[k].ncols, (unsigned long long *)need.ptr);
+        CLB_CHECK_LAUNCH();
+    }
+    CLB_RETURN_IF(read_scalars(ctl, need.ptr, slots_need, 1));
+    return CLB_SUCCESS;
+}
+
+int clb_dcsr_spgemm_batched_capture(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                                    const clb_spgemm_tuning *tuning, uint64_t slot_capacity, uint64_t *c_rpt,
+                                    uint32_t *c_rows, uint32_t *c_cols, uint64_t cols_capacity, uint64_t *result,
+                                    uint32_t *flags) {
+    if (!ctl || (count && (!a || !b)) || !result || !flags) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    if (count == 0) return fail(CLB_INVALID_ARGUMENT, "empty batch");
+    if (count > 65535) return fail(CLB_NOT_SUPPORTED, "at most 65535 pairs per batch");
+    CLB_RETURN_IF(check_tuning(tuning));
+    std::vector<PairDesc> da, db;
+    uint64_t arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax;
+    CLB_RETURN_IF(pair_descs(count, a, b, da, db, arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax));
+    if (!c_rpt || (anzr && !c_rows) || (cols_capacity && !c_cols))
+        return fail(CLB_INVALID_ARGUMENT, "NULL output array");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaMemsetAsync(flags, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(result, 0, (2 + 2 * ((uint64_t)count + 1)) * 8, ctl->stream),
+                 CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(c_rpt, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    if (annz == 0) return CLB_SUCCESS;
+    CLB_RETURN_IF(clear_status(ctl));
+    ctl->launches = 0;
+    Tuning t = to_tuning(tuning);
+    Temp<PairDesc> dda, ddb;
+    Temp<uint64_t> first, arpt, brpt;
+    Temp<uint32_t> rbase, arws, acls, brws, bcls, rnc;
+    CLB_RETURN_IF(dda.alloc(ctl, count));
+    CLB_RETURN_IF(ddb.alloc(ctl, count));
+    CLB_RETURN_IF(first.alloc(ctl, count));
+    CLB_RETURN_IF(rbase.alloc(ctl, count));
+    CLB_RETURN_IF(arpt.alloc(ctl, anzr + 1));
+    CLB_RETURN_IF(arws.alloc(ctl, anzr));
+    CLB_RETURN_IF(rnc.alloc(ctl, anzr));
+    CLB_RETURN_IF(acls.alloc(ctl, annz));
+    CLB_RETURN_IF(brpt.alloc(ctl, bnzr + 1));
+    CLB_RETURN_IF(brws.alloc(ctl, bnzr));
+    CLB_RETURN_IF(bcls.alloc(ctl, bnnz));
+    for (uint32_t k0 = 0; k0 < count; k0 += DESC_CHUNK) {
+        DescChunk ch{};
+        const uint32_t nk = std::min<uint32_t>(DESC_CHUNK, count - k0);
+        for (uint32_t j = 0; j < nk; ++j) {
+            ch.a[j] = da[k0 + j];
+            ch.b[j] = db[k0 + j];
+        }
+        store_descs_kernel<<<1, DESC_CHUNK, 0, ctl->stream>>>(ch, k0, nk, dda.ptr, ddb.ptr, first.ptr, rbase.ptr);
+        ctl->launches += 1;
+    }
+    CLB_CHECK_LAUNCH();
+    {
+        ProfScope ps(ctl, "batch_stack");
+        stack_kernel<<<dim3(stack_grid_x(ctl, amax, count), count), CAT_NT, 0, ctl->stream>>>(
+            dda.ptr, arpt.ptr, arws.ptr, acls.ptr, rnc.ptr, anzr, annz);
+        stack_kernel<<<dim3(stack_grid_x(ctl, bmax, count), count), CAT_NT, 0, ctl->stream>>>(
+            ddb.ptr, brpt.ptr, brws.ptr, bcls.ptr, nullptr, bnzr, bnnz);
+        ctl->launches += 2;
+        CLB_CHECK_LAUNCH();
+    }
+    const clb_dcsr As{arows, brows, annz, anzr, arpt.ptr, arws.ptr, acls.ptr};
+    const clb_dcsr Bs{brows, bcols, bnnz, bnzr, brpt.ptr, brws.ptr, bcls.ptr};
+    CLB_RETURN_IF(validate_spgemm(As, Bs));
+    t.row_ncols = rnc.ptr;
+    return spgemm_esc_capture(ctl, As, Bs, t, slot_capacity, first.ptr, rbase.ptr, count, c_rpt, c_rows, c_cols,
+                              cols_capacity, result, flags);
 }
 
 int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,

@@ -452,6 +452,175 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     return CLB_SUCCESS;
 }
 
+namespace {
+
+// cap[i] = min(work[i], columns of row i's product) (row_ncols: per stacked
+// row, from its pair; null = ncols).
+__global__ void upper_bound_cap_rows_kernel(const uint32_t *__restrict__ work, uint64_t n, uint64_t ncols,
+                                            const uint32_t *__restrict__ row_ncols, uint32_t *__restrict__ cap) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = row_ncols ? (uint64_t)row_ncols[i] : ncols;
+        cap[i] = (uint32_t)min((uint64_t)work[i], c);
+    }
+}
+
+// Rows whose slot would end past the caller's slot capacity get capacity 0:
+// every accumulator then flags them as overflowed instead of writing.
+__global__ void fit_slots_kernel(const uint64_t *__restrict__ slot_off, const uint32_t *__restrict__ capp, uint64_t n,
+                                 uint64_t limit, uint32_t *__restrict__ cap, uint32_t *__restrict__ flags) {
+    bool cut = false;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (slot_off[i] + capp[i] > limit) {
+            cap[i] = 0;
+            cut = true;
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, cut) && lane_id() == 0) atomicOr(flags, CAPTURE_SLOTS_FULL);
+}
+
+// Overflowed rows (only rows cut by fit_slots_kernel can overflow upper-bound
+// slots) keep no columns.
+__global__ void drop_overflow_kernel(const uint32_t *__restrict__ ovf, uint64_t n, uint32_t *__restrict__ row_nnz,
+                                     uint32_t *__restrict__ flags) {
+    bool any = false;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (ovf[i]) {
+            row_nnz[i] = 0;
+            any = true;
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, any) && lane_id() == 0) atomicOr(flags, CAPTURE_SLOTS_FULL);
+}
+
+// C.rpt / C.rows with sizes read on the device (nzr = *d_nzr, nnz = *d_nnz):
+// row ids are made local to their pair (first[k] = first stacked row of
+// pair k, row_base[k] = its row-id offset; count pairs).
+__global__ void assemble_capture_kernel(const uint32_t *__restrict__ work, const uint32_t *__restrict__ pos,
+                                        const uint64_t *__restrict__ off, const uint32_t *__restrict__ a_rows,
+                                        uint64_t n, const uint64_t *__restrict__ first,
+                                        const uint32_t *__restrict__ row_base, uint32_t count,
+                                        const uint64_t *__restrict__ d_nzr, const uint64_t *__restrict__ d_nnz,
+                                        uint64_t *__restrict__ c_rpt, uint32_t *__restrict__ c_rows) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (work[i] > 0) {
+            uint32_t lo = 0, hi = count;  // last k with first[k] <= i
+            while (hi - lo > 1) {
+                const uint32_t m = (lo + hi) / 2;
+                if (first[m] <= i) lo = m; else hi = m;
+            }
+            const uint32_t p = pos[i];
+            c_rpt[p] = off[i];
+            c_rows[p] = a_rows[i] - row_base[lo];
+        }
+        if (i == 0) c_rpt[*d_nzr] = *d_nnz;
+    }
+}
+
+// Per-pair bounds: out[k] = first C row of pair k, out[count + 1 + k] = its
+// first column position (k = count: the totals).
+__global__ void capture_bounds_kernel(const uint32_t *__restrict__ pos, const uint64_t *__restrict__ off, uint64_t n,
+                                      const uint64_t *__restrict__ first, uint32_t count,
+                                      const uint64_t *__restrict__ d_nzr, const uint64_t *__restrict__ d_nnz,
+                                      uint64_t *__restrict__ out) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= count; k += gridDim.x * blockDim.x) {
+        const uint64_t f = k < count ? first[k] : n;
+        out[k] = f < n ? (uint64_t)pos[f] : *d_nzr;
+        out[count + 1 + k] = f < n ? off[f] : *d_nnz;
+    }
+}
+
+// Compaction into the caller's column buffer; rows past its capacity are
+// not written and flag the call.
+__global__ void compact_capture_kernel(const uint32_t *__restrict__ row_nnz, const uint64_t *__restrict__ slot_off,
+                                       const uint64_t *__restrict__ off, const uint32_t *__restrict__ pre, uint64_t n,
+                                       uint64_t cols_cap, uint32_t *__restrict__ ccols, uint32_t *__restrict__ flags) {
+    const uint32_t lane = lane_id();
+    const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); i < n; i += nw) {
+        const uint32_t len = row_nnz[i];
+        if (!len) continue;
+        if (off[i] + len > cols_cap) {
+            if (lane == 0) atomicOr(flags, CAPTURE_COLS_FULL);
+            continue;
+        }
+        warp_copy_aligned_src(pre + slot_off[i], ccols + off[i], len);
+    }
+}
+
+// Device check failures of the accumulators (the controls' status word).
+__global__ void capture_status_kernel(const uint32_t *__restrict__ status, uint32_t *__restrict__ flags) {
+    if (threadIdx.x == 0 && *status) atomicOr(flags, CAPTURE_DEVICE_CHECK);
+}
+
+}  // namespace
+
+int spgemm_esc_capture(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const Tuning &t,
+                       uint64_t slot_capacity, const uint64_t *first, const uint32_t *row_base, uint32_t count,
+                       uint64_t *c_rpt, uint32_t *c_rows, uint32_t *c_cols, uint64_t cols_capacity,
+                       uint64_t *d_result, uint32_t *d_flags) {
+    const uint64_t n = A.nzr;
+    const AView a{A.rpt, A.rows, A.cols, A.nzr};
+    BRows b;
+    Temp<uint64_t> dense;
+    CLB_RETURN_IF(prepare_b(ctl, B, dense, b));
+    Temp<uint32_t> work, cap, capp, list, info, flags, row_nnz, ovf, pre;
+    Temp<uint64_t> slot_off, off, scal;
+    CLB_RETURN_IF(work.alloc(ctl, n));
+    CLB_RETURN_IF(cap.alloc(ctl, n));
+    CLB_RETURN_IF(capp.alloc(ctl, n));
+    CLB_RETURN_IF(list.alloc(ctl, n));
+    CLB_RETURN_IF(info.alloc(ctl, 2 * NUM_BINS));
+    CLB_RETURN_IF(flags.alloc(ctl, n));
+    CLB_RETURN_IF(row_nnz.alloc(ctl, n));
+    CLB_RETURN_IF(ovf.alloc(ctl, n));
+    CLB_RETURN_IF(slot_off.alloc(ctl, n));
+    CLB_RETURN_IF(off.alloc(ctl, n));
+    CLB_RETURN_IF(scal.alloc(ctl, 8));
+    CLB_RETURN_IF(pre.alloc(ctl, slot_capacity + 4));  // + 4: the vector copy reads up to 3 words past a slot
+    CLB_TRY_CUDA(cudaMemsetAsync(scal.ptr, 0, 8 * sizeof(uint64_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(row_nnz.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(ovf.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, scal.ptr + 6));
+    upper_bound_cap_rows_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(work.ptr, n, B.ncols, t.row_ncols, cap.ptr);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    CLB_RETURN_IF(launch_binning(ctl, work.ptr, work.ptr, n, B.ncols, info.ptr, list.ptr, flags.ptr, t));
+    CLB_RETURN_IF(scan_u32_inplace(ctl, flags.ptr, n, scal.ptr + 0));  // C row positions, nzr
+    slot_sizes_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(cap.ptr, n, capp.ptr,
+                                                                 (unsigned long long *)(scal.ptr + 7));
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, capp.ptr, slot_off.ptr, n, scal.ptr + 1));
+    fit_slots_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(slot_off.ptr, capp.ptr, n, slot_capacity, cap.ptr,
+                                                                d_flags);
+    ctl->launches += 2;
+    CLB_CHECK_LAUNCH();
+    const BinLists bl{list.ptr, info.ptr};
+    RowOut num{row_nnz.ptr, slot_off.ptr, cap.ptr, ovf.ptr, pre.ptr, ctl->d_status};
+    num.row_ncols = t.row_ncols;
+    num.row_products = work.ptr;
+    // every bin is launched (no host read of the bin sizes); empty ones exit at once
+    CLB_RETURN_IF(launch_esc_accumulators(ctl, bl, a, b, num, work.ptr, n, nullptr));
+    CLB_RETURN_IF(launch_accumulators_subset(ctl, bl, a, b, num, B.ncols, n, /*hash_bins=*/false, t, nullptr));
+    drop_overflow_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, n, row_nnz.ptr, d_flags);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, row_nnz.ptr, off.ptr, n, scal.ptr + 5));  // C row offsets, nnz
+    const unsigned g = persistent_grid(ctl, 8, ceil_div_u(n, 256));
+    assemble_capture_kernel<<<g, 256, 0, ctl->stream>>>(work.ptr, flags.ptr, off.ptr, A.rows, n, first, row_base,
+                                                        count, scal.ptr + 0, scal.ptr + 5, c_rpt, c_rows);
+    capture_bounds_kernel<<<(count + 256) / 256, 256, 0, ctl->stream>>>(flags.ptr, off.ptr, n, first, count,
+                                                                        scal.ptr + 0, scal.ptr + 5, d_result + 2);
+    compact_capture_kernel<<<grid_for(ctl, n * 32, 32), 256, 0, ctl->stream>>>(
+        row_nnz.ptr, slot_off.ptr, off.ptr, pre.ptr, n, cols_capacity, c_cols, d_flags);
+    capture_status_kernel<<<1, 32, 0, ctl->stream>>>(ctl->d_status, d_flags);
+    ctl->launches += 4;
+    CLB_CHECK_LAUNCH();
+    CLB_TRY_CUDA(cudaMemcpyAsync(d_result, scal.ptr + 0, 8, cudaMemcpyDeviceToDevice, ctl->stream),
+                 CLB_COPY_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(d_result + 1, scal.ptr + 5, 8, cudaMemcpyDeviceToDevice, ctl->stream),
+                 CLB_COPY_BUFFER_ERROR);
+    return CLB_SUCCESS;
+}
+
 }  // namespace clb
 
 using namespace clb;

@@ -116,6 +116,17 @@ CLB_API int clb_controls_set_stream(clb_controls *ctl, void *stream);
 CLB_API void *clb_controls_get_stream(clb_controls *ctl);
 CLB_API int clb_controls_set_allocator(clb_controls *ctl, clb_alloc_fn alloc, clb_free_fn release, void *ctx);
 CLB_API int clb_controls_sync(clb_controls *ctl);
+/* CUDA graphs over the controls' stream (no counterpart in the reference,
+ * which enqueues OpenCL commands one by one).  clb_graph_begin starts
+ * capturing the stream (thread-local mode); operations that read nothing back
+ * to the host -- clb_dcsr_spgemm_batched_capture -- can then be recorded;
+ * clb_graph_end stops and instantiates (*graph = a cudaGraphExec_t);
+ * clb_graph_launch replays it on the stream without synchronising.  The
+ * stream must not be the legacy default stream. */
+CLB_API int clb_graph_begin(clb_controls *ctl);
+CLB_API int clb_graph_end(clb_controls *ctl, void **graph);
+CLB_API int clb_graph_launch(clb_controls *ctl, void *graph);
+CLB_API int clb_graph_destroy(void *graph);
 CLB_API int clb_controls_device(clb_controls *ctl);
 
 /* Replaces show_devices() (src/common/env.cpp:38-54). */
@@ -312,6 +323,39 @@ CLB_API int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb
 CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                 clb_spgemm_tuning *best, clb_spgemm_tuning *tried, double *ms, uint32_t max_tried,
                                 uint32_t *n_tried);
+
+/* Host-sync-free batched product (no counterpart in the reference): the
+ * pairs are stacked as in clb_dcsr_spgemm_batched and multiplied by the
+ * single-pass form into upper-bound slots, but every size comes from the
+ * caller and nothing is read back to the host, so the call can be recorded
+ * into a CUDA graph (clb_graph_begin / clb_graph_end) and replayed while the
+ * pairs' device arrays keep their sizes and change their contents.
+ * Temporaries come from the controls' stream-ordered pool (graph memory
+ * nodes when captured); tuning->form is ignored.
+ *   slot_capacity  slot entries; clb_spgemm_batched_plan gives the need of the
+ *                  current contents (sum over stacked rows of
+ *                  round_up(min(products, ncols), 4));
+ *   c_rpt, c_rows  device, rows_need + 1 and rows_need entries (rows_need =
+ *                  stored rows of the pairs with entries on both sides);
+ *   c_cols         device, cols_capacity entries (slots_need always suffices);
+ *   result         device u64[2 + 2 * (count + 1)]: [0] nzr, [1] nnz of the
+ *                  stacked C, [2 + k] its first row of pair k, [3 + count + k]
+ *                  its first column position of pair k (k = count: totals).
+ *                  Pair k is rows [r_k, r_k+1) with rpt c_rpt[r_k..r_k+1]
+ *                  minus c_rpt[r_k], row ids local to the pair, and columns
+ *                  c_cols[j_k, j_k+1);
+ *   flags          device u32, 0 when C is complete; bit 0: slot capacity
+ *                  too small (rows left empty), bit 1: cols_capacity too
+ *                  small (rows not written), bit 2: a device check failed.
+ * Returns once the work is enqueued (no synchronisation). */
+CLB_API int clb_dcsr_spgemm_batched_capture(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                                            const clb_spgemm_tuning *tuning, uint64_t slot_capacity,
+                                            uint64_t *c_rpt, uint32_t *c_rows, uint32_t *c_cols,
+                                            uint64_t cols_capacity, uint64_t *result, uint32_t *flags);
+/* Sizes for clb_dcsr_spgemm_batched_capture on the pairs' current contents
+ * (runs the workload pass and synchronises; call it outside a capture). */
+CLB_API int clb_spgemm_batched_plan(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                                    uint64_t *rows_need, uint64_t *slots_need);
 
 /* Products per A row (count_workload, dcsr_matrix_multiplication.cpp:388-404):
  * workload has a->nzr entries in device memory; *total = their sum. */
