@@ -352,10 +352,15 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     return line
 
 
+E2E_BLOCKS = 8  # row blocks of the end-to-end call (copy of one overlaps the next's product)
+
+
 def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev, mxm) -> dict:
-    """products/s through the public API: pinned host A -> device, SpGEMM,
-    all of C -> pinned host, per step."""
+    """products/s through the public API: pinned host A -> device, then
+    C = A*B delivered into pinned host arrays by clb_dcsr_spgemm_to_host (row
+    blocks: each block's copy overlaps the next block's product), per step."""
     import ctypes
+    from clbool_b200 import batched, sizing
     lib = cb.lib
 
     def pinned(nbytes):
@@ -369,9 +374,12 @@ def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev, m
     ctypes.memmove(h_cols, scols.ctypes.data, scols.nbytes)
     # size of C, to stage the read-back in pinned memory
     c0 = mxm(cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(srpt, srows, scols), n), A_full)
-    c_bytes = (8 * (c0.nzr() + 1) + 4 * c0.nzr() + 4 * c0.nnz()) if c0.nnz() else 0
+    c_nzr, c_nnz = c0.nzr(), c0.nnz()
+    c_bytes = (8 * (c_nzr + 1) + 4 * c_nzr + 4 * c_nnz) if c_nnz else 0
     h_c = pinned(c_bytes)
     del c0
+    sizer = sizing.RowSizer.load(ctl, args.sizer) if args.form == "learned" else None
+    tune = batched.tuning(form="single_pass") if args.form == "esc" else None
     steps = max(1, min(args.steps, 3))
     times = []
     for _ in range(steps):
@@ -386,13 +394,13 @@ def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev, m
         lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(d_rows.ptr), h_rows, srows.nbytes)
         lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(d_cols.ptr), h_cols, scols.nbytes)
         A = cb.matrix_dcsr(d_rpt, d_rows, d_cols, n, n, scols.size, srows.size)
-        C = mxm(A, A_full)
-        if C.nnz():
-            off = 0
-            for buf, nb in ((C.rpt_gpu(), 8 * (C.nzr() + 1)), (C.rows_gpu(), 4 * C.nzr()), (C.cols_gpu(), 4 * C.nnz())):
-                lib.clb_memcpy_d2h(ctl.handle, ctypes.c_void_p(h_c.value + off), ctypes.c_void_p(buf.ptr), nb)
-                off += nb
-        del C, A, d_rpt, d_rows, d_cols
+        if c_nnz:
+            base = h_c.value
+            got = sizing.matrix_multiplication_to_host(ctl, A, A_full, base, base + 8 * (c_nzr + 1),
+                                                       base + 8 * (c_nzr + 1) + 4 * c_nzr, c_nzr, c_nnz,
+                                                       sizer=sizer, blocks=E2E_BLOCKS, tune=tune)
+            assert got == (c_nzr, c_nnz), got
+        del A, d_rpt, d_rows, d_cols
         ctl.sync()
         dt = time.perf_counter() - t0
         if dist is not None:
@@ -413,7 +421,8 @@ def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev, m
         tot_products = float(t[0])
     sec = statistics.median(times)
     return {"value": tot_products / sec, "unit": UNIT, "h2d_bytes_per_step": int(srpt.nbytes + srows.nbytes + scols.nbytes),
-            "d2h_bytes_per_step": int(c_bytes), "s_per_step": sec, "steps": steps}
+            "d2h_bytes_per_step": int(c_bytes), "s_per_step": sec, "steps": steps,
+            "call": "clb_dcsr_spgemm_to_host", "row_blocks": E2E_BLOCKS}
 
 
 # ------------------------------------------------------------ CPU baselines --

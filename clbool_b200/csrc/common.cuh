@@ -50,6 +50,7 @@ struct clb_controls {
     int sm_count = 148;
     size_t smem_optin = 0;
     uint64_t *h_scalars = nullptr;  // pinned scalar staging (64 entries)
+    uint64_t *d_h_scalars = nullptr;  // the same staging as the device addresses it
     uint32_t *d_status = nullptr;   // device status word
     clb_alloc_fn alloc = nullptr;
     clb_free_fn release = nullptr;
@@ -126,6 +127,12 @@ struct ProfScope {
 
 // Reads `count` 64-bit scalars from device memory (one sync).
 int read_scalars(clb_controls *ctl, const uint64_t *d_src, uint64_t *h_dst, int count);
+// Reads `bytes` (a multiple of 4, at most 512) of device memory into h_dst
+// through the page-locked staging: a one-warp kernel stores the words there
+// over PCIe, so the read does not queue behind large copies on the copy
+// engine (clb_dcsr_spgemm_to_host copies row blocks while the next block's
+// call reads its sizes back).  Synchronises the stream.
+int read_small(clb_controls *ctl, const void *d_src, void *h_dst, size_t bytes);
 // Clears, then after the call checks, the device status word.
 int clear_status(clb_controls *ctl);
 int check_status(clb_controls *ctl, const char *op);

@@ -43,12 +43,28 @@ void dev_free(clb_controls *ctl, void *p) {
     cudaFreeAsync(p, ctl->stream);
 }
 
-int read_scalars(clb_controls *ctl, const uint64_t *d_src, uint64_t *h_dst, int count) {
-    CLB_TRY_CUDA(cudaMemcpyAsync(ctl->h_scalars, d_src, sizeof(uint64_t) * count, cudaMemcpyDeviceToHost, ctl->stream),
-                 CLB_READ_BUFFER_ERROR);
+namespace {
+// Device words -> page-locked host staging, stored by the SMs over PCIe.
+__global__ void stage_words_kernel(const uint32_t *__restrict__ src, uint32_t n, volatile uint32_t *dst) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+    __threadfence_system();
+}
+}  // namespace
+
+int read_small(clb_controls *ctl, const void *d_src, void *h_dst, size_t bytes) {
+    if (bytes == 0) return CLB_SUCCESS;
+    if (bytes > 64 * sizeof(uint64_t) || (bytes & 3)) return fail(CLB_INVALID_ARGUMENT, "read_small: bad size");
+    stage_words_kernel<<<1, 32, 0, ctl->stream>>>(static_cast<const uint32_t *>(d_src), (uint32_t)(bytes / 4),
+                                                   reinterpret_cast<volatile uint32_t *>(ctl->d_h_scalars));
+    CLB_TRY_CUDA(cudaGetLastError(), CLB_RUN_KERNEL_FAILURE);
+    ctl->launches += 1;
     CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
-    memcpy(h_dst, ctl->h_scalars, sizeof(uint64_t) * count);
+    memcpy(h_dst, ctl->h_scalars, bytes);
     return CLB_SUCCESS;
+}
+
+int read_scalars(clb_controls *ctl, const uint64_t *d_src, uint64_t *h_dst, int count) {
+    return read_small(ctl, d_src, h_dst, sizeof(uint64_t) * (size_t)count);
 }
 
 int clear_status(clb_controls *ctl) {
@@ -57,11 +73,8 @@ int clear_status(clb_controls *ctl) {
 }
 
 int check_status(clb_controls *ctl, const char *op) {
-    CLB_TRY_CUDA(cudaMemcpyAsync(ctl->h_scalars + 63, ctl->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                 ctl->stream),
-                 CLB_READ_BUFFER_ERROR);
-    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
-    uint32_t s = (uint32_t)(ctl->h_scalars[63] & 0xFFFFFFFFu);
+    uint32_t s = 0;
+    CLB_RETURN_IF(read_small(ctl, ctl->d_status, &s, sizeof(uint32_t)));
     if (s != 0) {
         char buf[160];
         snprintf(buf, sizeof(buf), "%s: device status word 0x%x", op, s);
@@ -180,6 +193,7 @@ int clb_controls_create(int device, clb_controls **out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctl->stream, cudaStreamNonBlocking);
     ctl->own_stream = true;
     if (e == cudaSuccess) e = cudaMallocHost(&ctl->h_scalars, 64 * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&ctl->d_h_scalars, ctl->h_scalars, 0);
     if (e == cudaSuccess) e = cudaMalloc(&ctl->d_status, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(ctl->d_status, 0, sizeof(uint32_t));
     if (e == cudaSuccess) {

@@ -169,9 +169,7 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     CLB_TRY_CUDA(cudaMemsetAsync(row_nnz.ptr, 0, n * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     // rows per bin: only the bins with rows are launched, sized to them
     uint32_t hinfo[NUM_BINS];
-    CLB_TRY_CUDA(cudaMemcpyAsync(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost, ctl->stream),
-                 CLB_READ_BUFFER_ERROR);
-    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    CLB_RETURN_IF(read_small(ctl, info.ptr, hinfo, sizeof(hinfo)));
 
     BinLists bl{list.ptr, info.ptr};
     RowOut sym{row_nnz.ptr, nullptr, nullptr, nullptr, nullptr, ctl->d_status};

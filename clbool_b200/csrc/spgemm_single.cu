@@ -319,9 +319,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     CLB_RETURN_IF(read_scalars(ctl, scal.ptr + 7, &capacity, 1));
     const uint64_t nzr = h[0], slots = h[1];
     uint32_t hinfo[NUM_BINS];  // rows per bin: only bins with rows are launched
-    CLB_TRY_CUDA(cudaMemcpyAsync(hinfo, info.ptr, sizeof(hinfo), cudaMemcpyDeviceToHost, ctl->stream),
-                 CLB_READ_BUFFER_ERROR);
-    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    CLB_RETURN_IF(read_small(ctl, info.ptr, hinfo, sizeof(hinfo)));
     if (st) {
         for (int k = 0; k < NUM_BINS; ++k) st->rows_per_bin[k] = hinfo[k];
         st->capacity = capacity;

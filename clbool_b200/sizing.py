@@ -147,3 +147,26 @@ def matrix_multiplication_learned(controls: Controls, matrix_out: matrix_dcsr | 
     if stats is not None:
         stats.update(st.as_dict())
     return res if matrix_out is None else matrix_out._assign(res)
+
+
+def matrix_multiplication_to_host(controls: Controls, a: matrix_dcsr, b: matrix_dcsr, h_rpt, h_rows, h_cols,
+                                  rows_capacity: int, cols_capacity: int, sizer: RowSizer | None = None,
+                                  margin_log2: float = DEFAULT_MARGIN_LOG2, slack: float = DEFAULT_SLACK,
+                                  blocks: int = 8, tune=None, stats: dict | None = None):
+    """C = A*B written into host arrays (numpy arrays or raw addresses of
+    page-locked buffers): row blocks of A are multiplied in turn (learned form
+    when `sizer` is given, else the tuned form) while the previous block's
+    rows are copied out.  Returns (nzr, nnz)."""
+    def addr(x):
+        return C.c_void_p(x.ctypes.data if isinstance(x, np.ndarray) else int(x))
+    nzr, nnz = C.c_uint64(), C.c_uint64()
+    st = clb_spgemm_stats()
+    sa, sb = a.c_struct(), b.c_struct()
+    check(lib.clb_dcsr_spgemm_to_host(controls.handle, C.byref(sa), C.byref(sb), sizer.handle if sizer else None,
+                                      float(margin_log2), float(slack), C.byref(tune) if tune is not None else None,
+                                      int(blocks), addr(h_rpt), addr(h_rows), addr(h_cols), int(rows_capacity),
+                                      int(cols_capacity), C.byref(nzr), C.byref(nnz), C.byref(st)),
+          "matrix_multiplication_to_host")
+    if stats is not None:
+        stats.update(st.as_dict())
+    return int(nzr.value), int(nnz.value)

@@ -324,6 +324,24 @@ CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcs
                                 clb_spgemm_tuning *best, clb_spgemm_tuning *tried, double *ms, uint32_t max_tried,
                                 uint32_t *n_tried);
 
+/* C = A*B written into host memory (no counterpart in the reference, whose
+ * product stays on the device until matrix_dcsr_to_cpu,
+ * src/common/matrices_conversions.cpp:115-139).  A's stored rows are cut into
+ * `blocks` (1..64) ranges of about equal products; each block is one call of
+ * the learned form (sizer != NULL, with margin_log2 / slack / tuning as in
+ * clb_dcsr_spgemm_learned) or of clb_dcsr_spgemm_tuned (sizer == NULL), and
+ * its rows are copied to the host on a second stream while the next block
+ * is multiplied.  h_rpt: rows_capacity + 1 entries, h_rows: rows_capacity,
+ * h_cols: cols_capacity (page-locked memory, e.g. clb_host_alloc, lets the
+ * copies overlap; pageable memory works without overlap).  On return
+ * *nzr / *nnz give C's size and the arrays hold C; too small arrays give
+ * CLB_INVALID_VALUE.  stats (optional) sums the blocks. */
+CLB_API int clb_dcsr_spgemm_to_host(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_sizer *sizer,
+                                    float margin_log2, float slack, const clb_spgemm_tuning *tuning,
+                                    uint32_t blocks, uint64_t *h_rpt, uint32_t *h_rows, uint32_t *h_cols,
+                                    uint64_t rows_capacity, uint64_t cols_capacity, uint64_t *nzr, uint64_t *nnz,
+                                    clb_spgemm_stats *stats);
+
 /* Host-sync-free batched product (no counterpart in the reference): the
  * pairs are stacked as in clb_dcsr_spgemm_batched and multiplied by the
  * single-pass form into upper-bound slots, but every size comes from the
