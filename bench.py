@@ -564,6 +564,24 @@ def run_batch(args) -> dict:
     ms_default = _event_ms(stream, batched(default), args.steps)
     ms_seq = _event_ms(stream, sequential, max(1, args.steps // 2))
     batched(best)()
+    # the host-sync-free batched form recorded once into a CUDA graph, replayed
+    from clbool_b200 import batched as bt
+    cap = bt.CapturedBatch(ctl, pairs, tune=best)
+    graph = bt.Graph(ctl, cap.enqueue)
+    for _ in range(max(3, args.warmup)):
+        graph.launch()
+    got = cap.result()
+    ref = cb.dcsr.matrix_multiplication_batched(ctl, pairs, tune=best)
+    exact = True
+    for (rpt, rws, cls), c in zip(got, ref):
+        h = cb.matrix_dcsr_from_gpu(ctl, c) if c.nnz() else None
+        if h is None:
+            exact &= len(cls) == 0
+        else:
+            exact &= bool(np.array_equal(rpt, h.rpt) and np.array_equal(rws, h.rows) and np.array_equal(cls, h.cols))
+    del ref
+    ms_graph = _event_ms(stream, graph.launch, args.steps)
+    graph.close()
     return {"metric": METRIC, "workload": f"batch{args.pairs}_powerlaw", "value": products / (ms_best / 1e3),
             "unit": UNIT, "ms_per_step": ms_best, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
             "higher_is_better": True, "dtype": "u32", "data": "synthetic",
@@ -572,8 +590,66 @@ def run_batch(args) -> dict:
                        "row_lengths": "power law 2.1, mean 6, max 4096"},
             "autotuned": best.as_dict(), "default_ms": ms_default, "sequential_ms": ms_seq,
             "batched_over_sequential": ms_seq / ms_best,
+            "graph_replay": {"ms": ms_graph, "products_per_s": products / (ms_graph / 1e3),
+                             "bit_exact_vs_batched": exact, "slot_capacity": cap.slot_capacity},
             "kernel_launches_per_batch": st.get("kernel_launches"),
             "candidates_ms": sorted(((t, round(m, 3)) for t, m in tried), key=lambda x: x[1])}
+
+
+def run_rmat_add(args) -> dict:
+    """The headline workload's second operation: CSR addition C + A with
+    C = A*A at R-MAT scale 20 (entries/s of C + A; 64 seeded rows of the sum
+    checked against the union of the operands' rows)."""
+    import ctypes
+
+    import torch
+
+    import clbool_b200 as cb
+    from clbool_b200 import sizing
+    ctl = cb.create_controls(0, 0)
+    stream = torch.cuda.ExternalStream(ctl.stream, device="cuda:0")
+    n, rpt, rows, cols = rmat_a(args.scale)
+    A = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(rpt, rows, cols), n)
+    sizer = sizing.RowSizer.load(ctl, args.sizer)
+    C = sizing.matrix_multiplication_learned(ctl, None, A, A, sizer)
+    Cc, Ac = cb.dcsr_to_csr(ctl, C), cb.dcsr_to_csr(ctl, A)
+    del C
+    S = cb.csr.matrix_addition(ctl, None, Cc, Ac)
+    nnz_c, nnz_s = Cc.nnz(), S.nnz()
+
+    def row(m, r, rp):
+        lo, hi = int(rp[r]), int(rp[r + 1])
+        seg = np.empty(hi - lo, np.uint32)
+        if hi > lo:
+            cb.lib.clb_memcpy_d2h(ctl.handle, seg.ctypes.data_as(ctypes.c_void_p),
+                                  ctypes.c_void_p(m.cols_gpu().ptr + 4 * lo), 4 * (hi - lo))
+        return seg
+    crp, srp = Cc.rpt_gpu().to_host(n + 1), S.rpt_gpu().to_host(n + 1)
+    arp = np.zeros(n + 1, np.int64)
+    arp[rows.astype(np.int64) + 1] = np.diff(rpt.astype(np.int64))
+    arp = np.cumsum(arp)
+    exact = True
+    for r in np.random.default_rng(5).choice(n, 64, replace=False):
+        want = np.union1d(row(Cc, r, crp), cols[arp[r]:arp[r + 1]])
+        exact &= bool(np.array_equal(row(S, r, srp), want))
+    del S
+
+    def step():
+        out = cb.csr.matrix_addition(ctl, None, Cc, Ac)
+        del out
+    for _ in range(max(1, args.warmup - 1)):
+        step()
+    ms = _event_ms(stream, step, max(3, args.steps))
+    alg = 4 * (cols.size + nnz_c + nnz_s) + 8 * (n + 1) * 3
+    peak, kind = peaks()
+    achieved = alg / (ms / 1e3) / 1e9
+    return {"metric": "bool CSR addition entries/s (C + A)", "workload": f"rmat_s{args.scale}_csr_add",
+            "value": nnz_s / (ms / 1e3), "unit": "entries/s", "ms_per_step": ms, "n_gpus": 1, "data": "synthetic",
+            "higher_is_better": True, "dtype": "u32",
+            "config": {"workload": f"rmat_s{args.scale}_C_plus_A", "nnz_A": int(cols.size), "nnz_C": int(nnz_c),
+                       "nnz_sum": int(nnz_s), "rows_checked": 64, "rows_match_union": exact},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": kind, "unit": "GB/s",
+                         "frac": achieved / peak, "alg_bytes": alg}}
 
 
 def run_small(args) -> dict:
@@ -767,14 +843,14 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="rmat",
-                    choices=["rmat", "batch", "poisson4096", "cfpq", "kron", "rmat21"],
+                    choices=["rmat", "batch", "poisson4096", "cfpq", "kron", "rmat21", "rmat_add"],
                     help="rmat: the headline A*A; batch / poisson4096: secondary workloads (own JSON line)")
     ap.add_argument("--pairs", type=int, default=256)
     ap.add_argument("--blocks", type=int, default=4, help="row blocks of the scale-21 run")
     args = ap.parse_args()
     if args.workload != "rmat":
         fn = {"batch": run_batch, "poisson4096": run_small, "cfpq": run_cfpq, "kron": run_kron,
-              "rmat21": run_rmat21}[args.workload]
+              "rmat21": run_rmat21, "rmat_add": run_rmat_add}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
     if args.form is None:

@@ -19,6 +19,8 @@
 // entry's row comes from a search of the row pointer over the tile's row
 // range.  C's CSR row pointer is lenA + lenB - (duplicates of the row),
 // counted with one atomic per duplicate, then scanned.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace clb {
@@ -196,6 +198,218 @@ __global__ void __launch_bounds__(MP_NT) merge_tile_kernel(CooSide Ac, CooSide B
     }
 }
 
+// ------------------------------------------------- CSR insertion path --
+// When one operand is much sparser than the other (the closure step C + A,
+// say), C's row r is the longer row X of the two with the shorter row Y
+// inserted: every entry of Y finds its place in X by binary search (a warp
+// takes 32 entries at a time, each search starting where the previous
+// chunk ended), and X is copied in the segments between the insertions.
+// X is read once, by coalesced copies; no keys are staged.
+
+// Sum over rows of min(lenA, lenB): the entries that need a search.
+__global__ void csr_min_sum_kernel(const uint64_t *__restrict__ arpt, const uint64_t *__restrict__ brpt, uint64_t nrows,
+                                   unsigned long long *__restrict__ out) {
+    unsigned long long mine = 0;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += (uint64_t)gridDim.x * blockDim.x)
+        mine += min(arpt[r + 1] - arpt[r], brpt[r + 1] - brpt[r]);
+    mine = warp_sum(mine);
+    if (lane_id() == 0 && mine) atomicAdd(out, mine);
+}
+
+// First position in x[lo, n) whose value is >= y.
+__device__ __forceinline__ uint64_t lower_bound_from(const uint32_t *x, uint64_t lo, uint64_t n, uint32_t y) {
+    uint64_t hi = n;
+    while (lo < hi) {
+        const uint64_t m = lo + (hi - lo) / 2;
+        if (__ldg(x + m) < y) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
+struct RowPair {
+    const uint32_t *x, *y;  // longer and shorter row
+    uint64_t nx, ny;
+};
+
+__device__ __forceinline__ RowPair row_pair(const CsrSide &A, const CsrSide &B, uint64_t r) {
+    const uint64_t a0 = A.rpt[r], a1 = A.rpt[r + 1], b0 = B.rpt[r], b1 = B.rpt[r + 1];
+    const uint64_t la = a1 - a0, lb = b1 - b0;
+    return la >= lb ? RowPair{A.cols + a0, B.cols + b0, la, lb} : RowPair{B.cols + b0, A.cols + a0, lb, la};
+}
+
+// Warp copy of x[from, to) to dst[from .. to) (dst already shifted).
+// Eight loads in flight per lane before the stores: a warp may copy a row
+// of a million entries, which one load at a time would leave latency-bound.
+__device__ __forceinline__ void warp_copy_seg(const uint32_t *__restrict__ x, uint64_t from, uint64_t to,
+                                              uint32_t *__restrict__ dst) {
+    uint64_t j = from + lane_id();
+    for (; j + 7 * 32 < to; j += 8 * 32) {
+        uint32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldg(x + j + u * 32);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) dst[j + u * 32] = v[u];
+    }
+    for (; j < to; j += 32) dst[j] = __ldg(x + j);
+}
+
+// MODE 0: out_cnt[r] = |X| + |Y| - |X and Y|.  MODE 1: row r of the sum at
+// cols + rpt[r].  One warp per row.
+// Rows whose shorter side has more than INS_LONG entries (the hub rows of a
+// power-law matrix) are listed by the count pass and left to
+// csr_insert_long_kernel, which spreads their chunks over a CTA.
+constexpr uint64_t INS_LONG = 256;
+constexpr uint32_t INS_MAX_CHUNKS = 4096;  // the CTA kernel's chunk table (longer rows stay here)
+
+__device__ __forceinline__ bool ins_long_row(uint64_t ny) {
+    return ny > INS_LONG && ny <= (uint64_t)INS_MAX_CHUNKS * 32;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) csr_insert_kernel(CsrSide A, CsrSide B, uint64_t nrows,
+                                                         uint64_t *__restrict__ out_cnt,
+                                                         const uint64_t *__restrict__ rpt,
+                                                         uint32_t *__restrict__ cols,
+                                                         uint32_t *__restrict__ long_rows,
+                                                         uint32_t *__restrict__ n_long) {
+    const uint32_t lane = lane_id();
+    const uint32_t ltmask = (1u << lane) - 1u;
+    const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t r = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); r < nrows; r += nw) {
+        const RowPair p = row_pair(A, B, r);
+        if (ins_long_row(p.ny)) {
+            if (MODE == 0 && lane == 0) long_rows[atomicAdd(n_long, 1u)] = (uint32_t)r;
+            continue;
+        }
+        uint32_t *const dst = MODE ? cols + rpt[r] : nullptr;
+        if (p.ny == 0) {
+            if (MODE == 0) {
+                if (lane == 0) out_cnt[r] = p.nx;
+            } else {
+                warp_copy_seg(p.x, 0, p.nx, dst);
+            }
+            continue;
+        }
+        uint64_t lo = 0, copied = 0, shift = 0, dups = 0;
+        for (uint64_t c0 = 0; c0 < p.ny; c0 += 32) {
+            const uint64_t k = c0 + lane;
+            const bool valid = k < p.ny;
+            const uint32_t y = valid ? __ldg(p.y + k) : 0xFFFFFFFFu;
+            const uint64_t pos = valid ? lower_bound_from(p.x, lo, p.nx, y) : p.nx;
+            const bool dup = valid && pos < p.nx && __ldg(p.x + pos) == y;
+            const uint32_t mdup = __ballot_sync(0xFFFFFFFFu, dup);
+            const uint32_t mins = __ballot_sync(0xFFFFFFFFu, valid && !dup);
+            dups += __popc(mdup);
+            if (MODE == 1) {
+                const uint32_t excl = __popc(mins & ltmask);
+                if (valid && !dup) dst[pos + shift + excl] = y;
+                // X up to each insertion point, shifted by the insertions before it
+                uint32_t m = mins;
+                uint32_t before = 0;
+                while (m) {
+                    const uint32_t l = __ffs(m) - 1;
+                    m &= m - 1;
+                    const uint64_t pl = __shfl_sync(0xFFFFFFFFu, pos, l);
+                    warp_copy_seg(p.x, copied, pl, dst + shift + before);
+                    copied = pl;
+                    ++before;
+                }
+                shift += __popc(mins);
+            }
+            // the next chunk's entries are larger: search from the last position
+            const uint32_t last = p.ny - c0 >= 32 ? 31u : (uint32_t)(p.ny - 1 - c0);
+            lo = __shfl_sync(0xFFFFFFFFu, pos, last);
+        }
+        if (MODE == 0) {
+            if (lane == 0) out_cnt[r] = p.nx + p.ny - dups;
+        } else {
+            warp_copy_seg(p.x, copied, p.nx, dst + shift);
+        }
+    }
+}
+
+// The listed long rows, one CTA each.  Chunk c (Y entries 32c..32c+31)
+// owns X[S_c, S_c+1) with S_0 = 0, S_c = position of its first entry (c > 0)
+// and S_last = |X|; its entries' insertions shift that range by the
+// non-duplicate entries of the chunks before it (a block scan over the
+// chunks).  MODE 0: out_cnt[r]; MODE 1: the row at cols + rpt[r].
+template <int MODE>
+__global__ void __launch_bounds__(256) csr_insert_long_kernel(CsrSide A, CsrSide B, const uint32_t *__restrict__ long_rows,
+                                                              const uint32_t *__restrict__ n_long,
+                                                              uint64_t *__restrict__ out_cnt,
+                                                              const uint64_t *__restrict__ rpt,
+                                                              uint32_t *__restrict__ cols) {
+    constexpr int NWARP = 8;
+    __shared__ uint32_t s_start[INS_MAX_CHUNKS + 1];  // S_c
+    __shared__ uint32_t s_nd[INS_MAX_CHUNKS];         // non-duplicate entries of chunk c, then their prefix
+    __shared__ uint32_t scratch[33];
+    const uint32_t lane = lane_id(), w = warp_id();
+    const uint32_t ltmask = (1u << lane) - 1u;
+    const uint32_t nl = *n_long;
+    for (uint32_t item = blockIdx.x; item < nl; item += gridDim.x) {
+        const uint64_t r = long_rows[item];
+        const RowPair p = row_pair(A, B, r);
+        const uint32_t nch = (uint32_t)((p.ny + 31) / 32);
+        // pass over the chunks: positions of the first entries and counts
+        for (uint32_t c = w; c < nch; c += NWARP) {
+            const uint64_t k = (uint64_t)c * 32 + lane;
+            const bool valid = k < p.ny;
+            const uint32_t y = valid ? __ldg(p.y + k) : 0xFFFFFFFFu;
+            const uint64_t pos = valid ? lower_bound_from(p.x, 0, p.nx, y) : p.nx;
+            const bool dup = valid && pos < p.nx && __ldg(p.x + pos) == y;
+            const uint32_t mins = __ballot_sync(0xFFFFFFFFu, valid && !dup);
+            if (lane == 0) {
+                s_start[c] = c == 0 ? 0u : (uint32_t)pos;
+                s_nd[c] = __popc(mins);
+            }
+        }
+        if (threadIdx.x == 0) s_start[nch] = (uint32_t)p.nx;
+        __syncthreads();
+        // prefix of the non-duplicate counts over the chunks
+        uint32_t run = 0;
+        const uint32_t per = (nch + blockDim.x - 1) / blockDim.x;
+        const uint32_t c0 = threadIdx.x * per, c1 = min(c0 + per, nch);
+        for (uint32_t c = c0; c < c1; ++c) run += s_nd[c];
+        uint32_t total;
+        uint32_t base = block_exclusive_scan<uint32_t, 256>(run, scratch, &total);
+        if (MODE == 0) {
+            if (threadIdx.x == 0) out_cnt[r] = p.nx + total;
+            __syncthreads();
+        } else {
+        for (uint32_t c = c0; c < c1; ++c) {
+            const uint32_t v = s_nd[c];
+            s_nd[c] = base;
+            base += v;
+        }
+        __syncthreads();
+        uint32_t *const dst = cols + rpt[r];
+        for (uint32_t c = w; c < nch; c += NWARP) {
+            const uint64_t k = (uint64_t)c * 32 + lane;
+            const bool valid = k < p.ny;
+            const uint32_t y = valid ? __ldg(p.y + k) : 0xFFFFFFFFu;
+            const uint64_t lo = s_start[c];
+            const uint64_t pos = valid ? lower_bound_from(p.x, lo, p.nx, y) : p.nx;
+            const bool dup = valid && pos < p.nx && __ldg(p.x + pos) == y;
+            const uint32_t mins = __ballot_sync(0xFFFFFFFFu, valid && !dup);
+            const uint64_t shift = s_nd[c];
+            if (valid && !dup) dst[pos + shift + __popc(mins & ltmask)] = y;
+            uint64_t copied = lo;
+            uint32_t m = mins, before = 0;
+            while (m) {
+                const uint32_t l = __ffs(m) - 1;
+                m &= m - 1;
+                const uint64_t pl = __shfl_sync(0xFFFFFFFFu, pos, l);
+                warp_copy_seg(p.x, copied, pl, dst + shift + before);
+                copied = pl;
+                ++before;
+            }
+            warp_copy_seg(p.x, copied, s_start[c + 1], dst + shift + before);
+        }
+        __syncthreads();
+        }
+    }
+}
+
 // c_cnt[r] = lenA + lenB - dup[r]  (scanned afterwards into C's rpt).
 __global__ void csr_row_counts_kernel(const uint64_t *__restrict__ arpt, const uint64_t *__restrict__ brpt,
                                       const uint32_t *__restrict__ dup, uint64_t nrows, uint64_t *__restrict__ out) {
@@ -312,6 +526,51 @@ int clb_csr_add(clb_controls *ctl, const clb_csr *a_, const clb_csr *b_, clb_csr
     if (a.nrows >= (1ull << 32)) return fail(CLB_NOT_SUPPORTED, "2^32 or more rows");
     ProfScope ps(ctl, "csr_add");
     const CsrSide A{a.rpt, a.cols, a.nnz}, B{b.rpt, b.cols, b.nnz};
+    {
+        // one operand much sparser (at most 1/16 of the entries need a
+        // search): insertion path
+        Temp<uint64_t> ms;
+        CLB_RETURN_IF(ms.alloc(ctl, 1));
+        CLB_TRY_CUDA(cudaMemsetAsync(ms.ptr, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+        csr_min_sum_kernel<<<grid_for(ctl, a.nrows), 256, 0, ctl->stream>>>(a.rpt, b.rpt, a.nrows,
+                                                                             (unsigned long long *)ms.ptr);
+        CLB_CHECK_LAUNCH();
+        uint64_t searched = 0;
+        CLB_RETURN_IF(read_scalars(ctl, ms.ptr, &searched, 1));
+        if (searched * 16 <= a.nnz + b.nnz) {
+            Temp<uint64_t> rpt, tot;
+            CLB_RETURN_IF(rpt.alloc(ctl, a.nrows + 1));
+            CLB_RETURN_IF(tot.alloc(ctl, 1));
+            const unsigned gw = (unsigned)std::min<uint64_t>((a.nrows + 7) / 8, (uint64_t)ctl->sm_count * 8);
+            Temp<uint32_t> lrows, nlong;
+            CLB_RETURN_IF(lrows.alloc(ctl, a.nrows));
+            CLB_RETURN_IF(nlong.alloc(ctl, 1));
+            CLB_TRY_CUDA(cudaMemsetAsync(nlong.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+            csr_insert_kernel<0><<<gw, 256, 0, ctl->stream>>>(A, B, a.nrows, rpt.ptr, nullptr, nullptr, lrows.ptr,
+                                                              nlong.ptr);
+            csr_insert_long_kernel<0><<<ctl->sm_count * 2, 256, 0, ctl->stream>>>(A, B, lrows.ptr, nlong.ptr, rpt.ptr,
+                                                                                 nullptr, nullptr);
+            CLB_CHECK_LAUNCH();
+            CLB_RETURN_IF(scan_u64_inplace(ctl, rpt.ptr, a.nrows, tot.ptr));
+            uint64_t nnz = 0;
+            CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &nnz, 1));
+            CLB_TRY_CUDA(cudaMemcpyAsync(rpt.ptr + a.nrows, tot.ptr, 8, cudaMemcpyDeviceToDevice, ctl->stream),
+                         CLB_COPY_BUFFER_ERROR);
+            Temp<uint32_t> cols;
+            CLB_RETURN_IF(cols.alloc(ctl, nnz));
+            csr_insert_kernel<1><<<gw, 256, 0, ctl->stream>>>(A, B, a.nrows, nullptr, rpt.ptr, cols.ptr, nullptr,
+                                                              nullptr);
+            csr_insert_long_kernel<1><<<ctl->sm_count * 2, 256, 0, ctl->stream>>>(A, B, lrows.ptr, nlong.ptr, nullptr,
+                                                                                 rpt.ptr, cols.ptr);
+            CLB_CHECK_LAUNCH();
+            CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+            c.nnz = nnz;
+            c.rpt = rpt.release_ownership();
+            c.cols = cols.release_ownership();
+            *out = c;
+            return CLB_SUCCESS;
+        }
+    }
     const CooSide none{nullptr, nullptr, 0};
     const uint64_t total = a.nnz + b.nnz, ntiles = (total + MP_TILE - 1) / MP_TILE;
     if (ntiles >= (1ull << 31)) return fail(CLB_NOT_SUPPORTED, "addition too large");

@@ -82,6 +82,47 @@ def test_addition_csr_skewed(controls):
     assert np.array_equal(h.rpt, want.rpt) and np.array_equal(h.cols, want.cols)
 
 
+def test_addition_csr_insertion(controls):
+    """One operand far sparser than the other (the insertion path): entries
+    before, between (several at one gap) and after the long row's entries,
+    duplicates, rows only one side has, a row where the sparse side is the
+    longer one, both operand orders."""
+    import clbool_b200 as cb
+    rng = np.random.default_rng(8)
+    n, ncols = 3000, 100000
+    big_r, big_c, small_r, small_c = [], [], [], []
+    for r in range(n):
+        if r % 7 == 3:
+            continue  # empty on the long side
+        cols = np.sort(rng.choice(np.arange(10, ncols - 10), 300, replace=False))
+        big_r.append(np.full(cols.size, r)); big_c.append(cols)
+        if r % 5 == 0:
+            k = int(rng.integers(1, 6))
+            picks = [0, ncols - 1, int(cols[0]) + 1 if cols[1] > cols[0] + 2 else 1]
+            picks += list(rng.choice(cols, k))                       # duplicates
+            picks += [int(cols[40]) + 1, int(cols[40]) + 2] if cols[41] > cols[40] + 3 else []
+            sc = np.unique(np.array(picks))
+            small_r.append(np.full(sc.size, r)); small_c.append(sc)
+    for r in (3, 10, 17):  # rows the long side does not have
+        sc = np.sort(rng.choice(ncols, 4, replace=False))
+        small_r.append(np.full(sc.size, r)); small_c.append(sc)
+    sc = np.arange(0, 700, 1)  # the sparse side is longer in this row (r = 24 has 300 on the other)
+    small_r.append(np.full(sc.size, 24)); small_c.append(sc)
+    br, bc = np.concatenate(big_r).astype(np.uint32), np.concatenate(big_c).astype(np.uint32)
+    sr, sc_ = np.concatenate(small_r).astype(np.uint32), np.concatenate(small_c).astype(np.uint32)
+    o = np.lexsort((sc_, sr)); sr, sc_ = sr[o], sc_[o]
+    keep = np.concatenate([[True], (sr[1:] != sr[:-1]) | (sc_[1:] != sc_[:-1])]); sr, sc_ = sr[keep], sc_[keep]
+    big = O.coo_to_csr(O.Coo(n, ncols, br, bc))
+    small = O.coo_to_csr(O.Coo(n, ncols, sr, sc_))
+    assert len(small.cols) * 16 < len(big.cols)
+    for x, y in ((big, small), (small, big)):
+        X = cb.csr_from_cpu(controls, cb.matrix_csr_cpu(x.rpt, x.cols, n, ncols))
+        Y = cb.csr_from_cpu(controls, cb.matrix_csr_cpu(y.rpt, y.cols, n, ncols))
+        h = cb.matrix_csr_from_gpu(controls, cb.csr.matrix_addition(controls, None, X, Y))
+        want = O.csr_add(x, y)
+        assert np.array_equal(h.rpt, want.rpt) and np.array_equal(h.cols, want.cols)
+
+
 def test_addition_empty_and_shape(controls):
     import clbool_b200 as cb
     a = _coo_dev(controls, *O.generate_coo_pairs(500, 100), 100)
