@@ -110,6 +110,26 @@ int main(int argc, char **argv) {
         EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, batch[0])) == product(pa, pb));
         EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, batch[1])) == product(pb, pa));
         EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, batch[2])) == product(pa, pa));
+        // C written straight into host memory, in 3 row blocks
+        {
+            matrix_dcsr_cpu h = dcsr::matrix_multiplication_to_host(controls, A, B, n, (uint64_t)n * n, &sizer, 3);
+            matrix_dcsr_cpu w = matrix_dcsr_from_gpu(controls, C);
+            EXPECT(h.rpt == w.rpt && h.rows == w.rows && h.cols == w.cols);
+        }
+        // the host-sync-free batch, recorded into a CUDA graph and replayed twice
+        {
+            dcsr::CapturedBatch cap(controls, {{A, B}, {B, A}});
+            dcsr::Graph graph(controls, [&] { cap.enqueue(); });
+            for (int rep = 0; rep < 2; ++rep) {
+                graph.launch();
+                auto got = cap.result();
+                EXPECT(got.size() == 2);
+                matrix_dcsr_cpu w0 = matrix_dcsr_from_gpu(controls, batch[0]);
+                matrix_dcsr_cpu w1 = matrix_dcsr_from_gpu(controls, batch[1]);
+                EXPECT(got[0].rpt == w0.rpt && got[0].rows == w0.rows && got[0].cols == w0.cols);
+                EXPECT(got[1].rpt == w1.rpt && got[1].rows == w1.rows && got[1].cols == w1.cols);
+            }
+        }
 
         std::vector<uint32_t> ar, ac, br, bc;
         for (auto &p : pa) { ar.push_back(p.first); ac.push_back(p.second); }

@@ -451,6 +451,120 @@ inline std::vector<matrix_dcsr> matrix_multiplication_batched(
     for (auto &m : vc) out.push_back(matrix_dcsr::adopt(c, m));
     return out;
 }
+
+// C = A*B written into host memory, in row blocks of A whose copies overlap
+// the next block's product (learned form with a sizer, exact form without).
+// rows_capacity / cols_capacity bound C's stored rows / entries.
+inline matrix_dcsr_cpu matrix_multiplication_to_host(Controls &c, const matrix_dcsr &a, const matrix_dcsr &b,
+                                                     uint64_t rows_capacity, uint64_t cols_capacity,
+                                                     const RowSizer *sizer = nullptr, uint32_t blocks = 8,
+                                                     clb_spgemm_stats *stats = nullptr) {
+    clb_dcsr va = a.view(), vb = b.view();
+    matrix_dcsr_cpu out;
+    out.rpt.resize(rows_capacity + 1);
+    out.rows.resize(rows_capacity);
+    out.cols.resize(cols_capacity);
+    uint64_t nzr = 0, nnz = 0;
+    details::check(clb_dcsr_spgemm_to_host(c.get(), &va, &vb, sizer ? sizer->get() : nullptr, 0.25f, 8.0f, nullptr,
+                                           blocks, out.rpt.data(), out.rows.data(), out.cols.data(), rows_capacity,
+                                           cols_capacity, &nzr, &nnz, stats));
+    out.rpt.resize(nzr + 1);
+    out.rows.resize(nzr);
+    out.cols.resize(nnz);
+    return out;
+}
+
+// A CUDA graph recorded from the controls' stream: Graph g(c, [&] { ... });
+// then g.launch() replays the recorded work.
+class Graph {
+public:
+    template <class F>
+    Graph(Controls &c, F &&record) : c_(c) {
+        details::check(clb_graph_begin(c.get()));
+        void *g = nullptr;
+        try {
+            record();
+        } catch (...) {
+            clb_graph_end(c.get(), &g);
+            clb_graph_destroy(g);
+            throw;
+        }
+        details::check(clb_graph_end(c.get(), &g));
+        g_.reset(g, [](void *p) { clb_graph_destroy(p); });
+    }
+    void launch() { details::check(clb_graph_launch(c_.get(), g_.get())); }
+
+private:
+    Controls c_;
+    std::shared_ptr<void> g_;
+};
+
+// The host-sync-free batched product (clb_dcsr_spgemm_batched_capture) with
+// its buffers sized once from clb_spgemm_batched_plan: enqueue() may be
+// recorded into a Graph; result() synchronises and returns each pair's C.
+class CapturedBatch {
+public:
+    CapturedBatch(Controls &c, const std::vector<std::pair<matrix_dcsr, matrix_dcsr>> &pairs,
+                  const clb_spgemm_tuning *tuning = nullptr)
+        : c_(c), pairs_(pairs) {
+        for (const auto &p : pairs) {
+            va_.push_back(p.first.view());
+            vb_.push_back(p.second.view());
+        }
+        if (tuning) {
+            tuning_ = *tuning;
+            has_tuning_ = true;
+        }
+        details::check(clb_spgemm_batched_plan(c.get(), (uint32_t)pairs.size(), va_.data(), vb_.data(), &rows_, &slots_));
+        rpt_ = alloc(c, (rows_ + 1) * 8);
+        rws_ = alloc(c, std::max<uint64_t>(rows_, 1) * 4);
+        cls_ = alloc(c, std::max<uint64_t>(slots_, 1) * 4);
+        res_ = alloc(c, (2 + 2 * (pairs.size() + 1)) * 8);
+        flags_ = alloc(c, 4);
+    }
+    void enqueue() {
+        details::check(clb_dcsr_spgemm_batched_capture(
+            c_.get(), (uint32_t)pairs_.size(), va_.data(), vb_.data(), has_tuning_ ? &tuning_ : nullptr, slots_,
+            (uint64_t *)rpt_.get(), (uint32_t *)rws_.get(), (uint32_t *)cls_.get(), slots_, (uint64_t *)res_.get(),
+            (uint32_t *)flags_.get()));
+    }
+    std::vector<matrix_dcsr_cpu> result() {
+        details::check(clb_controls_sync(c_.get()));
+        uint32_t flags = 0;
+        details::check(clb_memcpy_d2h(c_.get(), &flags, flags_.get(), 4));
+        if (flags) throw Exception("captured batch incomplete (capacity exceeded)", CLBOOL_RUN_KERNEL_FAILURE);
+        const size_t k = pairs_.size();
+        std::vector<uint64_t> r(2 + 2 * (k + 1));
+        details::check(clb_memcpy_d2h(c_.get(), r.data(), res_.get(), r.size() * 8));
+        std::vector<uint64_t> rpt(r[0] + 1);
+        std::vector<uint32_t> rows(r[0]), cols(r[1]);
+        details::check(clb_memcpy_d2h(c_.get(), rpt.data(), rpt_.get(), rpt.size() * 8));
+        if (r[0]) details::check(clb_memcpy_d2h(c_.get(), rows.data(), rws_.get(), rows.size() * 4));
+        if (r[1]) details::check(clb_memcpy_d2h(c_.get(), cols.data(), cls_.get(), cols.size() * 4));
+        std::vector<matrix_dcsr_cpu> out(k);
+        for (size_t i = 0; i < k; ++i) {
+            const uint64_t r0 = r[2 + i], r1 = r[3 + i], j0 = r[3 + k + i], j1 = r[4 + k + i];
+            for (uint64_t q = r0; q <= r1; ++q) out[i].rpt.push_back(rpt[q] - j0);
+            out[i].rows.assign(rows.begin() + r0, rows.begin() + r1);
+            out[i].cols.assign(cols.begin() + j0, cols.begin() + j1);
+        }
+        return out;
+    }
+
+private:
+    static Buffer alloc(Controls &c, size_t bytes) {
+        void *p = nullptr;
+        details::check(clb_malloc(c.get(), bytes, &p));
+        return Buffer(c, p, bytes);
+    }
+    Controls c_;
+    std::vector<std::pair<matrix_dcsr, matrix_dcsr>> pairs_;  // keeps the operands alive
+    std::vector<clb_dcsr> va_, vb_;
+    clb_spgemm_tuning tuning_{};
+    bool has_tuning_ = false;
+    uint64_t rows_ = 0, slots_ = 0;
+    Buffer rpt_, rws_, cls_, res_, flags_;
+};
 }  // namespace dcsr
 
 namespace coo {
