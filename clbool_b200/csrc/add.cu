@@ -253,6 +253,42 @@ __device__ __forceinline__ void warp_copy_seg(const uint32_t *__restrict__ x, ui
     for (; j < to; j += 32) dst[j] = __ldg(x + j);
 }
 
+// dst[j + base + (insertions at or before j)] = x[j] for j in [from, to):
+// ins[0, n) are the sorted insertion positions (an insertion at p goes
+// before x[p]).  Each lane keeps its own cursor into ins (its j only grow),
+// so the copy keeps eight loads in flight per lane across the insertions and
+// every store instruction writes 32 consecutive words.  (16-byte loads with
+// word stores measured no faster on scale-20 C + A.)
+__device__ __forceinline__ void warp_copy_shifted(const uint32_t *__restrict__ x, uint64_t from, uint64_t to,
+                                                  uint32_t *__restrict__ dst, const uint32_t *ins, uint32_t n,
+                                                  uint64_t base) {
+    uint32_t q = 0;
+    uint64_t nxt = n ? ins[0] : ~0ull;
+    uint64_t j = from + lane_id();
+    for (; j + 7 * 32 < to; j += 8 * 32) {
+        uint32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldg(x + j + u * 32);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const uint64_t jj = j + u * 32;
+            while (nxt <= jj) {
+                ++q;
+                nxt = q < n ? ins[q] : ~0ull;
+            }
+            dst[jj + base + q] = v[u];
+        }
+    }
+    for (; j < to; j += 32) {
+        const uint32_t v = __ldg(x + j);
+        while (nxt <= j) {
+            ++q;
+            nxt = q < n ? ins[q] : ~0ull;
+        }
+        dst[j + base + q] = v;
+    }
+}
+
 // MODE 0: out_cnt[r] = |X| + |Y| - |X and Y|.  MODE 1: row r of the sum at
 // cols + rpt[r].  One warp per row.
 // Rows whose shorter side has more than INS_LONG entries (the hub rows of a
@@ -264,6 +300,12 @@ constexpr uint32_t INS_MAX_CHUNKS = 4096;  // the CTA kernel's chunk table (long
 __device__ __forceinline__ bool ins_long_row(uint64_t ny) {
     return ny > INS_LONG && ny <= (uint64_t)INS_MAX_CHUNKS * 32;
 }
+// Rows with a short Y but an X too long for one warp to copy in good time
+// (power-law products: a short A row can reach a C row of ~10^6 entries) are
+// filled by the CTA kernel too, X split into pieces over its warps.
+constexpr uint64_t INS_WIDE = 32768;
+constexpr uint64_t INS_PIECE = 8192;
+__device__ __forceinline__ bool ins_wide_row(uint64_t nx, uint64_t ny) { return ny <= INS_LONG && nx > INS_WIDE; }
 
 template <int MODE>
 __global__ void __launch_bounds__(256) csr_insert_kernel(CsrSide A, CsrSide B, uint64_t nrows,
@@ -272,14 +314,20 @@ __global__ void __launch_bounds__(256) csr_insert_kernel(CsrSide A, CsrSide B, u
                                                          uint32_t *__restrict__ cols,
                                                          uint32_t *__restrict__ long_rows,
                                                          uint32_t *__restrict__ n_long) {
+    __shared__ uint32_t s_ins[8][INS_LONG];  // per warp: the row's insertion positions
     const uint32_t lane = lane_id();
     const uint32_t ltmask = (1u << lane) - 1u;
+    uint32_t *const ins = s_ins[warp_id()];
     const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
     for (uint64_t r = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); r < nrows; r += nw) {
         const RowPair p = row_pair(A, B, r);
         if (ins_long_row(p.ny)) {
             if (MODE == 0 && lane == 0) long_rows[atomicAdd(n_long, 1u)] = (uint32_t)r;
             continue;
+        }
+        if (ins_wide_row(p.nx, p.ny)) {
+            if (MODE == 1) continue;  // counted below, filled by the CTA kernel
+            if (lane == 0) long_rows[atomicAdd(n_long, 1u)] = (uint32_t)r;
         }
         uint32_t *const dst = MODE ? cols + rpt[r] : nullptr;
         if (p.ny == 0) {
@@ -290,7 +338,12 @@ __global__ void __launch_bounds__(256) csr_insert_kernel(CsrSide A, CsrSide B, u
             }
             continue;
         }
-        uint64_t lo = 0, copied = 0, shift = 0, dups = 0;
+        // Y of at most INS_LONG entries: insertion positions listed, then one
+        // shifted copy of X; longer Y (past the CTA kernel's table): X copied
+        // segment by segment between the insertions
+        const bool listed = p.ny <= INS_LONG;
+        uint64_t lo = 0, dups = 0, copied = 0;
+        uint32_t nins = 0;  // non-duplicate entries of Y so far
         for (uint64_t c0 = 0; c0 < p.ny; c0 += 32) {
             const uint64_t k = c0 + lane;
             const bool valid = k < p.ny;
@@ -301,29 +354,36 @@ __global__ void __launch_bounds__(256) csr_insert_kernel(CsrSide A, CsrSide B, u
             const uint32_t mins = __ballot_sync(0xFFFFFFFFu, valid && !dup);
             dups += __popc(mdup);
             if (MODE == 1) {
-                const uint32_t excl = __popc(mins & ltmask);
-                if (valid && !dup) dst[pos + shift + excl] = y;
-                // X up to each insertion point, shifted by the insertions before it
-                uint32_t m = mins;
-                uint32_t before = 0;
-                while (m) {
-                    const uint32_t l = __ffs(m) - 1;
-                    m &= m - 1;
-                    const uint64_t pl = __shfl_sync(0xFFFFFFFFu, pos, l);
-                    warp_copy_seg(p.x, copied, pl, dst + shift + before);
-                    copied = pl;
-                    ++before;
+                const uint32_t at = nins + __popc(mins & ltmask);
+                if (valid && !dup) {
+                    dst[pos + at] = y;
+                    if (listed) ins[at] = (uint32_t)pos;
                 }
-                shift += __popc(mins);
+                if (!listed) {
+                    uint32_t m = mins, before = 0;
+                    while (m) {
+                        const uint32_t l = __ffs(m) - 1;
+                        m &= m - 1;
+                        const uint64_t pl = __shfl_sync(0xFFFFFFFFu, pos, l);
+                        warp_copy_seg(p.x, copied, pl, dst + nins + before);
+                        copied = pl;
+                        ++before;
+                    }
+                }
             }
+            nins += __popc(mins);
             // the next chunk's entries are larger: search from the last position
             const uint32_t last = p.ny - c0 >= 32 ? 31u : (uint32_t)(p.ny - 1 - c0);
             lo = __shfl_sync(0xFFFFFFFFu, pos, last);
         }
         if (MODE == 0) {
             if (lane == 0) out_cnt[r] = p.nx + p.ny - dups;
+        } else if (listed) {
+            __syncwarp();
+            warp_copy_shifted(p.x, 0, p.nx, dst, ins, nins, 0);
+            __syncwarp();
         } else {
-            warp_copy_seg(p.x, copied, p.nx, dst + shift);
+            warp_copy_seg(p.x, copied, p.nx, dst + nins);
         }
     }
 }
@@ -343,12 +403,18 @@ __global__ void __launch_bounds__(256) csr_insert_long_kernel(CsrSide A, CsrSide
     __shared__ uint32_t s_start[INS_MAX_CHUNKS + 1];  // S_c
     __shared__ uint32_t s_nd[INS_MAX_CHUNKS];         // non-duplicate entries of chunk c, then their prefix
     __shared__ uint32_t scratch[33];
+    __shared__ uint32_t s_ins[NWARP][32];  // per warp: its chunk's insertion positions
+    __shared__ uint32_t s_all[INS_LONG];   // wide rows: all the row's insertion positions
+    __shared__ uint32_t s_wpos[INS_LONG];  // wide rows: each Y entry's position (~0 = duplicate)
     const uint32_t lane = lane_id(), w = warp_id();
     const uint32_t ltmask = (1u << lane) - 1u;
+    uint32_t *const ins = s_ins[w];
     const uint32_t nl = *n_long;
     for (uint32_t item = blockIdx.x; item < nl; item += gridDim.x) {
         const uint64_t r = long_rows[item];
         const RowPair p = row_pair(A, B, r);
+        const bool wide = ins_wide_row(p.nx, p.ny);
+        if (MODE == 0 && wide) continue;  // counted by the warp kernel (block-uniform)
         const uint32_t nch = (uint32_t)((p.ny + 31) / 32);
         // pass over the chunks: positions of the first entries and counts
         for (uint32_t c = w; c < nch; c += NWARP) {
@@ -362,6 +428,7 @@ __global__ void __launch_bounds__(256) csr_insert_long_kernel(CsrSide A, CsrSide
                 s_start[c] = c == 0 ? 0u : (uint32_t)pos;
                 s_nd[c] = __popc(mins);
             }
+            if (MODE == 1 && wide && valid) s_wpos[k] = dup ? 0xFFFFFFFFu : (uint32_t)pos;  // kept: no second search
         }
         if (threadIdx.x == 0) s_start[nch] = (uint32_t)p.nx;
         __syncthreads();
@@ -388,22 +455,43 @@ __global__ void __launch_bounds__(256) csr_insert_long_kernel(CsrSide A, CsrSide
             const bool valid = k < p.ny;
             const uint32_t y = valid ? __ldg(p.y + k) : 0xFFFFFFFFu;
             const uint64_t lo = s_start[c];
-            const uint64_t pos = valid ? lower_bound_from(p.x, lo, p.nx, y) : p.nx;
-            const bool dup = valid && pos < p.nx && __ldg(p.x + pos) == y;
+            uint64_t pos;
+            bool dup;
+            if (wide) {
+                const uint32_t wp = valid ? s_wpos[k] : 0xFFFFFFFFu;
+                dup = valid && wp == 0xFFFFFFFFu;
+                pos = valid && !dup ? (uint64_t)wp : p.nx;
+            } else {
+                pos = valid ? lower_bound_from(p.x, lo, p.nx, y) : p.nx;
+                dup = valid && pos < p.nx && __ldg(p.x + pos) == y;
+            }
             const uint32_t mins = __ballot_sync(0xFFFFFFFFu, valid && !dup);
             const uint64_t shift = s_nd[c];
-            if (valid && !dup) dst[pos + shift + __popc(mins & ltmask)] = y;
-            uint64_t copied = lo;
-            uint32_t m = mins, before = 0;
-            while (m) {
-                const uint32_t l = __ffs(m) - 1;
-                m &= m - 1;
-                const uint64_t pl = __shfl_sync(0xFFFFFFFFu, pos, l);
-                warp_copy_seg(p.x, copied, pl, dst + shift + before);
-                copied = pl;
-                ++before;
+            const uint32_t at = __popc(mins & ltmask);
+            if (valid && !dup) {
+                dst[pos + shift + at] = y;
+                if (wide) s_all[shift + at] = (uint32_t)pos;
+                else ins[at] = (uint32_t)pos;
             }
-            warp_copy_seg(p.x, copied, s_start[c + 1], dst + shift + before);
+            if (!wide) {
+                __syncwarp();
+                warp_copy_shifted(p.x, lo, s_start[c + 1], dst, ins, __popc(mins), shift);
+                __syncwarp();
+            }
+        }
+        if (wide) {
+            // X in pieces over the warps, each starting its cursor at the
+            // first insertion at or after the piece
+            __syncthreads();
+            const uint32_t nins = total;
+            for (uint64_t j0 = (uint64_t)w * INS_PIECE; j0 < p.nx; j0 += NWARP * INS_PIECE) {
+                uint32_t q0 = 0, hi = nins;  // first insertion with position >= j0
+                while (q0 < hi) {
+                    const uint32_t m = (q0 + hi) / 2;
+                    if (s_all[m] < j0) q0 = m + 1; else hi = m;
+                }
+                warp_copy_shifted(p.x, j0, min(j0 + INS_PIECE, p.nx), dst, s_all + q0, nins - q0, q0);
+            }
         }
         __syncthreads();
         }
@@ -548,7 +636,7 @@ int clb_csr_add(clb_controls *ctl, const clb_csr *a_, const clb_csr *b_, clb_csr
             CLB_TRY_CUDA(cudaMemsetAsync(nlong.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
             csr_insert_kernel<0><<<gw, 256, 0, ctl->stream>>>(A, B, a.nrows, rpt.ptr, nullptr, nullptr, lrows.ptr,
                                                               nlong.ptr);
-            csr_insert_long_kernel<0><<<ctl->sm_count * 2, 256, 0, ctl->stream>>>(A, B, lrows.ptr, nlong.ptr, rpt.ptr,
+            csr_insert_long_kernel<0><<<ctl->sm_count * 6, 256, 0, ctl->stream>>>(A, B, lrows.ptr, nlong.ptr, rpt.ptr,
                                                                                  nullptr, nullptr);
             CLB_CHECK_LAUNCH();
             CLB_RETURN_IF(scan_u64_inplace(ctl, rpt.ptr, a.nrows, tot.ptr));
@@ -560,7 +648,7 @@ int clb_csr_add(clb_controls *ctl, const clb_csr *a_, const clb_csr *b_, clb_csr
             CLB_RETURN_IF(cols.alloc(ctl, nnz));
             csr_insert_kernel<1><<<gw, 256, 0, ctl->stream>>>(A, B, a.nrows, nullptr, rpt.ptr, cols.ptr, nullptr,
                                                               nullptr);
-            csr_insert_long_kernel<1><<<ctl->sm_count * 2, 256, 0, ctl->stream>>>(A, B, lrows.ptr, nlong.ptr, nullptr,
+            csr_insert_long_kernel<1><<<ctl->sm_count * 6, 256, 0, ctl->stream>>>(A, B, lrows.ptr, nlong.ptr, nullptr,
                                                                                  rpt.ptr, cols.ptr);
             CLB_CHECK_LAUNCH();
             CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);

@@ -86,7 +86,8 @@ def test_addition_csr_insertion(controls):
     """One operand far sparser than the other (the insertion path): entries
     before, between (several at one gap) and after the long row's entries,
     duplicates, rows only one side has, a row where the sparse side is the
-    longer one, both operand orders."""
+    longer one, rows of 60000 entries (split over a CTA), both operand
+    orders."""
     import clbool_b200 as cb
     rng = np.random.default_rng(8)
     n, ncols = 3000, 100000
@@ -94,9 +95,10 @@ def test_addition_csr_insertion(controls):
     for r in range(n):
         if r % 7 == 3:
             continue  # empty on the long side
-        cols = np.sort(rng.choice(np.arange(10, ncols - 10), 300, replace=False))
+        wide = r >= n - 6  # rows longer than one warp's share: copied in pieces by a CTA
+        cols = np.sort(rng.choice(np.arange(10, ncols - 10), 60000 if wide else 300, replace=False))
         big_r.append(np.full(cols.size, r)); big_c.append(cols)
-        if r % 5 == 0:
+        if r % 5 == 0 or wide:
             k = int(rng.integers(1, 6))
             picks = [0, ncols - 1, int(cols[0]) + 1 if cols[1] > cols[0] + 2 else 1]
             picks += list(rng.choice(cols, k))                       # duplicates
