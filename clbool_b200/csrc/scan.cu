@@ -68,16 +68,25 @@ __global__ void __launch_bounds__(TS_NT) tiles_scan_kernel(uint64_t *__restrict_
     if (threadIdx.x == 0 && d_total) *d_total = carry;
 }
 
+// tile_offsets == nullptr: the whole input is one tile (n <= SCAN_TILE); the
+// scan then takes this one launch, which also writes the total.
 template <class TIn, class TOut>
 __global__ void __launch_bounds__(SCAN_NT) downsweep_kernel(const TIn *in, TOut *out, uint64_t n,
-                                                            const uint64_t *__restrict__ tile_offsets) {
+                                                            const uint64_t *__restrict__ tile_offsets,
+                                                            uint64_t *__restrict__ d_total = nullptr) {
     __shared__ uint64_t wsum[SCAN_WARPS];
     uint64_t tile_beg = (uint64_t)blockIdx.x * SCAN_TILE;
     uint64_t seg_beg = tile_beg + warp_id() * SCAN_SEG;
     uint64_t s = warp_segment_sum(in, seg_beg, n);
     if (lane_id() == 0) wsum[warp_id()] = s;
     __syncthreads();
-    uint64_t carry = tile_offsets[blockIdx.x];
+    if (!tile_offsets && d_total && threadIdx.x == 0) {
+        uint64_t t = 0;
+#pragma unroll
+        for (int w = 0; w < SCAN_WARPS; ++w) t += wsum[w];
+        *d_total = t;
+    }
+    uint64_t carry = tile_offsets ? tile_offsets[blockIdx.x] : 0;
     for (unsigned w = 0; w < warp_id(); ++w) carry += wsum[w];
     // The segment is read fully by warp_segment_sum before any write below,
     // and no other warp touches it, so `out` may alias `in`.
@@ -99,6 +108,13 @@ int scan_impl(clb_controls *ctl, const TIn *in, TOut *out, uint64_t n, uint64_t 
     }
     uint64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (ntiles > 0x7FFFFFFFull) return fail(CLB_NOT_SUPPORTED, "scan too long");
+    if (ntiles == 1) {  // one tile: one launch
+        ProfScope ps(ctl, "scan");
+        downsweep_kernel<TIn, TOut><<<1, SCAN_NT, 0, ctl->stream>>>(in, out, n, nullptr, d_total);
+        ctl->launches += 1;
+        CLB_CHECK_LAUNCH();
+        return CLB_SUCCESS;
+    }
     Temp<uint64_t> sums;
     CLB_RETURN_IF(sums.alloc(ctl, ntiles));
     ProfScope ps(ctl, "scan");
