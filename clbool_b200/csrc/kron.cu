@@ -33,29 +33,61 @@ __global__ void kron_rows_kernel(const uint64_t *__restrict__ arpt, const uint32
 
 constexpr int KR_NT = 256;
 
+// One warp per C row, rows taken with a grid stride: (ia, ib) advance by the
+// stride without dividing (dq, dr = stride / bnzr, stride % bnzr), and the
+// next row's pointers are loaded before the current row is written, so the
+// row-pointer latency overlaps the stores.  Rows whose B row has at most 128
+// entries keep it in registers (four per lane) and write one A entry's copy
+// per step; longer B rows loop over it; B rows shorter than 32 entries are
+// flattened over (ja, jb) so all lanes write.
 __global__ void __launch_bounds__(KR_NT) kron_cols_kernel(const uint64_t *__restrict__ arpt,
                                                           const uint32_t *__restrict__ acols, uint64_t anzr,
                                                           const uint64_t *__restrict__ brpt,
                                                           const uint32_t *__restrict__ bcols, uint64_t bnzr,
-                                                          uint64_t bncols, const uint64_t *__restrict__ crpt,
+                                                          uint64_t bnnz, uint64_t bncols, uint64_t dq, uint64_t dr,
                                                           uint32_t *__restrict__ ccols) {
     const uint64_t nzr = anzr * bnzr;
     const uint32_t lane = lane_id();
     const uint64_t nwarps = (uint64_t)gridDim.x * (KR_NT / 32);
-    for (uint64_t k = (uint64_t)blockIdx.x * (KR_NT / 32) + warp_id(); k < nzr; k += nwarps) {
-        const uint64_t ia = k / bnzr, ib = k - ia * bnzr;
-        const uint64_t a0 = arpt[ia], la = arpt[ia + 1] - a0;
-        const uint64_t b0 = brpt[ib], lb = brpt[ib + 1] - b0;
-        uint32_t *dst = ccols + crpt[k];
-        if (lb >= 32) {
+    uint64_t k = (uint64_t)blockIdx.x * (KR_NT / 32) + warp_id();
+    if (k >= nzr) return;
+    uint64_t ia = k / bnzr, ib = k - ia * bnzr;
+    uint64_t a0 = arpt[ia], a1 = arpt[ia + 1], b0 = brpt[ib], b1 = brpt[ib + 1];
+    while (k < nzr) {
+        // the next row's pointers, in flight while this row is written
+        const uint64_t kn = k + nwarps;
+        uint64_t ian = ia + dq, ibn = ib + dr;
+        if (ibn >= bnzr) {
+            ibn -= bnzr;
+            ++ian;
+        }
+        uint64_t na0 = 0, na1 = 0, nb0 = 0, nb1 = 0;
+        if (kn < nzr) {
+            na0 = __ldg(arpt + ian);
+            na1 = __ldg(arpt + ian + 1);
+            nb0 = __ldg(brpt + ibn);
+            nb1 = __ldg(brpt + ibn + 1);
+        }
+        const uint64_t la = a1 - a0, lb = b1 - b0;
+        uint32_t *dst = ccols + a0 * bnnz + la * b0;  // C's row pointer, closed form
+        if (lb > 128) {
             for (uint64_t ja = 0; ja < la; ++ja) {
                 const uint64_t base = (uint64_t)__ldg(acols + a0 + ja) * bncols;
                 for (uint64_t jb = lane; jb < lb; jb += 32)
                     dst[ja * lb + jb] = (uint32_t)(base + __ldg(bcols + b0 + jb));
             }
+        } else if (lb >= 32) {
+            uint32_t bv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) bv[u] = lane + 32u * u < lb ? __ldg(bcols + b0 + lane + 32u * u) : 0u;
+            for (uint64_t ja = 0; ja < la; ++ja) {
+                const uint64_t base = (uint64_t)__ldg(acols + a0 + ja) * bncols;
+                uint32_t *d = dst + ja * lb;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (lane + 32u * u < lb) d[lane + 32u * u] = (uint32_t)(base + bv[u]);
+            }
         } else if (lb) {
-            // short B rows: flatten (ja, jb) so all lanes stay busy; each lane
-            // steps its (ja, jb) by 32 positions without dividing
             const uint64_t n = la * lb;
             const uint32_t l = (uint32_t)lb, da = 32u / l, db = 32u % l;
             uint32_t ja = lane / l, jb = lane % l;
@@ -69,6 +101,13 @@ __global__ void __launch_bounds__(KR_NT) kron_cols_kernel(const uint64_t *__rest
                 }
             }
         }
+        k = kn;
+        ia = ian;
+        ib = ibn;
+        a0 = na0;
+        a1 = na1;
+        b0 = nb0;
+        b1 = nb1;
     }
 }
 
@@ -119,8 +158,10 @@ int clb_dcsr_kronecker(clb_controls *ctl, const clb_dcsr *a_, const clb_dcsr *b_
                                                                   b.nrows, rpt.ptr, rows.ptr);
     CLB_CHECK_LAUNCH();
     uint64_t warps = nzr, g2 = (warps + KR_NT / 32 - 1) / (KR_NT / 32), cap = (uint64_t)ctl->sm_count * 8;
-    kron_cols_kernel<<<(unsigned)(g2 > cap ? cap : g2), KR_NT, 0, ctl->stream>>>(a.rpt, a.cols, a.nzr, b.rpt, b.cols,
-                                                                                 b.nzr, b.ncols, rpt.ptr, cols.ptr);
+    const unsigned grid2 = (unsigned)(g2 > cap ? cap : g2);
+    const uint64_t stride = (uint64_t)grid2 * (KR_NT / 32);
+    kron_cols_kernel<<<grid2, KR_NT, 0, ctl->stream>>>(a.rpt, a.cols, a.nzr, b.rpt, b.cols, b.nzr, b.nnz, b.ncols,
+                                                        stride / b.nzr, stride % b.nzr, cols.ptr);
     CLB_CHECK_LAUNCH();
     CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
     c.nnz = nnz;
