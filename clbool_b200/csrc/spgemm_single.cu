@@ -266,10 +266,10 @@ int launch_esc_accumulators(clb_controls *ctl, const BinLists &bl, const AView &
         CLB_RETURN_IF((launch_cta_esc<4096, 512>(ctl, bl, BIN_H8K, a, b, o, work, rows(BIN_H8K), ctr.ptr + 0,
                                                  "cta_esc4096")));
     if (rows(BIN_H4K))
-        CLB_RETURN_IF((launch_cta_esc<2048, 256>(ctl, bl, BIN_H4K, a, b, o, work, rows(BIN_H4K), ctr.ptr + 1,
+        CLB_RETURN_IF((launch_cta_esc<2048, 128>(ctl, bl, BIN_H4K, a, b, o, work, rows(BIN_H4K), ctr.ptr + 1,
                                                  "cta_esc2048")));
     if (rows(BIN_H2K))
-        CLB_RETURN_IF((launch_cta_esc<1024, 256>(ctl, bl, BIN_H2K, a, b, o, work, rows(BIN_H2K), ctr.ptr + 2,
+        CLB_RETURN_IF((launch_cta_esc<1024, 128>(ctl, bl, BIN_H2K, a, b, o, work, rows(BIN_H2K), ctr.ptr + 2,
                                                  "cta_esc1024")));
     if (rows(BIN_H1K))
         CLB_RETURN_IF((launch_cta_esc<512, 128>(ctl, bl, BIN_H1K, a, b, o, work, rows(BIN_H1K), ctr.ptr + 3,
