@@ -975,6 +975,85 @@ __device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t n
     }
 }
 
+// One level of pairwise merges: segments [sb[2i], sb[2i+1]) and
+// [sb[2i+1], sb[2i+2]) of src (nseg segments, sb[nseg] = P) merge into
+// [sb[2i], sb[2i+2]) of dst, A side first on ties.  Each thread writes ITEMS
+// consecutive outputs: it finds their pair, splits the pair by a merge-path
+// search and merges sequentially.
+template <int NT, int ITEMS>
+__device__ __forceinline__ void merge_level(const uint32_t *src, uint32_t *dst, const uint32_t *sb, uint32_t nseg,
+                                            uint32_t P) {
+    const uint32_t npairs = (nseg + 1) / 2;
+    for (uint32_t p0 = threadIdx.x * ITEMS; p0 < P; p0 += NT * ITEMS) {
+        uint32_t p = p0;
+        const uint32_t pend = min(p0 + (uint32_t)ITEMS, P);
+        while (p < pend) {
+            uint32_t lo = 0, hi = npairs - 1;  // last pair starting at or before p
+            while (lo < hi) {
+                const uint32_t m = (lo + hi + 1) >> 1;
+                if (sb[2 * m] <= p) lo = m; else hi = m - 1;
+            }
+            const uint32_t a0 = sb[2 * lo], a1 = sb[min(2 * lo + 1, nseg)], b1 = sb[min(2 * lo + 2, nseg)];
+            const uint32_t la = a1 - a0, lb = b1 - a1, d = p - a0;
+            uint32_t x0 = d > lb ? d - lb : 0, x1 = min(d, la);
+            while (x0 < x1) {
+                const uint32_t m = (x0 + x1) >> 1;
+                if (src[a0 + m] <= src[a1 + d - 1 - m]) x0 = m + 1; else x1 = m;
+            }
+            uint32_t ia = x0, ib = d - x0;
+            const uint32_t stop = min(pend, b1);
+            for (; p < stop; ++p) {
+                const bool take_a = ib >= lb || (ia < la && src[a0 + ia] <= src[a1 + ib]);
+                dst[p] = take_a ? src[a0 + ia++] : src[a1 + ib++];
+            }
+        }
+    }
+}
+
+// Rows whose A entries are few merge their B rows (each sorted) instead of
+// sorting or bitmapping all products.
+constexpr uint32_t MERGE_SEGS = 64;
+
+// Sorts the products of A row i (at most MERGE_SEGS A entries), expanded into
+// buf0[0, P) in A-entry order, by pairwise merges of the B rows; returns the
+// buffer holding the result (buf0 or buf1).  sb: MERGE_SEGS + 1 words of
+// shared memory.  Ends with a block barrier.
+template <int NT, int ITEMS>
+__device__ __forceinline__ uint32_t *merge_row_segments(const AView &a, const BRows &b, uint32_t i, uint32_t P,
+                                                         uint32_t *buf0, uint32_t *buf1, uint32_t *sb) {
+    const uint64_t ja = a.rpt[i];
+    const uint32_t nseg0 = (uint32_t)(a.rpt[i + 1] - ja);
+    if (warp_id() == 0) {  // bounds = prefix of the B-row lengths (clamped to P)
+        const uint32_t lane = lane_id();
+        uint64_t bb;
+        const uint32_t l0 = lane < nseg0 ? b_row(b, __ldg(a.cols + ja + lane), bb) : 0u;
+        const uint32_t l1 = lane + 32 < nseg0 ? b_row(b, __ldg(a.cols + ja + lane + 32), bb) : 0u;
+        const uint32_t i0 = warp_inclusive_scan(l0);
+        const uint32_t t0 = __shfl_sync(0xFFFFFFFFu, i0, 31);
+        const uint32_t i1 = warp_inclusive_scan(l1);
+        if (lane < nseg0) sb[lane] = min(i0 - l0, P);
+        if (lane + 32 < nseg0) sb[lane + 32] = min(t0 + i1 - l1, P);
+        if (lane == 0) sb[nseg0] = P;
+    }
+    __syncthreads();
+    uint32_t nseg = nseg0;
+    uint32_t *src = buf0, *dst = buf1;
+    while (nseg > 1) {
+        merge_level<NT, ITEMS>(src, dst, sb, nseg, P);
+        const uint32_t nn = (nseg + 1) / 2;
+        const uint32_t nb = threadIdx.x < nn ? sb[2 * threadIdx.x] : 0u;
+        __syncthreads();
+        if (threadIdx.x < nn) sb[threadIdx.x] = nb;
+        if (threadIdx.x == 0) sb[nn] = P;
+        __syncthreads();
+        nseg = nn;
+        uint32_t *t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
 // Shared-memory layout of the bitmap kernels (32-bit words, bitmap of W).
 struct BitmapSmem {
     uint32_t *bm, *s_beg, *s_len, *s_upre, *s_list, *s_soff, *s_stage;

@@ -27,54 +27,17 @@ namespace clb {
 namespace {
 
 // ------------------------------------------------------------ CTA ESC ----
-// Rows with at most this many A entries merge their sorted B rows pairwise
+// Rows with at most MERGE_SEGS A entries merge their sorted B rows pairwise
 // instead of sorting all products: on R-MAT scale 20 the rows of 512..4096
 // products have a median of 1 to 3 such entries (a single B row is already
 // sorted and duplicate-free).
-constexpr uint32_t ESC_MERGE_SEGS = 64;
-
-// One level of pairwise merges: segments [sb[2i], sb[2i+1]) and
-// [sb[2i+1], sb[2i+2]) of src (nseg segments, sb[nseg] = P) merge into
-// [sb[2i], sb[2i+2]) of dst, A side first on ties.  Each thread writes ITEMS
-// consecutive outputs: it finds their pair, splits the pair by a merge-path
-// search and merges sequentially.
-template <int NT, int ITEMS>
-__device__ __forceinline__ void merge_level(const uint32_t *src, uint32_t *dst, const uint32_t *sb, uint32_t nseg,
-                                            uint32_t P) {
-    const uint32_t npairs = (nseg + 1) / 2;
-    for (uint32_t p0 = threadIdx.x * ITEMS; p0 < P; p0 += NT * ITEMS) {
-        uint32_t p = p0;
-        const uint32_t pend = min(p0 + (uint32_t)ITEMS, P);
-        while (p < pend) {
-            uint32_t lo = 0, hi = npairs - 1;  // last pair starting at or before p
-            while (lo < hi) {
-                const uint32_t m = (lo + hi + 1) >> 1;
-                if (sb[2 * m] <= p) lo = m; else hi = m - 1;
-            }
-            const uint32_t a0 = sb[2 * lo], a1 = sb[min(2 * lo + 1, nseg)], b1 = sb[min(2 * lo + 2, nseg)];
-            const uint32_t la = a1 - a0, lb = b1 - a1, d = p - a0;
-            uint32_t x0 = d > lb ? d - lb : 0, x1 = min(d, la);
-            while (x0 < x1) {
-                const uint32_t m = (x0 + x1) >> 1;
-                if (src[a0 + m] <= src[a1 + d - 1 - m]) x0 = m + 1; else x1 = m;
-            }
-            uint32_t ia = x0, ib = d - x0;
-            const uint32_t stop = min(pend, b1);
-            for (; p < stop; ++p) {
-                const bool take_a = ib >= lb || (ia < la && src[a0 + ia] <= src[a1 + ib]);
-                dst[p] = take_a ? src[a0 + ia++] : src[a1 + ib++];
-            }
-        }
-    }
-}
-
 template <int NP, int NT>
 __global__ void __launch_bounds__(NT) cta_esc_kernel(BinLists bl, int bin, AView a, BRows b, RowOut o,
                                                      const uint32_t *__restrict__ work, uint32_t *counter) {
     constexpr int SPT = NP / NT;
     __shared__ uint32_t keys[NP];
     __shared__ uint32_t keys2[NP];                   // merge ping-pong buffer
-    __shared__ uint32_t s_sb[ESC_MERGE_SEGS + 1];    // segment bounds of the merges
+    __shared__ uint32_t s_sb[MERGE_SEGS + 1];        // segment bounds of the merges
     __shared__ uint32_t s_pre[HASH_ECH + 1];
     __shared__ uint32_t s_beg[HASH_ECH];
     __shared__ uint32_t scratch[33];
@@ -94,40 +57,10 @@ __global__ void __launch_bounds__(NT) cta_esc_kernel(BinLists bl, int bin, AView
         balanced_products<NT, HASH_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t idx) {
             if (valid && idx < (uint32_t)NP) keys[idx] = c;
         });
-        const uint64_t ja = a.rpt[i];
-        const uint32_t nseg0 = (uint32_t)(a.rpt[i + 1] - ja);
         const uint32_t *sorted = keys;
-        if (nseg0 <= ESC_MERGE_SEGS) {
-            // few sorted B rows: pairwise merges (bounds = prefix of their lengths)
-            if (warp_id() == 0) {
-                const uint32_t lane = lane_id();
-                uint64_t bb;
-                const uint32_t l0 = lane < nseg0 ? b_row(b, __ldg(a.cols + ja + lane), bb) : 0u;
-                const uint32_t l1 = lane + 32 < nseg0 ? b_row(b, __ldg(a.cols + ja + lane + 32), bb) : 0u;
-                const uint32_t i0 = warp_inclusive_scan(l0);
-                const uint32_t t0 = __shfl_sync(0xFFFFFFFFu, i0, 31);
-                const uint32_t i1 = warp_inclusive_scan(l1);
-                if (lane < nseg0) s_sb[lane] = min(i0 - l0, P);  // clamped: never past the keys
-                if (lane + 32 < nseg0) s_sb[lane + 32] = min(t0 + i1 - l1, P);
-                if (lane == 0) s_sb[nseg0] = P;
-            }
-            __syncthreads();
-            uint32_t nseg = nseg0;
-            uint32_t *src = keys, *dst = keys2;
-            while (nseg > 1) {
-                merge_level<NT, NP / NT>(src, dst, s_sb, nseg, P);
-                const uint32_t nn = (nseg + 1) / 2;
-                const uint32_t nb = threadIdx.x < nn ? s_sb[2 * threadIdx.x] : 0u;
-                __syncthreads();
-                if (threadIdx.x < nn) s_sb[threadIdx.x] = nb;
-                if (threadIdx.x == 0) s_sb[nn] = P;
-                __syncthreads();
-                nseg = nn;
-                uint32_t *t = src;
-                src = dst;
-                dst = t;
-            }
-            sorted = src;
+        if (a.rpt[i + 1] - a.rpt[i] <= MERGE_SEGS) {
+            // few sorted B rows: pairwise merges
+            sorted = merge_row_segments<NT, NP / NT>(a, b, i, P, keys, keys2, s_sb);
         } else {
             for (uint32_t s = P + threadIdx.x; s < (uint32_t)NP; s += NT) keys[s] = EMPTY;
             __syncthreads();
