@@ -811,6 +811,10 @@ def run_rmat21(args) -> dict:
         srpt = (rpt[lo:hi + 1] - rpt[lo]).astype(np.uint64)
         A = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(srpt, rows[lo:hi], cols[int(rpt[lo]):int(rpt[hi])]), n)
         st = {}
+        # one untimed call first: the memory pool grows to the block's footprint
+        # and every kernel is loaded, as in the scale-20 warm-up steps
+        c = sizing.matrix_multiplication_learned(ctl, None, A, A_full, sizer)
+        del c
         ms = _event_ms(stream, lambda: sizing.matrix_multiplication_learned(ctl, None, A, A_full, sizer, stats=st), 1)
         for key in ("products", "nnz", "capacity", "spilled_rows", "fallback_rows"):
             tot[key] += int(st.get(key, 0))
