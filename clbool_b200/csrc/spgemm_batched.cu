@@ -542,7 +542,9 @@ int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, co
     uint32_t n = 0;
     for (const auto &t : cand) {
         double tms = 1e300;
-        for (int rep = 0; rep < 2 && rc == CLB_SUCCESS; ++rep) {  // first run warms up
+        // first run warms up; the best of three timed runs (one run alone let
+        // candidates within 1% of each other swap places from call to call)
+        for (int rep = 0; rep < 4 && rc == CLB_SUCCESS; ++rep) {
             cudaEventRecord(e0, ctl->stream);
             rc = clb_dcsr_spgemm_batched(ctl, count, a, b, out.data(), &t, nullptr);
             cudaEventRecord(e1, ctl->stream);
@@ -550,7 +552,7 @@ int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, co
             float f = 0.f;
             cudaEventElapsedTime(&f, e0, e1);
             for (uint32_t k = 0; k < count; ++k) clb_dcsr_release(ctl, &out[k]);
-            if (rep == 1) tms = f;
+            if (rep > 0 && f < tms) tms = f;
         }
         if (rc != CLB_SUCCESS) break;
         if (n < max_tried) {

@@ -318,7 +318,8 @@ CLB_API int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb
  * bitmap_min x bitmap_threads x warp_max x small_lanes; twice that with both
  * wide_rows settings when a pair has more than 2^20 columns) on the given
  * pairs and returns the
- * fastest in *best; tried/ms (optional, max_tried entries) receive each
+ * fastest in *best (each candidate: one warm-up call, then the best of three
+ * timed calls); tried/ms (optional, max_tried entries) receive each
  * candidate and its device time in ms, *n_tried their number. */
 CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                 clb_spgemm_tuning *best, clb_spgemm_tuning *tried, double *ms, uint32_t max_tried,
