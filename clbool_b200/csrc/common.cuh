@@ -243,7 +243,18 @@ struct BRows {
     const uint32_t *cols;
     uint64_t nzr;
     uint64_t nrows;
+    // B's rows as runs of one 32-bit bitmap word: (word, OR of the run's
+    // bits) pairs; wdense maps a row to its pairs like `dense` (null = absent)
+    const uint64_t *wdense = nullptr;
+    const uint2 *wpairs = nullptr;
 };
+
+// Pairs [beg, beg + n) of B row k (wdense present).
+__device__ __forceinline__ uint32_t b_words(const BRows &b, uint32_t k, uint64_t &beg) {
+    if (k >= b.nrows) { beg = 0; return 0; }
+    beg = __ldg(b.wdense + k);
+    return (uint32_t)(__ldg(b.wdense + k + 1) - beg);
+}
 
 __device__ __forceinline__ uint32_t b_row(const BRows &b, uint32_t k, uint64_t &beg) {
     if (b.dense) {

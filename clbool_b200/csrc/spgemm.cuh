@@ -8,6 +8,12 @@ namespace clb {
 int validate_spgemm(const clb_dcsr &A, const clb_dcsr &B);
 // Builds B's dense row map when worthwhile and fills the row view.
 int prepare_b(clb_controls *ctl, const clb_dcsr &B, Temp<uint64_t> &dense, BRows &b);
+// B's rows as word runs for the bitmap insertion: built when b has the dense
+// row map, B has at least B_WORDS_MIN_NNZ entries and (hinfo, rows per bin,
+// when given) some row is in a bitmap bin; otherwise b is left as it is.
+constexpr uint64_t B_WORDS_MIN_NNZ = 1ull << 16;
+int prepare_b_words(clb_controls *ctl, const clb_dcsr &B, const uint32_t *hinfo, Temp<uint64_t> &wdense,
+                    Temp<uint2> &wpairs, BRows &b);
 // work[i] = products of A row i; *d_total += their sum.
 int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t *work, uint64_t *d_total);
 // Histogram + scatter of the rows into accumulator bins.  The bound of

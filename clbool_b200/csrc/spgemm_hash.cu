@@ -103,6 +103,90 @@ int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t 
     return CLB_SUCCESS;
 }
 
+namespace {
+
+// flag[j] = 1 where entry j starts a word run: a new bitmap word (c >> 5)
+// or, set by the next kernel, the first entry of a row.
+__global__ void run_flags_kernel(const uint32_t *__restrict__ cols, uint64_t nnz, uint32_t *__restrict__ flag) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += (uint64_t)gridDim.x * blockDim.x)
+        flag[j] = (j == 0 || (__ldg(cols + j) >> 5) != (__ldg(cols + j - 1) >> 5)) ? 1u : 0u;
+}
+
+__global__ void row_start_flags_kernel(const uint64_t *__restrict__ rpt, uint64_t nzr, uint32_t *__restrict__ flag) {
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nzr; r += (uint64_t)gridDim.x * blockDim.x)
+        if (rpt[r] < rpt[r + 1]) flag[rpt[r]] = 1u;
+}
+
+// pairs[p] = (word, OR of the run's bits) for run p.  pos = exclusive scan of
+// the flags over nnz + 1 entries, so entry j is in run pos[j + 1] - 1.  The
+// bits are OR-ed within each warp over the lanes of one run (consecutive, the
+// rows being sorted), then one atomic per run and warp into zeroed pairs.
+__global__ void run_pairs_kernel(const uint32_t *__restrict__ cols, uint64_t nnz, const uint32_t *__restrict__ pos,
+                                 uint2 *__restrict__ pairs) {
+    const uint32_t lane = lane_id();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t j0 = (uint64_t)blockIdx.x * blockDim.x; j0 < nnz; j0 += stride) {
+        const uint64_t j = j0 + threadIdx.x;
+        const bool valid = j < nnz;
+        const uint32_t c = valid ? __ldg(cols + j) : 0u;
+        const uint32_t run = valid ? pos[j + 1] - 1u : 0xFFFFFFFFu;
+        const bool start = valid && pos[j + 1] != pos[j];
+        uint32_t m = valid ? 1u << (c & 31) : 0u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t om = __shfl_down_sync(0xFFFFFFFFu, m, d);
+            const uint32_t orun = __shfl_down_sync(0xFFFFFFFFu, run, d);
+            if (lane + d < 32 && orun == run) m |= om;
+        }
+        const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, run, 1);
+        if (valid && (lane == 0 || prev != run)) {
+            if (start) pairs[run].x = c >> 5;
+            atomicOr(&pairs[run].y, m);
+        }
+    }
+}
+
+// wdense[k] = first run of B row k (B's dense row map `dense`, nrows + 1).
+__global__ void run_rows_kernel(const uint64_t *__restrict__ dense, uint64_t nrows, uint64_t nnz,
+                                const uint32_t *__restrict__ pos, uint64_t *__restrict__ wdense) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= nrows; k += (uint64_t)gridDim.x * blockDim.x)
+        wdense[k] = pos[min(dense[k], nnz)];
+}
+
+}  // namespace
+
+int prepare_b_words(clb_controls *ctl, const clb_dcsr &B, const uint32_t *hinfo, Temp<uint64_t> &wdense,
+                    Temp<uint2> &wpairs, BRows &b) {
+    // the word form rides on the dense row map; it pays for its passes over B
+    // only when bitmap rows multiply a large B
+    if (!b.dense || B.nzr == 0 || B.nnz < B_WORDS_MIN_NNZ) return CLB_SUCCESS;
+    if (hinfo && hinfo[BIN_BMP_XL] + hinfo[BIN_BMP_L] + hinfo[BIN_BMP] == 0) return CLB_SUCCESS;
+    const uint64_t nnz = B.nnz;
+    Temp<uint32_t> pos;
+    CLB_RETURN_IF(pos.alloc(ctl, nnz + 1));
+    CLB_RETURN_IF(wpairs.alloc(ctl, nnz));  // runs <= entries: sized by the entries (no host read)
+    CLB_RETURN_IF(wdense.alloc(ctl, B.nrows + 1));
+    ProfScope ps(ctl, "b_word_runs");
+    const unsigned ge = persistent_grid(ctl, 8, ceil_div_u(nnz, 256));
+    run_flags_kernel<<<ge, 256, 0, ctl->stream>>>(B.cols, nnz, pos.ptr);
+    CLB_CHECK_LAUNCH();
+    row_start_flags_kernel<<<persistent_grid(ctl, 8, ceil_div_u(B.nzr, 256)), 256, 0, ctl->stream>>>(B.rpt, B.nzr,
+                                                                                                       pos.ptr);
+    CLB_CHECK_LAUNCH();
+    CLB_TRY_CUDA(cudaMemsetAsync(pos.ptr + nnz, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_RETURN_IF(scan_u32_inplace(ctl, pos.ptr, nnz + 1, nullptr));
+    CLB_TRY_CUDA(cudaMemsetAsync(wpairs.ptr, 0, nnz * sizeof(uint2), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    run_pairs_kernel<<<ge, 256, 0, ctl->stream>>>(B.cols, nnz, pos.ptr, wpairs.ptr);
+    CLB_CHECK_LAUNCH();
+    run_rows_kernel<<<persistent_grid(ctl, 8, ceil_div_u(B.nrows + 1, 256)), 256, 0, ctl->stream>>>(
+        b.dense, B.nrows, nnz, pos.ptr, wdense.ptr);
+    CLB_CHECK_LAUNCH();
+    ctl->launches += 4;
+    b.wdense = wdense.ptr;
+    b.wpairs = wpairs.ptr;
+    return CLB_SUCCESS;
+}
+
 int prepare_b(clb_controls *ctl, const clb_dcsr &B, Temp<uint64_t> &dense, BRows &b) {
     b.rpt = B.rpt;
     b.rows = B.rows;
@@ -170,6 +254,9 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     // rows per bin: only the bins with rows are launched, sized to them
     uint32_t hinfo[NUM_BINS];
     CLB_RETURN_IF(read_small(ctl, info.ptr, hinfo, sizeof(hinfo)));
+    Temp<uint64_t> wdense;
+    Temp<uint2> wpairs;
+    CLB_RETURN_IF(prepare_b_words(ctl, B, hinfo, wdense, wpairs, b));
 
     BinLists bl{list.ptr, info.ptr};
     RowOut sym{row_nnz.ptr, nullptr, nullptr, nullptr, nullptr, ctl->d_status};

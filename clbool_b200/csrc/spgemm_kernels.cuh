@@ -620,6 +620,7 @@ constexpr uint32_t BMP_STEP_WORDS = 128;      // emission step: 4 words per lane
 constexpr uint32_t BMP_MAX_STEPS = BMP_MAX_WORDS / BMP_STEP_WORDS;
 constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (columns)
 constexpr uint32_t BMP_FEW = 16;  // steps with at most this many outputs skip the balanced windows
+constexpr uint32_t BMP_DENSE = 1024;  // steps with at least this many outputs (1/4 of the bits) emit bit-parallel
 constexpr uint32_t BMP_SHORT = 64;            // products per A entry below which a row uses the per-product mapping
 
 // Words of the bitmap for `ncols` columns: a multiple of the emission step,
@@ -754,11 +755,18 @@ __device__ __forceinline__ void unit_products(const AView &a, const BRows &b, ui
 // covers a valid position, so it never leaves the 16-byte block of a valid
 // column.  Columns are clamped to the bitmap (memory safety on malformed
 // input).  Requires B.nnz <= 2^32 - 4096.
-template <int NT, int ECH, class SetBit>
+//
+// With B's word runs (b.wpairs: (word, bits) per run of entries in one
+// bitmap word, built once per call), the same sweeps run over the pairs and
+// `set_word(w, m)` issues one atomic per run instead of one per entry: on
+// R-MAT scale 20 the products fall in 1.69 times fewer words than entries.
+template <int NT, int ECH, class SetBit, class SetWord>
 __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b, uint32_t i, uint32_t shift,
-                                                  uint32_t maxcol, SetBit &&set_bit, uint32_t *s_beg, uint32_t *s_len,
-                                                  uint32_t *s_upre, uint32_t *scratch, uint32_t part = 0,
-                                                  uint32_t nparts = 1) {
+                                                  uint32_t maxcol, SetBit &&set_bit, SetWord &&set_word,
+                                                  uint32_t *s_beg, uint32_t *s_len, uint32_t *s_upre,
+                                                  uint32_t *scratch, uint32_t part = 0, uint32_t nparts = 1) {
+    const bool words = b.wpairs != nullptr;
+    const uint32_t maxword = maxcol >> 5;
     static_assert(ECH % NT == 0, "entry chunk must be a multiple of the block");
     constexpr int EPT = ECH / NT;
     constexpr int NW = NT / 32;
@@ -775,7 +783,8 @@ __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b
             units[k] = 0;
             if (e < n) {
                 uint64_t bb;
-                const uint32_t len = b_row(b, __ldg(a.cols + c0 + e), bb);
+                const uint32_t k_col = __ldg(a.cols + c0 + e);
+                const uint32_t len = words ? b_words(b, k_col, bb) : b_row(b, k_col, bb);
                 s_beg[e] = (uint32_t)bb;
                 s_len[e] = len;
                 if (len) units[k] = (uint32_t)(((bb + len - 1) >> shift) - (bb >> shift) + 1);
@@ -807,6 +816,24 @@ __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b
 #pragma unroll 1
             for (uint32_t k0 = ws; k0 < vhi; k0 += 256u) {
                 const uint32_t p0 = k0 + lane * 8u;
+                if (words) {
+                    // eight pairs: four 16-byte loads (p0 is a multiple of 8,
+                    // the pair array 16-byte aligned), each only when it holds
+                    // a pair of [vlo, vhi)
+                    const uint4 *p4 = reinterpret_cast<const uint4 *>(b.wpairs + p0);
+                    uint4 t[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        t[q] = (p0 + 2u * q + 2u > vlo && p0 + 2u * q < vhi) ? __ldg(p4 + q) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const uint32_t q = p0 + (uint32_t)j;
+                        const uint32_t wd = (j & 1) ? t[j >> 1].z : t[j >> 1].x;
+                        const uint32_t mk = (j & 1) ? t[j >> 1].w : t[j >> 1].y;
+                        if (q >= vlo && q < vhi) set_word(min(wd, maxword), mk);
+                    }
+                    continue;
+                }
                 uint32_t v[8];
                 if (vec) {
                     const uint4 *p4 = reinterpret_cast<const uint4 *>(b.cols + p0);
@@ -896,7 +923,8 @@ __device__ __forceinline__ uint32_t bitmap_list_steps(const uint4 *bm4, uint32_t
 // of its first output (shuffle search over the scan, then nth_set_bit) and
 // walks the bitmap from there into the warp's staging buffer, which the warp
 // copies out with coalesced stores.  A step with at most BMP_FEW outputs
-// skips the windows: each lane writes its own bits at its scan offset.  Cost
+// skips the windows: each lane writes its own bits at its scan offset.  A
+// step with at least BMP_DENSE outputs is emitted bit-parallel instead.  Cost
 // follows the non-empty steps and the output, not the bitmap width.  The
 // caller synchronises the block after.
 __device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t nlist, const uint32_t *s_list,
@@ -912,6 +940,31 @@ __device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t n
         const uint32_t pos = s_soff[g];
         const uint32_t T = s_soff[g + 1] - pos;
         const uint32_t q4 = st * 32u + lane;  // lane's uint4 of the step
+        if (T >= BMP_DENSE) {
+            // dense step: bit-parallel.  Lane l tests bit l of every word (one
+            // broadcast 16-byte load per four words); a word's outputs land at
+            // consecutive addresses, one store instruction per word.
+            const uint32_t lb = 1u << lane, lt = lb - 1u;
+            const uint4 *s4 = bm4 + st * 32u;
+            const uint32_t cb = colbase + st * (BMP_STEP_WORDS * 32u) + lane;
+            uint32_t off = pos;
+#pragma unroll 4
+            for (uint32_t q = 0; q < 32; ++q) {
+                const uint4 y = s4[q];
+                const uint32_t c = cb + q * 128u;
+                if (y.x & lb) out[off + __popc(y.x & lt)] = c;
+                off += __popc(y.x);
+                if (y.y & lb) out[off + __popc(y.y & lt)] = c + 32u;
+                off += __popc(y.y);
+                if (y.z & lb) out[off + __popc(y.z & lt)] = c + 64u;
+                off += __popc(y.z);
+                if (y.w & lb) out[off + __popc(y.w & lt)] = c + 96u;
+                off += __popc(y.w);
+            }
+            __syncwarp();  // every lane has read the step
+            bm4[q4] = make_uint4(0, 0, 0, 0);
+            continue;
+        }
         const uint4 x = bm4[q4];
         const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
         const uint32_t inc = warp_inclusive_scan(pc);
@@ -1129,6 +1182,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
             } else {
                 bitmap_insert_row<BMP_NT, BMP_ECH>(a, b, i, shift, (uint32_t)(chunk_cols - 1),
                                                    [&](uint32_t c) { atomicOr(bm + (c >> 5), 1u << (c & 31)); },
+                                                   [&](uint32_t wd, uint32_t mk) { atomicOr(bm + wd, mk); },
                                                    S.s_beg, S.s_len, S.s_upre, scratch);
             }
             if (!NUMERIC || overflowed) {
@@ -1233,22 +1287,23 @@ __global__ void __launch_bounds__(1024, 1) bitmap_cluster_kernel(BinLists bl, in
         const uint32_t shift = item < nheavy ? 9u : 8u;
         const bool short_b = o.row_products &&
                              (uint64_t)o.row_products[i] < (uint64_t)BMP_SHORT * (a.rpt[i + 1] - a.rpt[i]);
-        auto set_bit = [&](uint32_t c) {
-            const uint32_t q = c >> CLB_CHUNK_SHIFT;
+        auto set_bit_word = [&](uint32_t wd, uint32_t mk) {  // wd: word of the cluster's bitmap
+            const uint32_t q = wd >> (CLB_CHUNK_SHIFT - 5);
             uint32_t *sl = slices[0];  // select, not an indexed (local-memory) load
 #pragma unroll
             for (int k = 1; k < CL; ++k)
                 if (q == (uint32_t)k) sl = slices[k];
-            atomicOr(sl + ((c & ((1u << CLB_CHUNK_SHIFT) - 1)) >> 5), 1u << (c & 31));
+            atomicOr(sl + (wd & ((1u << (CLB_CHUNK_SHIFT - 5)) - 1)), mk);
         };
+        auto set_bit = [&](uint32_t c) { set_bit_word(c >> 5, 1u << (c & 31)); };
         if (short_b) {
             balanced_products<NT, BMP_ECH, 4>(a, b, i, S.s_upre, S.s_beg, scratch,
                                               [&](uint32_t c, bool valid, uint32_t) {
                 if (valid) set_bit(min(c, maxcol));
             }, rank, CL);
         } else {
-            bitmap_insert_row<NT, BMP_ECH>(a, b, i, shift, maxcol, set_bit, S.s_beg, S.s_len, S.s_upre, scratch, rank,
-                                           CL);
+            bitmap_insert_row<NT, BMP_ECH>(a, b, i, shift, maxcol, set_bit, set_bit_word, S.s_beg, S.s_len,
+                                           S.s_upre, scratch, rank, CL);
         }
         cluster.sync();  // every product's bit is set, in every slice
         uint32_t nlist = 0, ctot;

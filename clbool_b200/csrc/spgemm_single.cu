@@ -294,7 +294,7 @@ int launch_esc_accumulators(clb_controls *ctl, const BinLists &bl, const AView &
 // `esc` selects the ESC accumulators for rows of <= 4096 products and bins
 // those rows by products; otherwise rows are binned by capacity and use the
 // hash accumulators.
-int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
+int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b_in,
                        const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
                        clb_spgemm_stats *st, uint64_t arena_div, const Tuning &t) {
     const uint64_t n = A.nzr;
@@ -332,6 +332,10 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     const uint64_t nzr = h[0], slots = h[1];
     uint32_t hinfo[NUM_BINS];  // rows per bin: only bins with rows are launched
     CLB_RETURN_IF(read_small(ctl, info.ptr, hinfo, sizeof(hinfo)));
+    BRows b = b_in;
+    Temp<uint64_t> wdense;
+    Temp<uint2> wpairs;
+    CLB_RETURN_IF(prepare_b_words(ctl, B, hinfo, wdense, wpairs, b));
     if (st) {
         for (int k = 0; k < NUM_BINS; ++k) st->rows_per_bin[k] = hinfo[k];
         st->capacity = capacity;
