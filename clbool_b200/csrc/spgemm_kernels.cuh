@@ -1138,21 +1138,31 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
     const BitmapSmem S(smem, W);
     uint32_t *const bm = S.bm;
     __shared__ uint32_t scratch[33];
-    __shared__ uint32_t s_slot, s_next;
+    __shared__ uint32_t s_slot, s_row, s_next;
     __shared__ unsigned long long s_spill;
     uint32_t beg, cnt = 0, tmp;
     bin_range(bl, bin_lo, beg, tmp);
     for (int q = bin_lo; q <= bin_hi; ++q) cnt += bl.info[q];
     // rows of the bins above BIN_BMP (over 2^17 products) come first
     const uint32_t nheavy = bin_hi > bin_lo ? cnt - bl.info[bin_hi] : 0;
+    // Rows are claimed one ahead: the claim of the next row (a global atomic)
+    // and its row index are in flight while this row runs, and thread 0
+    // publishes both at the row's end (s_slot, s_row).
+    if (threadIdx.x == 0) {
+        const uint32_t it = atomicAdd(counter, 1u);
+        s_slot = it;
+        s_row = it < cnt ? bl.list[beg + it] : 0;
+    }
     for (uint32_t w = threadIdx.x; w < W; w += BMP_NT) bm[w] = 0;
     __syncthreads();
     uint4 *bm4 = reinterpret_cast<uint4 *>(bm);
     uint32_t *const stage = S.s_stage + warp_id() * BMP_STAGE;
     for (;;) {
-        const uint32_t item = next_item(counter, &s_slot);
+        const uint32_t item = s_slot;
         if (item >= cnt) break;
-        const uint32_t i = bl.list[beg + item];
+        const uint32_t i = s_row;
+        uint32_t nxt = 0;  // thread 0: the next row's claim, read at the row's end
+        if (threadIdx.x == 0) nxt = atomicAdd(counter, 1u);
         const uint32_t shift = item < nheavy ? 9u : 8u;
         // this row's columns (a batched pair can be narrower than the batch)
         const uint64_t rn = o.row_ncols ? (uint64_t)o.row_ncols[i] : ncols;
@@ -1185,6 +1195,8 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                                                    [&](uint32_t wd, uint32_t mk) { atomicOr(bm + wd, mk); },
                                                    S.s_beg, S.s_len, S.s_upre, scratch);
             }
+            if (threadIdx.x == 0 && c0 == 0 && nxt < cnt)
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(bl.list + beg + nxt));
             if (!NUMERIC || overflowed) {
                 total += bitmap_count_clear<BMP_NT>(bm4, Wr, scratch);
                 continue;
@@ -1227,7 +1239,10 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 if (overflowed) o.overflow[i] = 1;
                 else o.row_nnz[i] = (uint32_t)total;
             }
+            s_slot = nxt;
+            s_row = nxt < cnt ? bl.list[beg + nxt] : 0;
         }
+        __syncthreads();
     }
 }
 

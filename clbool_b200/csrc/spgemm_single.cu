@@ -41,13 +41,24 @@ __global__ void __launch_bounds__(NT) cta_esc_kernel(BinLists bl, int bin, AView
     __shared__ uint32_t s_pre[HASH_ECH + 1];
     __shared__ uint32_t s_beg[HASH_ECH];
     __shared__ uint32_t scratch[33];
-    __shared__ uint32_t s_slot;
+    __shared__ uint32_t s_slot, s_row;
     uint32_t beg, cnt;
     bin_range(bl, bin, beg, cnt);
+    // Rows are claimed one ahead: the next claim (a global atomic) and its
+    // row index are in flight while this row runs; thread 0 publishes them
+    // at the row's end.
+    if (threadIdx.x == 0) {
+        const uint32_t it = atomicAdd(counter, 1u);
+        s_slot = it;
+        s_row = it < cnt ? bl.list[beg + it] : 0;
+    }
+    __syncthreads();
     for (;;) {
-        const uint32_t item = next_item(counter, &s_slot);
+        const uint32_t item = s_slot;
         if (item >= cnt) break;
-        const uint32_t i = bl.list[beg + item];
+        const uint32_t i = s_row;
+        uint32_t nxt = 0;  // thread 0: the next row's claim, read after the expansion
+        if (threadIdx.x == 0) nxt = atomicAdd(counter, 1u);
         uint32_t P = work[i];
         if (P > (uint32_t)NP) {  // binning guarantees P <= NP
             if (threadIdx.x == 0) raise_status(o.status, DEV_BOUNDS);
@@ -57,6 +68,7 @@ __global__ void __launch_bounds__(NT) cta_esc_kernel(BinLists bl, int bin, AView
         balanced_products<NT, HASH_ECH, 4>(a, b, i, s_pre, s_beg, scratch, [&](uint32_t c, bool valid, uint32_t idx) {
             if (valid && idx < (uint32_t)NP) keys[idx] = c;
         });
+        if (threadIdx.x == 0 && nxt < cnt) asm volatile("prefetch.global.L1 [%0];" ::"l"(bl.list + beg + nxt));
         const uint32_t *sorted = keys;
         if (a.rpt[i + 1] - a.rpt[i] <= MERGE_SEGS) {
             // few sorted B rows: pairwise merges
@@ -81,13 +93,17 @@ __global__ void __launch_bounds__(NT) cta_esc_kernel(BinLists bl, int bin, AView
         uint32_t pos = block_exclusive_scan<uint32_t, NT>(mine, scratch, &nnz);
         if (o.row_cap && nnz > o.row_cap[i]) {
             if (threadIdx.x == 0) o.overflow[i] = 1;
-            continue;
-        }
-        uint32_t *dst = o.cols + o.row_off[i] + pos;
+        } else {
+            uint32_t *dst = o.cols + o.row_off[i] + pos;
 #pragma unroll
-        for (int k = 0; k < SPT; ++k)
-            if (flags & (1u << k)) *dst++ = v[k];
-        if (threadIdx.x == 0) o.row_nnz[i] = nnz;
+            for (int k = 0; k < SPT; ++k)
+                if (flags & (1u << k)) *dst++ = v[k];
+            if (threadIdx.x == 0) o.row_nnz[i] = nnz;
+        }
+        if (threadIdx.x == 0) {
+            s_slot = nxt;
+            s_row = nxt < cnt ? bl.list[beg + nxt] : 0;
+        }
         __syncthreads();
     }
 }
