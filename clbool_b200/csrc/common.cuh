@@ -104,6 +104,16 @@ struct Temp {
         if (!ptr) return fail(CLB_CREATE_BUFFER_ERROR, "device allocation of " + std::to_string(count * sizeof(T)) + " bytes failed");
         return CLB_SUCCESS;
     }
+    // Like alloc, but a failure is not an error of the call (the caller has
+    // another way); returns whether the buffer exists.
+    bool try_alloc(clb_controls *c, size_t count) {
+        reset();
+        ctl = c;
+        n = count;
+        if (count == 0) return true;
+        ptr = static_cast<T *>(dev_alloc(c, count * sizeof(T)));
+        return ptr != nullptr;
+    }
     T *release_ownership() {
         T *p = ptr;
         ptr = nullptr;

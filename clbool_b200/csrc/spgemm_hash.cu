@@ -162,10 +162,14 @@ int prepare_b_words(clb_controls *ctl, const clb_dcsr &B, const uint32_t *hinfo,
     if (!b.dense || B.nzr == 0 || B.nnz < B_WORDS_MIN_NNZ) return CLB_SUCCESS;
     if (hinfo && hinfo[BIN_BMP_XL] + hinfo[BIN_BMP_L] + hinfo[BIN_BMP] == 0) return CLB_SUCCESS;
     const uint64_t nnz = B.nnz;
+    // runs <= entries: the pairs are sized by the entries (no host read).
+    // Without room for them the bitmap rows insert B's entries instead.
     Temp<uint32_t> pos;
-    CLB_RETURN_IF(pos.alloc(ctl, nnz + 1));
-    CLB_RETURN_IF(wpairs.alloc(ctl, nnz));  // runs <= entries: sized by the entries (no host read)
-    CLB_RETURN_IF(wdense.alloc(ctl, B.nrows + 1));
+    if (!pos.try_alloc(ctl, nnz + 1) || !wpairs.try_alloc(ctl, nnz) || !wdense.try_alloc(ctl, B.nrows + 1)) {
+        wpairs.reset();
+        wdense.reset();
+        return CLB_SUCCESS;
+    }
     ProfScope ps(ctl, "b_word_runs");
     const unsigned ge = persistent_grid(ctl, 8, ceil_div_u(nnz, 256));
     run_flags_kernel<<<ge, 256, 0, ctl->stream>>>(B.cols, nnz, pos.ptr);
