@@ -29,6 +29,11 @@ int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, con
 // C.rpt/C.rows from the row flags' exclusive scan (pos) and the row offsets.
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
                     const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz);
+// Deferred bitmap rows (RowOut::defer; at most nmax of them): bitmaps from
+// their slots, columns to ccols + off[i].
+int launch_bitmap_expand(clb_controls *ctl, const uint32_t *list, const uint32_t *count, uint64_t nmax,
+                         const uint64_t *slot_off, const uint32_t *slots, const uint64_t *off,
+                         const uint32_t *row_ncols, uint64_t ncols, uint32_t *ccols);
 // Numeric accumulators without (hash_bins = false) the hash bins.
 int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
                                const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins,

@@ -137,6 +137,12 @@ struct RowOut {
     uint64_t arena_cap = 0;                        // entries
     const uint32_t *row_ncols = nullptr;           // columns of row i's product (batched pairs), or all
     const uint32_t *row_products = nullptr;        // products of row i (picks the bitmap insertion path)
+    // Single-pass forms: bitmap rows with at least as many columns as bitmap
+    // words store the bitmap in their slot instead (defer[i] = 1, listed in
+    // defer_list[0, *defer_count)); bitmap_expand_kernel writes their columns.
+    uint32_t *defer = nullptr;
+    uint32_t *defer_list = nullptr;
+    uint32_t *defer_count = nullptr;
 };
 
 // ------------------------------------------------------------- warp ESC ----
@@ -1204,6 +1210,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
             uint32_t nlist;
             const uint32_t ctot = bitmap_list_steps<BMP_NT>(bm4, nsteps, S.s_list, S.s_soff, &s_next, scratch, nlist);
             uint32_t *out = o.cols + out_base + total;
+            bool in_slot = true;
             if (o.row_cap && total + ctot > o.row_cap[i]) {
                 // single-pass forms: the row does not fit its slot.  A
                 // single-chunk row knows its exact count now: reserve it in
@@ -1226,7 +1233,26 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                     continue;
                 }
                 out = o.arena + s_spill;
+                in_slot = false;
                 if (threadIdx.x == 0) o.spill[i] = s_spill;
+            }
+            if (!MULTI && o.defer && in_slot && ctot >= Wr) {
+                // the bitmap is no larger than the row's columns: it is
+                // stored in the row's slot (16-byte aligned, >= ctot >= Wr
+                // words) and expanded straight into C once C's offsets are
+                // known, so these columns skip the slot-to-C compaction
+                uint4 *dst = reinterpret_cast<uint4 *>(out);
+                for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) {
+                    dst[w4] = bm4[w4];
+                    bm4[w4] = make_uint4(0, 0, 0, 0);
+                }
+                if (threadIdx.x == 0) {
+                    o.defer[i] = 1;
+                    o.defer_list[atomicAdd(o.defer_count, 1u)] = i;
+                }
+                total += ctot;
+                __syncthreads();
+                continue;
             }
             bitmap_emit(bm, bm4, nlist, S.s_list, S.s_soff, &s_next, stage, out, (uint32_t)c0);
             total += ctot;
@@ -1242,6 +1268,40 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
             s_slot = nxt;
             s_row = nxt < cnt ? bl.list[beg + nxt] : 0;
         }
+        __syncthreads();
+    }
+}
+
+// Deferred bitmap rows (RowOut::defer): each row's bitmap, stored in its
+// slot by bitmap_cta_kernel, is loaded back into shared memory and emitted
+// at the row's final offset in C, once the offsets are known.  One row per
+// CTA at a time, rows taken from `counter`.  (Emitting straight from the
+// bitmap in global memory, one warp per step and no block barriers, was
+// measured slower: the emission's bitmap walk waits on every load.)
+template <int BMP_NT>
+__global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_expand_kernel(
+    const uint32_t *__restrict__ list, const uint32_t *__restrict__ count, const uint64_t *__restrict__ slot_off,
+    const uint32_t *__restrict__ slots, const uint64_t *__restrict__ off, const uint32_t *__restrict__ row_ncols,
+    uint64_t ncols, uint32_t W, uint32_t *__restrict__ ccols, uint32_t *counter) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    const BitmapSmem S(smem, W);
+    uint32_t *const bm = S.bm;
+    uint4 *const bm4 = reinterpret_cast<uint4 *>(bm);
+    __shared__ uint32_t scratch[33];
+    __shared__ uint32_t s_slot, s_next;
+    uint32_t *const stage = S.s_stage + warp_id() * BMP_STAGE;
+    const uint32_t cnt = *count;
+    for (;;) {
+        const uint32_t item = next_item(counter, &s_slot);
+        if (item >= cnt) break;
+        const uint32_t i = list[item];
+        const uint32_t Wr = bitmap_words(row_ncols ? (uint64_t)row_ncols[i] : ncols);
+        const uint4 *src = reinterpret_cast<const uint4 *>(slots + slot_off[i]);
+        for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) bm4[w4] = src[w4];
+        __syncthreads();
+        uint32_t nlist;
+        bitmap_list_steps<BMP_NT>(bm4, Wr / BMP_STEP_WORDS, S.s_list, S.s_soff, &s_next, scratch, nlist);
+        bitmap_emit(bm, bm4, nlist, S.s_list, S.s_soff, &s_next, stage, ccols + off[i], 0u);
         __syncthreads();
     }
 }

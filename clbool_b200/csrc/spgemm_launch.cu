@@ -279,6 +279,26 @@ int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AVie
     return launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t, hc, hash_bins);
 }
 
+int launch_bitmap_expand(clb_controls *ctl, const uint32_t *list, const uint32_t *count, uint64_t nmax,
+                         const uint64_t *slot_off, const uint32_t *slots, const uint64_t *off,
+                         const uint32_t *row_ncols, uint64_t ncols, uint32_t *ccols) {
+    constexpr int NT = 1024;
+    const uint32_t W = bitmap_words(ncols);
+    const size_t smem = bitmap_smem_bytes(W, NT);
+    auto kern = bitmap_expand_kernel<NT>;
+    CLB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 CLB_RUN_KERNEL_FAILURE);
+    Temp<uint32_t> ctr;
+    CLB_RETURN_IF(ctr.alloc(ctl, 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(ctr.ptr, 0, sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    const unsigned grid = persistent_grid(ctl, occupancy(kern, NT, smem), nmax);
+    ProfScope ps(ctl, "bitmap_expand");
+    kern<<<grid, NT, smem, ctl->stream>>>(list, count, slot_off, slots, off, row_ncols, ncols, W, ccols, ctr.ptr);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
                     const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz) {
     unsigned grid = persistent_grid(ctl, 8, ceil_div_u(n, 256));

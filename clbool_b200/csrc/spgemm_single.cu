@@ -209,19 +209,19 @@ __device__ __forceinline__ void warp_copy_aligned_src(const uint32_t *__restrict
 }
 
 // C.cols <- every row from its slot (or the spill arena, both 16-byte
-// aligned: vector copy), or from C' for recomputed rows (scalar copy).  One
-// warp per row.
+// aligned: vector copy), or from C' for recomputed rows (scalar copy),
+// except the deferred bitmap rows.  One warp per row.
 __global__ void compact_rows_kernel(const uint32_t *__restrict__ row_nnz, const uint64_t *__restrict__ slot_off,
                                     const uint64_t *__restrict__ off, const uint32_t *__restrict__ pre,
                                     const uint32_t *__restrict__ ovf, const uint32_t *__restrict__ pos,
                                     const uint64_t *__restrict__ sub_crpt, const uint32_t *__restrict__ sub_ccols,
                                     const uint64_t *__restrict__ spill, const uint32_t *__restrict__ arena,
-                                    uint64_t n, uint32_t *__restrict__ ccols) {
+                                    const uint32_t *__restrict__ defer, uint64_t n, uint32_t *__restrict__ ccols) {
     const uint32_t lane = lane_id();
     const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
     for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); i < n; i += nw) {
         const uint32_t len = row_nnz[i];
-        if (!len) continue;
+        if (!len || (defer && defer[i])) continue;  // deferred rows: bitmap_expand_kernel
         uint32_t *dst = ccols + off[i];
         if (ovf && ovf[i]) {
             const uint32_t *src = sub_ccols + sub_crpt[pos[i]];
@@ -363,6 +363,21 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     RowOut num{row_nnz.ptr, slot_off.ptr, cap, ovf.ptr, pre.ptr, ctl->d_status};
     num.row_ncols = t.row_ncols;
     num.row_products = work;
+    // bitmap rows denser than their bitmap keep the bitmap in their slot
+    // (without room for the row flags every row is emitted in place)
+    const uint64_t nbmp = (uint64_t)hinfo[BIN_BMP_XL] + hinfo[BIN_BMP_L] + hinfo[BIN_BMP];
+    Temp<uint32_t> defer, dlist, dcount;
+    const bool deferring =
+        nbmp && defer.try_alloc(ctl, n) && dlist.try_alloc(ctl, nbmp) && dcount.try_alloc(ctl, 1);
+    if (deferring) {
+        CLB_TRY_CUDA(cudaMemsetAsync(defer.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+        CLB_TRY_CUDA(cudaMemsetAsync(dcount.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+        num.defer = defer.ptr;
+        num.defer_list = dlist.ptr;
+        num.defer_count = dcount.ptr;
+    } else {
+        defer.reset();
+    }
     // spill arena for single-chunk bitmap rows over their capacity
     Temp<uint64_t> spill;
     Temp<uint32_t> arena;
@@ -457,11 +472,14 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
             ProfScope ps(ctl, "compact");
             compact_rows_kernel<<<grid_for(ctl, n * 32, 32), 256, 0, ctl->stream>>>(
                 row_nnz.ptr, slot_off.ptr, off.ptr, pre.ptr, novf ? ovf.ptr : nullptr, opos.ptr, sub_c.rpt,
-                sub_c.cols, spill.ptr, arena.ptr, n, c_cols.ptr);
+                sub_c.cols, spill.ptr, arena.ptr, defer.ptr, n, c_cols.ptr);
             ctl->launches += 1;
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) rc = fail(CLB_RUN_KERNEL_FAILURE, cudaGetErrorString(e));
         }
+        if (rc == CLB_SUCCESS && deferring)
+            rc = launch_bitmap_expand(ctl, dlist.ptr, dcount.ptr, nbmp, slot_off.ptr, pre.ptr, off.ptr, t.row_ncols,
+                                      B.ncols, c_cols.ptr);
     }
     if (rc == CLB_SUCCESS) rc = check_status(ctl, esc ? "matrix_multiplication" : "matrix_multiplication_learned");
     if (sub_c.rpt) clb_dcsr_release(ctl, &sub_c);
