@@ -138,8 +138,9 @@ struct RowOut {
     const uint32_t *row_ncols = nullptr;           // columns of row i's product (batched pairs), or all
     const uint32_t *row_products = nullptr;        // products of row i (picks the bitmap insertion path)
     // Single-pass forms: bitmap rows with at least as many columns as bitmap
-    // words store the bitmap in their slot instead (defer[i] = 1, listed in
-    // defer_list[0, *defer_count)); bitmap_expand_kernel writes their columns.
+    // words (bitmaps of at least BMP_DEFER_MIN_WORDS words) store the bitmap
+    // in their slot instead (defer[i] = 1, listed in defer_list[0,
+    // *defer_count)); bitmap_expand_kernel writes their columns.
     uint32_t *defer = nullptr;
     uint32_t *defer_list = nullptr;
     uint32_t *defer_count = nullptr;
@@ -625,6 +626,9 @@ constexpr int BMP_U = 8;                      // B-column loads in flight per la
 constexpr uint32_t BMP_STEP_WORDS = 128;      // emission step: 4 words per lane
 constexpr uint32_t BMP_MAX_STEPS = BMP_MAX_WORDS / BMP_STEP_WORDS;
 constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (columns)
+// Bitmaps at least this wide (2^18 columns) may be kept for bitmap_expand_kernel:
+// narrower ones cost more per row to reload than their compaction.
+constexpr uint32_t BMP_DEFER_MIN_WORDS = 8192;
 constexpr uint32_t BMP_FEW = 16;  // steps with at most this many outputs skip the balanced windows
 constexpr uint32_t BMP_DENSE = 1024;  // steps with at least this many outputs (1/4 of the bits) emit bit-parallel
 constexpr uint32_t BMP_SHORT = 64;            // products per A entry below which a row uses the per-product mapping
@@ -1236,7 +1240,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 in_slot = false;
                 if (threadIdx.x == 0) o.spill[i] = s_spill;
             }
-            if (!MULTI && o.defer && in_slot && ctot >= Wr) {
+            if (!MULTI && o.defer && in_slot && ctot >= Wr && Wr >= BMP_DEFER_MIN_WORDS) {
                 // the bitmap is no larger than the row's columns: it is
                 // stored in the row's slot (16-byte aligned, >= ctot >= Wr
                 // words) and expanded straight into C once C's offsets are
