@@ -2,8 +2,8 @@
 // of each row block of C overlapped with the product of the next block.
 //
 // No counterpart in the reference, where the product stays in device
-// buffers until matrix_dcsr_to_cpu copies it out after the call
-// (src/common/matrices_conversions.cpp:115-139).  For a large C the copy over
+// buffers until matrix_dcsr_from_gpu copies it out after the call
+// (src/common/matrices_conversions.cpp:121-140).  For a large C the copy over
 // PCIe outlasts the product (scale-20 R-MAT A*A: 38.9 GB of columns against
 // ~90 ms of kernels), so the product runs in row blocks of A balanced by
 // products: block j+1 is multiplied while block j travels on a second

@@ -100,20 +100,27 @@ typedef void *(*clb_alloc_fn)(void *ctx, size_t bytes, void *stream);
 typedef void (*clb_free_fn)(void *ctx, void *ptr, void *stream);
 
 /* ------------------------------------------------------------- runtime -- */
-/* Name of a status code; never NULL. */
+/* Name of a status code; never NULL.  Replaces operator<<(ostream&, Status)
+ * (src/core/error.hpp:154-180) over the same Status order (error.hpp:130-151). */
 CLB_API const char *clb_status_string(int status);
-/* Message of the last failing call on this host thread ("" if none). */
+/* Message of the last failing call on this host thread ("" if none): what
+ * clbool::Exception carried across the C++ surface (src/core/error.hpp:183-213). */
 CLB_API const char *clb_last_error(void);
-/* Library version: major*10000 + minor*100 + patch. */
+/* Library version: major*10000 + minor*100 + patch (no counterpart). */
 CLB_API int clb_version(void);
 
 /* Replaces create_controls(platform_id, device_id)
  * (src/common/env.cpp:7-36): one controls object per CUDA device. */
 CLB_API int clb_controls_create(int device, clb_controls **out);
+/* End of a Controls' lifetime (src/core/controls.hpp:12-28). */
 CLB_API int clb_controls_destroy(clb_controls *ctl);
-/* Run subsequent operations on `stream` (a cudaStream_t; NULL = own stream). */
+/* Run subsequent operations on `stream` (a cudaStream_t; NULL = own stream):
+ * the counterpart of Controls::queue / async_queue (src/core/controls.hpp:15-16);
+ * clb_controls_sync waits for it like queue.finish(). */
 CLB_API int clb_controls_set_stream(clb_controls *ctl, void *stream);
 CLB_API void *clb_controls_get_stream(clb_controls *ctl);
+/* Caller-supplied allocator for every device buffer (no counterpart: the
+ * reference allocates cl::Buffer objects itself). */
 CLB_API int clb_controls_set_allocator(clb_controls *ctl, clb_alloc_fn alloc, clb_free_fn release, void *ctx);
 CLB_API int clb_controls_sync(clb_controls *ctl);
 /* CUDA graphs over the controls' stream (no counterpart in the reference,
@@ -127,6 +134,7 @@ CLB_API int clb_graph_begin(clb_controls *ctl);
 CLB_API int clb_graph_end(clb_controls *ctl, void **graph);
 CLB_API int clb_graph_launch(clb_controls *ctl, void *graph);
 CLB_API int clb_graph_destroy(void *graph);
+/* Controls::device (src/core/controls.hpp:13) as a CUDA device ordinal. */
 CLB_API int clb_controls_device(clb_controls *ctl);
 
 /* Replaces show_devices() (src/common/env.cpp:38-54). */
@@ -147,17 +155,22 @@ typedef struct clb_profile_entry {
 CLB_API int clb_profile_enable(clb_controls *ctl, int on);
 CLB_API int clb_profile_read(clb_controls *ctl, clb_profile_entry *out, int capacity, int *count);
 
-/* Device memory through the controls' allocator. */
+/* Device memory through the controls' allocator (the reference creates
+ * cl::Buffer objects inside its matrix constructors, src/core/matrix_dcsr.hpp:28-43). */
 CLB_API int clb_malloc(clb_controls *ctl, size_t bytes, void **out);
 CLB_API int clb_free(clb_controls *ctl, void *ptr);
-/* Stream-ordered copies; synchronous on return. */
+/* Stream-ordered copies; synchronous on return (the buffer transfers of
+ * matrix_dcsr_from_cpu / matrix_dcsr_from_gpu, src/common/matrices_conversions.cpp:93-140). */
 CLB_API int clb_memcpy_h2d(clb_controls *ctl, void *dst, const void *src, size_t bytes);
 CLB_API int clb_memcpy_d2h(clb_controls *ctl, void *dst, const void *src, size_t bytes);
 CLB_API int clb_memcpy_d2d(clb_controls *ctl, void *dst, const void *src, size_t bytes);
-/* Pinned host memory for staging. */
+/* Pinned host memory for staging (no counterpart). */
 CLB_API int clb_host_alloc(size_t bytes, void **out);
 CLB_API int clb_host_free(void *ptr);
 
+/* A matrix's buffers are freed: the end of the refcounted cl::Buffer members of
+ * matrix_dcsr / matrix_coo / matrix_csr (src/core/matrix_dcsr.hpp:11-84,
+ * matrix_coo.hpp:12-83, matrix_csr.hpp:7-42). */
 CLB_API int clb_dcsr_release(clb_controls *ctl, clb_dcsr *m);
 CLB_API int clb_coo_release(clb_controls *ctl, clb_coo *m);
 CLB_API int clb_csr_release(clb_controls *ctl, clb_csr *m);
@@ -326,8 +339,8 @@ CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcs
                                 uint32_t *n_tried);
 
 /* C = A*B written into host memory (no counterpart in the reference, whose
- * product stays on the device until matrix_dcsr_to_cpu,
- * src/common/matrices_conversions.cpp:115-139).  A's stored rows are cut into
+ * product stays on the device until matrix_dcsr_from_gpu,
+ * src/common/matrices_conversions.cpp:121-140).  A's stored rows are cut into
  * `blocks` (1..64) ranges of about equal products; each block is one call of
  * the learned form (sizer != NULL, with margin_log2 / slack / tuning as in
  * clb_dcsr_spgemm_learned) or of clb_dcsr_spgemm_tuned (sizer == NULL), and
