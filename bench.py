@@ -104,11 +104,29 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def load_gen():
+    """clbool_b200/gen.py (numpy only) loaded by file path, so that the
+    reference arm generates its inputs without importing the package (whose
+    import loads the CUDA library)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("clbool_b200_gen", os.path.join(ROOT, "clbool_b200", "gen.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def rmat_a(scale: int):
-    from clbool_b200 import gen
+    gen = load_gen()
     r, c = gen.rmat(scale, seed=1)
     rpt, rows, cols = gen.to_dcsr(r, c)
     return 1 << scale, rpt, rows, cols
+
+
+def rmat_config(scale: int, nnz_a: int, products: int, world: int, row_fraction: float = 1.0) -> dict:
+    """The workload's identity, the same in both arms."""
+    return {"workload": f"rmat_s{scale}_AxA" + (f"_rows{row_fraction:g}" if row_fraction < 1.0 else ""),
+            "scale": scale, "edge_factor": 16, "abcd": [0.57, 0.19, 0.19, 0.05], "seed": 1,
+            "nnz_A": nnz_a, "products": products, "parallelism": f"rows{world}"}
 
 
 def shard_rows(rpt_work: np.ndarray, world: int, rank: int) -> tuple[int, int]:
@@ -333,12 +351,10 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic", "impl": "ours",
-        "config": {"workload": f"rmat_s{args.scale}_AxA_{args.form}" + (
-                       f"_rows{args.row_fraction:g}" if args.row_fraction < 1.0 else ""),
-                   "scale": args.scale, "edge_factor": 16,
-                   "abcd": [0.57, 0.19, 0.19, 0.05], "nnz_A": int(nnz_a), "products": int(products_all),
-                   "nnz_C": int(nnz_all), "form": args.form, "parallelism": f"rows{world}",
-                   "l2": "256 MiB device memset between steps, outside the step events; C (>30 GB) also exceeds L2"},
+        "config": rmat_config(args.scale, int(nnz_a), int(products_all), world=world,
+                              row_fraction=args.row_fraction),
+        "form": args.form, "nnz_C": int(nnz_all),
+        "l2": "256 MiB device memset between steps, outside the step events; C (>30 GB) also exceeds L2",
         "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
@@ -460,6 +476,47 @@ def cpu_baseline(n, rpt, rows, cols, work) -> dict:
             "sample": f"10% of A's stored rows (seed 7): {pick.size} rows, {p} products, {dt:.2f} s"}
 
 
+def c1_cpu(ra, ca, rb, cb_, n: int, products: int, gpu_product, gpu_sum, reps: int = 5) -> dict:
+    """CPU legs of the 4096^2 Poisson pair, the one configuration where the
+    reference's own CPU functions are tractable in full: its
+    coo_utils::matrix_multiplication_cpu (coo_utils.cpp:470-514) and
+    matrix_addition_cpu (coo_utils.cpp:315-324) on the whole pair, single
+    threaded as written, each result compared with the GPU's; plus the
+    oracle's multithreaded product (the port baseline)."""
+    import oracle as O
+    A = O.coo_to_dcsr(O.Coo(n, n, ra, ca))
+    B = O.coo_to_dcsr(O.Coo(n, n, rb, cb_))
+
+    def med(fn):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            r = fn()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts), r
+
+    threads = O.set_threads(os.cpu_count() or 1)
+    t, _ = med(lambda: O.spgemm(A, B))
+    res = {"cpu_baseline": {"value": products / t, "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": f"whole 4096^2 pair, median of {reps} calls ({t * 1e6:.0f} us)"}}
+    if O.ref_available():
+        R = O.Ref()
+        tm, Cr = med(lambda: R.spgemm(A, B))
+        ta, Sr = med(lambda: R.coo_add(O.Coo(n, n, ra, ca), O.Coo(n, n, rb, cb_)))
+        rpt, rows, cols = gpu_product
+        res["reference"] = {
+            "kind": "reference", "cores": 1, "calls": reps,
+            "spgemm": {"function": "coo_utils::matrix_multiplication_cpu", "us": tm * 1e6,
+                       "products_per_s": products / tm,
+                       "bit_exact_vs_gpu": bool(np.array_equal(np.asarray(Cr.rpt, np.uint64), rpt) and
+                                                np.array_equal(Cr.rows, rows) and np.array_equal(Cr.cols, cols))},
+            "coo_add": {"function": "coo_utils::matrix_addition_cpu", "us": ta * 1e6,
+                        "entries_per_s": Sr.rows.size / ta,
+                        "bit_exact_vs_gpu": bool(np.array_equal(Sr.rows, gpu_sum[0]) and
+                                                 np.array_equal(Sr.cols, gpu_sum[1]))}}
+    return res
+
+
 def run_reference(args) -> dict:
     """The reference's own CPU product (matrix_multiplication_cpu) on bounded
     samples of A's rows, one sample per host thread."""
@@ -470,9 +527,7 @@ def run_reference(args) -> dict:
     R = O.Ref()
     n, rpt, rows, cols = rmat_a(args.scale)
     B = O.Dcsr(n, n, rpt, rows, cols)
-    work = np.diff(rpt.astype(np.int64))  # placeholder until products are known
-    Bd = O.Dcsr(n, n, rpt, rows, cols)
-    prod = O.workload(Bd, Bd).astype(np.int64)
+    prod = O.workload(B, B).astype(np.int64)
     threads = os.cpu_count() or 1
     rng = np.random.default_rng(11)
     # The reference's product looks every A entry's column up by a linear
@@ -503,7 +558,8 @@ def run_reference(args) -> dict:
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ts / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"rmat_s{args.scale}_AxA_{args.form}", "scale": args.scale},
+            "config": rmat_config(args.scale, int(cols.size), int(prod.sum()), world=args.gpus),
+            "form": "coo_utils::matrix_multiplication_cpu",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{threads} threads x {per_thread_rows} random stored rows of A per step "
                                        f"(coo_utils::matrix_multiplication_cpu)"},
@@ -709,9 +765,13 @@ def run_small(args) -> dict:
     ms = _event_ms(stream, cap.enqueue, max(20, args.steps))
     out["capture_form_direct"] = {"us": ms * 1e3, "products_per_s": products / (ms / 1e3)}
     graph.close()
+    coo_sum = cb.coo.matrix_addition(ctl, None, Ac, Bc)
+    got_sum = (coo_sum.rows_gpu().to_host(coo_sum.nnz()), coo_sum.cols_gpu().to_host(coo_sum.nnz()))
+    cpu = c1_cpu(ra, ca, rb, cb_, n, int(products), (want.rpt, want.rows, want.cols), got_sum)
     return {"metric": METRIC, "workload": "poisson4096", "unit": UNIT, "n_gpus": 1, "data": "synthetic",
             "config": {"workload": "poisson4096_AxB", "n": n, "lambda": 8, "products": int(products),
-                       "nnz_A": int(ra.size), "nnz_B": int(rb.size)}, "calls": out}
+                       "nnz_A": int(ra.size), "nnz_B": int(rb.size)}, "calls": out,
+            "cpu_baseline": cpu["cpu_baseline"], "reference_cpu": cpu.get("reference")}
 
 
 def run_cfpq(args) -> dict:

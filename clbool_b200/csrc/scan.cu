@@ -157,14 +157,24 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_scratch_mutex;
 uint64_t *g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
 
-// Device address of g_scan_scratch on `device`, resolved once per device
-// with that device current.  In host code the array's name is only a host
-// stand-in, never a device address, so kernels must get this pointer.
-int scratch_address(int device, uint64_t **out) {
+// Device address of g_scan_scratch on `device`, which must be current.  In
+// host code the array's name is only a host stand-in, never a device
+// address, so kernels must get this pointer.  The first call on a device
+// looks it up (and loads the library's device code there if nothing has
+// yet); later calls look it up again whenever `s` is not being captured, so
+// a primary context that was torn down and re-created (cudaDeviceReset)
+// never leaves a stale address behind.  A call on a capturing stream takes
+// the address of the device's previous call.
+int scratch_address(int device, cudaStream_t s, uint64_t **out) {
     if (device < 0 || device >= NOALLOC_MAX_DEVICES)
         return fail(CLB_NOT_SUPPORTED, "device ordinal beyond the static scratch table");
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[device]) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cap = cudaStreamCaptureStatusActive;  // treat as captured: keep the known address
+    }
+    if (!g_scratch_addr[device] || cap == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_scan_scratch);
         if (e != cudaSuccess || !p)
@@ -175,6 +185,23 @@ int scratch_address(int device, uint64_t **out) {
     *out = g_scratch_addr[device];
     return CLB_SUCCESS;
 }
+
+// Makes the device that owns stream `s` current for the scope (the current
+// device for the legacy and per-thread default streams).
+struct StreamDevice {
+    int prev = -1, device = -1;
+    int enter(cudaStream_t s) {
+        CLB_TRY_CUDA(cudaGetDevice(&prev), CLB_RUN_KERNEL_FAILURE);
+        device = prev;
+        if (s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread)
+            CLB_TRY_CUDA(cudaStreamGetDevice(s, &device), CLB_INVALID_ARGUMENT);
+        if (device != prev) CLB_TRY_CUDA(cudaSetDevice(device), CLB_RUN_KERNEL_FAILURE);
+        return CLB_SUCCESS;
+    }
+    ~StreamDevice() {
+        if (prev >= 0 && device != prev) cudaSetDevice(prev);
+    }
+};
 
 }  // namespace
 
@@ -190,14 +217,16 @@ int clb_prefix_sum_u32_noalloc(uint32_t *array, uint64_t n, uint64_t *d_total, v
         return fail(CLB_INVALID_ARGUMENT, "prefix sum of " + std::to_string(n) +
                                               " entries exceeds the static scratch limit of 2^28 entries");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // The scratch array is per device: take the one of the device that owns
+    // the stream, with that device current.
+    StreamDevice sd;
+    CLB_RETURN_IF(sd.enter(s));
     if (n == 0) {
         if (d_total) CLB_TRY_CUDA(cudaMemsetAsync(d_total, 0, sizeof(uint64_t), s), CLB_RUN_KERNEL_FAILURE);
         return CLB_SUCCESS;
     }
-    int device = 0;
-    CLB_TRY_CUDA(cudaGetDevice(&device), CLB_RUN_KERNEL_FAILURE);
     uint64_t *sums = nullptr;
-    CLB_RETURN_IF(scratch_address(device, &sums));
+    CLB_RETURN_IF(scratch_address(sd.device, s, &sums));
     // The tile sums are written in full by the first kernel before anything
     // reads them, so the array's leftovers from an earlier call need no
     // clearing.

@@ -188,13 +188,17 @@ CLB_API int clb_prefix_sum_u64(clb_controls *ctl, uint64_t *array, uint64_t n, u
  * synchronisation).  It allocates nothing: its scratch is a fixed 512 KiB
  * array inside the library, so n is limited to 2^28 entries (larger n is
  * rejected with CLB_INVALID_ARGUMENT).  It takes no controls object, launches
- * on `stream` (a cudaStream_t of the current device; NULL = legacy default
- * stream), does not synchronise, and writes the sum of the inputs to the
- * device pointer `d_total` when it is not NULL.  The first call on a device
- * looks up the scratch array's device address for that device; make that
- * first call before any stream capture.  Every call shares the one array, so
- * calls whose work overlaps on the GPU (different streams, or different host
- * threads on one device) race: serialise them. */
+ * on `stream` (a cudaStream_t; NULL = legacy default stream of the current
+ * device) with the stream's own device made current for the call, does not
+ * synchronise, and writes the sum of the inputs to the device pointer
+ * `d_total` when it is not NULL.  The first call on a device looks up the
+ * scratch array's device address for that device (loading the library's
+ * device code there if nothing has yet); make that first call before any
+ * stream capture.  Later calls look the address up again unless their stream
+ * is being captured, so the address stays right after cudaDeviceReset.
+ * Every call on one device shares the one array, so calls whose work
+ * overlaps on the GPU (different streams, or different host threads or
+ * controls on one device) race: serialise them. */
 CLB_API int clb_prefix_sum_u32_noalloc(uint32_t *array, uint64_t n, uint64_t *d_total, void *stream);
 
 /* fill_with (src/common/cl_operations.hpp:14, cl_operations.cpp:94-100). */

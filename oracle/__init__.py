@@ -54,9 +54,11 @@ def _p64(a):
 
 
 def build():
-    """Compile liboracle.so (and _ref when the reference sources exist)."""
+    """Compile liboracle.so (and _ref when CLBOOL_REFERENCE_SRC names the
+    reference's source tree)."""
     import subprocess
-    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    ref = os.environ.get("CLBOOL_REFERENCE_SRC", "")
+    subprocess.run(["make", "-s", "-C", HERE, "all"] + ([f"REF={ref}"] if ref else []), check=True)
 
 
 _lib = None

@@ -1,7 +1,7 @@
 """Generate tests/golden/golden.json from the reference's own CPU functions.
 
 Run in a checkout where the reference sources are available and
-``oracle/_ref/libclbool_ref.so`` has been built (``make -C oracle``):
+``oracle/_ref/libclbool_ref.so`` has been built (``make -C oracle REF=<reference tree>``):
 
     python tests/golden/make_golden.py
 
