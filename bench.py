@@ -618,11 +618,22 @@ def run_batch(args) -> dict:
             c = cb.dcsr.matrix_multiplication_hash(ctl, None, a, b)
             del c
 
+    from clbool_b200 import sizing
+    sizer_path = args.sizer_mixed if os.path.exists(args.sizer_mixed) else args.sizer
+    sizer = sizing.RowSizer.load(ctl, sizer_path)
+    st_l = {}
+
+    def learned():
+        outs = cb.dcsr.matrix_multiplication_batched_learned(ctl, pairs, sizer, stats=st_l)
+        del outs
+
     for _ in range(args.warmup):
         batched(best)()
+        learned()
         sequential()
     ms_best = _event_ms(stream, batched(best), args.steps)
     ms_default = _event_ms(stream, batched(default), args.steps)
+    ms_learned = _event_ms(stream, learned, args.steps)
     ms_seq = _event_ms(stream, sequential, max(1, args.steps // 2))
     batched(best)()
     # the host-sync-free batched form recorded once into a CUDA graph, replayed
@@ -643,6 +654,17 @@ def run_batch(args) -> dict:
     del ref
     ms_graph = _event_ms(stream, graph.launch, args.steps)
     graph.close()
+    # the learned-sized capture form, recorded once and replayed
+    capl = bt.CapturedBatch(ctl, pairs, tune=best, sizer=sizer)
+    graphl = bt.Graph(ctl, capl.enqueue)
+    for _ in range(max(3, args.warmup)):
+        graphl.launch()
+    gotl = capl.result()
+    exact_l = not capl.fell_back and all(
+        np.array_equal(x[2], y[2]) and np.array_equal(x[1], y[1]) and np.array_equal(x[0], y[0])
+        for x, y in zip(gotl, got))
+    ms_graph_l = _event_ms(stream, graphl.launch, args.steps)
+    graphl.close()
     return {"metric": METRIC, "workload": f"batch{args.pairs}_powerlaw", "value": products / (ms_best / 1e3),
             "unit": UNIT, "ms_per_step": ms_best, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
             "higher_is_better": True, "dtype": "u32", "data": "synthetic",
@@ -651,6 +673,13 @@ def run_batch(args) -> dict:
                        "row_lengths": "power law 2.1, mean 6, max 4096"},
             "autotuned": best.as_dict(), "default_ms": ms_default, "sequential_ms": ms_seq,
             "batched_over_sequential": ms_seq / ms_best,
+            "learned_batched": {"ms": ms_learned, "products_per_s": products / (ms_learned / 1e3),
+                                "over_two_pass_batched": ms_default / ms_learned,
+                                "capacity": st_l.get("capacity"), "spilled_rows": st_l.get("spilled_rows"),
+                                "fallback_rows": st_l.get("fallback_rows"),
+                                "graph_replay_ms": ms_graph_l, "graph_slot_capacity": capl.slot_capacity,
+                                "graph_bit_exact_vs_upper_bound_graph": exact_l,
+                                "sizer": os.path.basename(sizer_path)},
             "graph_replay": {"ms": ms_graph, "products_per_s": products / (ms_graph / 1e3),
                              "bit_exact_vs_batched": exact, "slot_capacity": cap.slot_capacity},
             "kernel_launches_per_batch": st.get("kernel_launches"),
@@ -795,11 +824,16 @@ def run_cfpq(args) -> dict:
     M = cfpq.union(ctl, [cfpq.identity(ctl, n)] + labels)
     best, _ = cb.dcsr.autotune(ctl, [(C2, M)])
     del C2
-    for method, tune in (("fused", None), ("fused_autotuned", best), ("batched", None)):
-        m = "batched" if method == "batched" else "fused"
-        cfpq.closure(ctl, labels, max_iters=2, method=m, tune=tune)  # warm-up
+    from clbool_b200 import sizing
+    sizer_path = args.sizer_mixed if os.path.exists(args.sizer_mixed) else args.sizer
+    sizer = sizing.RowSizer.load(ctl, sizer_path)
+    out["sizer"] = os.path.basename(sizer_path)
+    for method, tune, sz in (("fused", None, None), ("fused_autotuned", best, None), ("fused_learned", None, sizer),
+                             ("batched", None, None), ("batched_learned", None, sizer)):
+        m = "batched" if method.startswith("batched") else "fused"
+        cfpq.closure(ctl, labels, max_iters=2, method=m, tune=tune, sizer=sz)  # warm-up
         torch.cuda.synchronize()
-        C, hist = cfpq.closure(ctl, labels, max_iters=64, max_products=int(4e9), method=m, tune=tune)
+        C, hist = cfpq.closure(ctl, labels, max_iters=64, max_products=int(4e9), method=m, tune=tune, sizer=sz)
         out[method] = {"iterations": hist, "final_nnz": C.nnz(), "stop": hist[-1].get("stop"),
                        "products": sum(h["products"] for h in hist), "ms": sum(h["ms"] for h in hist)}
         if tune is not None:
@@ -845,6 +879,85 @@ def run_kron(args) -> dict:
             "roofline": {"bound": "hbm", "achieved": out_bytes / (ms / 1e3) / 1e9, "peak": peak, "peak_source": src,
                          "unit": "GB/s", "frac": out_bytes / (ms / 1e3) / 1e9 / peak,
                          "alg_bytes": out_bytes}}
+
+
+def run_primitives(args) -> dict:
+    """The primitives under the products, each on an input larger than L2
+    (126 MB) and timed with CUDA events on the library's stream (median of
+    `steps` calls, L2 flushed before each): COO addition of two R-MAT
+    scale-20 graphs (seeds 1 and 2, 2 x 16M entries, merge path), the COO
+    sort of the first graph's pairs shuffled (LSD radix), the prefix sum of
+    2^28 uint32 entries, and the DCSR -> CSR -> DCSR conversions of the first
+    graph.  Achieved GB/s are algorithmic bytes (each input read once, each
+    output written once) over the call's time."""
+    import ctypes
+
+    import torch
+
+    import clbool_b200 as cb
+    from clbool_b200 import gen
+    ctl = cb.create_controls(0, 0)
+    stream = torch.cuda.ExternalStream(ctl.stream, device="cuda:0")
+    n = 1 << 20
+    (ra, ca), (rb, cbb) = gen.rmat(20, seed=1), gen.rmat(20, seed=2)
+    Ac = cb.matrix_coo.from_host(ctl, ra, ca, n, n)
+    Bc = cb.matrix_coo.from_host(ctl, rb, cbb, n, n)
+    flush = cb.DeviceBuffer.empty(ctl, 256 << 20, np.uint8)
+    peak, src = peaks()
+    reps = max(3, args.steps)
+
+    def timed(fn):
+        out = []
+        for _ in range(reps):
+            cb.lib.clb_fill_u32(ctl.handle, ctypes.c_void_p(flush.ptr), (256 << 20) // 4, 0)
+            out.append(_event_ms(stream, fn, 1))
+        return statistics.median(out)
+
+    res = {}
+    S = cb.coo.matrix_addition(ctl, None, Ac, Bc)
+    nnz_s = S.nnz()
+    del S
+    ms = timed(lambda: cb.coo.matrix_addition(ctl, None, Ac, Bc))
+    alg = 8 * (ra.size + rb.size) + 8 * nnz_s
+    res["coo_add_rmat20_x2"] = {"ms": ms, "entries_per_s": nnz_s / (ms / 1e3), "alg_bytes": alg,
+                                "gbs": alg / (ms / 1e3) / 1e9, "nnz_a": int(ra.size), "nnz_b": int(rb.size),
+                                "nnz_c": int(nnz_s)}
+    perm = np.random.default_rng(9).permutation(ra.size)
+    pr, pc = ra[perm], ca[perm]
+    dr = cb.DeviceBuffer.from_host(ctl, pr, np.uint32)
+    dc = cb.DeviceBuffer.from_host(ctl, pc, np.uint32)
+
+    sort_ms = []
+    for _ in range(reps):
+        cb.lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(dr.ptr), pr.ctypes.data_as(ctypes.c_void_p), pr.nbytes)
+        cb.lib.clb_memcpy_h2d(ctl.handle, ctypes.c_void_p(dc.ptr), pc.ctypes.data_as(ctypes.c_void_p), pc.nbytes)
+        sort_ms.append(_event_ms(stream, lambda: cb.coo.sort_arrays(ctl, dr, dc, pr.size), 1))
+    ok = bool(np.array_equal(dr.to_host(), ra) and np.array_equal(dc.to_host(), ca))
+    ms = statistics.median(sort_ms)
+    alg = 16 * pr.size
+    res["coo_sort_rmat20_shuffled"] = {"ms": ms, "pairs_per_s": pr.size / (ms / 1e3), "alg_bytes": alg,
+                                       "gbs": alg / (ms / 1e3) / 1e9, "pairs": int(pr.size), "sorted_ok": ok}
+    m = 1 << 28
+    buf = cb.DeviceBuffer.empty(ctl, m, np.uint32)
+    cb.lib.clb_fill_u32(ctl.handle, ctypes.c_void_p(buf.ptr), m, 1)
+    tot = ctypes.c_uint64()
+    ms = timed(lambda: cb.lib.clb_prefix_sum_u32(ctl.handle, ctypes.c_void_p(buf.ptr), m, ctypes.byref(tot)))
+    res["prefix_sum_u32_2e28"] = {"ms": ms, "entries_per_s": m / (ms / 1e3), "alg_bytes": 8 * m,
+                                  "gbs": 8 * m / (ms / 1e3) / 1e9}
+    del buf
+    A = cb.coo_to_dcsr_shallow(ctl, Ac)
+    ms = timed(lambda: cb.dcsr_to_csr(ctl, A))
+    alg = 8 * (A.nzr() + 1) + 4 * A.nzr() + 8 * (n + 1)
+    res["dcsr_to_csr_rmat20"] = {"ms": ms, "alg_bytes": alg, "gbs": alg / (ms / 1e3) / 1e9}
+    Acsr = cb.dcsr_to_csr(ctl, A)
+    ms = timed(lambda: cb.csr_to_dcsr(ctl, Acsr))
+    res["csr_to_dcsr_rmat20"] = {"ms": ms, "alg_bytes": alg, "gbs": alg / (ms / 1e3) / 1e9}
+    for v in res.values():
+        if "gbs" in v:
+            v["frac"] = v["gbs"] / peak
+    return {"metric": "primitive throughput", "workload": "primitives_rmat20", "unit": "GB/s", "n_gpus": 1,
+            "data": "synthetic", "peak_gbs": peak, "peak_source": src, "calls": res,
+            "config": {"workload": "primitives_rmat20", "l2": "256 MiB memset before each timed call"}}
 
 
 def run_rmat21(args) -> dict:
@@ -906,20 +1019,23 @@ def main():
                     help="default: learned when the packaged predictor checkpoint exists, else two_pass")
     ap.add_argument("--sizer", default=os.path.join(ROOT, "clbool_b200", "sizer_rmat.npz"),
                     help="predictor checkpoint of the learned form")
+    ap.add_argument("--sizer-mixed", default=os.path.join(ROOT, "clbool_b200", "sizer_mixed.npz"),
+                    help="predictor checkpoint of the batch and closure workloads (trained on R-MAT, power-law, "
+                         "uniform and closure-step products); the R-MAT one when absent")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the two-pass form beside it")
     ap.add_argument("--row-fraction", type=float, default=1.0,
                     help="left operand = this seeded fraction of A's stored rows (profiling captures)")
     ap.add_argument("--ref-rows", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="rmat",
-                    choices=["rmat", "batch", "poisson4096", "cfpq", "kron", "rmat21", "rmat_add"],
+                    choices=["rmat", "batch", "poisson4096", "cfpq", "kron", "rmat21", "rmat_add", "primitives"],
                     help="rmat: the headline A*A; batch / poisson4096: secondary workloads (own JSON line)")
     ap.add_argument("--pairs", type=int, default=256)
     ap.add_argument("--blocks", type=int, default=4, help="row blocks of the scale-21 run")
     args = ap.parse_args()
     if args.workload != "rmat":
         fn = {"batch": run_batch, "poisson4096": run_small, "cfpq": run_cfpq, "kron": run_kron,
-              "rmat21": run_rmat21, "rmat_add": run_rmat_add}[args.workload]
+              "rmat21": run_rmat21, "rmat_add": run_rmat_add, "primitives": run_primitives}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
     if args.form is None:

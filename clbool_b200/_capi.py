@@ -99,6 +99,7 @@ _SIGS = {
     "clb_dcsr_spgemm_esc": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_stats)]),
     "clb_coo_add": (C.c_int, [vp, P(clb_coo), P(clb_coo), P(clb_coo)]),
     "clb_csr_add": (C.c_int, [vp, P(clb_csr), P(clb_csr), P(clb_csr)]),
+    "clb_csr_add_batched": (C.c_int, [vp, C.c_uint32, P(clb_csr), P(clb_csr), P(clb_csr)]),
     "clb_dcsr_kronecker": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr)]),
     "clb_dcsr_transpose": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr)]),
     "clb_dcsr_submatrix": (C.c_int, [vp, P(clb_dcsr), C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, P(clb_dcsr)]),
@@ -123,12 +124,20 @@ _SIGS = {
                                         P(clb_spgemm_stats)]),
     "clb_dcsr_spgemm_batched": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr),
                                           P(clb_spgemm_tuning), P(clb_spgemm_stats)]),
+    "clb_dcsr_spgemm_batched_learned": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr), vp,
+                                                  C.c_float, C.c_float, P(clb_spgemm_tuning),
+                                                  P(clb_spgemm_stats)]),
     "clb_spgemm_autotune": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_tuning),
                                       P(clb_spgemm_tuning), P(C.c_double), C.c_uint32, P(C.c_uint32)]),
     # host-sync-free batched product and CUDA graphs
     "clb_spgemm_batched_plan": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(C.c_uint64), P(C.c_uint64)]),
     "clb_dcsr_spgemm_batched_capture": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_tuning),
                                                   C.c_uint64, vp, vp, vp, C.c_uint64, vp, vp]),
+    "clb_spgemm_batched_plan_learned": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), vp, C.c_float,
+                                                  C.c_float, P(clb_spgemm_tuning), P(C.c_uint64), P(C.c_uint64)]),
+    "clb_dcsr_spgemm_batched_capture_learned": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), vp, C.c_float,
+                                                          C.c_float, P(clb_spgemm_tuning), C.c_uint64, C.c_uint64,
+                                                          vp, vp, vp, C.c_uint64, vp, vp]),
     "clb_dcsr_spgemm_to_host": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, C.c_float, C.c_float,
                                           P(clb_spgemm_tuning), C.c_uint32, vp, vp, vp, C.c_uint64, C.c_uint64,
                                           P(C.c_uint64), P(C.c_uint64), P(clb_spgemm_stats)]),

@@ -80,6 +80,29 @@ def matrix_multiplication_batched(controls: Controls, pairs, tune: clb_spgemm_tu
     return [matrix_dcsr.adopt(controls, out[k]) for k in range(n)]
 
 
+def matrix_multiplication_batched_learned(controls: Controls, pairs, sizer, margin_log2: float | None = None,
+                                          slack: float | None = None, tune: clb_spgemm_tuning | None = None,
+                                          stats: dict | None = None) -> list[matrix_dcsr]:
+    """[A_k * B_k for (A_k, B_k) in pairs] in one pass sized by `sizer` (a
+    sizing.RowSizer): the stacked pairs' bitmap rows get predicted slots, the
+    rest exact bounds; rows over their slot spill or are recomputed exactly,
+    so the result equals matrix_multiplication_batched's."""
+    from .sizing import DEFAULT_MARGIN_LOG2, DEFAULT_SLACK
+    n, A, B, _keep = _arrays(list(pairs))
+    if n == 0:
+        return []
+    out = (clb_dcsr * n)()
+    st = clb_spgemm_stats()
+    check(lib.clb_dcsr_spgemm_batched_learned(
+        controls.handle, n, A, B, out, sizer.handle,
+        float(DEFAULT_MARGIN_LOG2 if margin_log2 is None else margin_log2),
+        float(DEFAULT_SLACK if slack is None else slack), C.byref(tune) if tune else None, C.byref(st)),
+        "matrix_multiplication_batched_learned")
+    if stats is not None:
+        stats.update(st.as_dict())
+    return [matrix_dcsr.adopt(controls, out[k]) for k in range(n)]
+
+
 def autotune(controls: Controls, pairs, max_tried: int = 64):
     """(best tuning, [(tuning dict, ms), ...]) over the library's candidate tunings."""
     n, A, B, _keep = _arrays(list(pairs))
@@ -125,11 +148,20 @@ class Graph:
             pass
 
 
-def batched_plan(controls: Controls, pairs):
-    """(rows_need, slots_need) of CapturedBatch for the pairs' current contents."""
+def batched_plan(controls: Controls, pairs, sizer=None, margin_log2: float | None = None,
+                 slack: float | None = None, tune: clb_spgemm_tuning | None = None):
+    """(rows_need, slots_need) of CapturedBatch for the pairs' current
+    contents: upper-bound slots, or the learned slots when `sizer` is given."""
     n, A, B, _keep = _arrays(list(pairs))
     rows, slots = C.c_uint64(), C.c_uint64()
-    check(lib.clb_spgemm_batched_plan(controls.handle, n, A, B, C.byref(rows), C.byref(slots)), "batched_plan")
+    if sizer is None:
+        check(lib.clb_spgemm_batched_plan(controls.handle, n, A, B, C.byref(rows), C.byref(slots)), "batched_plan")
+    else:
+        from .sizing import DEFAULT_MARGIN_LOG2, DEFAULT_SLACK
+        check(lib.clb_spgemm_batched_plan_learned(
+            controls.handle, n, A, B, sizer.handle, float(DEFAULT_MARGIN_LOG2 if margin_log2 is None else margin_log2),
+            float(DEFAULT_SLACK if slack is None else slack), C.byref(tune) if tune else None, C.byref(rows),
+            C.byref(slots)), "batched_plan_learned")
     return int(rows.value), int(slots.value)
 
 
@@ -137,22 +169,40 @@ class CapturedBatch:
     """C_k = A_k * B_k for fixed pairs, into buffers sized once: ``enqueue()``
     issues the product without any host read (so it may run inside
     ``Graph(controls, batch.enqueue)``); ``result()`` synchronises and returns
-    the per-pair host arrays, raising when a capacity was too small."""
+    the per-pair host arrays, raising when a capacity was too small.
 
-    FLAG_NAMES = {1: "slot capacity", 2: "column capacity", 4: "device check"}
+    With a `sizer` (sizing.RowSizer) the slots are the learned ones
+    (clb_dcsr_spgemm_batched_capture_learned) plus a spill arena of
+    `arena_capacity` entries (default: a quarter of the slots, at least 2^20);
+    a row that outgrows both is reported in the flags, and ``result()`` then
+    recomputes the batch by the exact batched form (``fell_back`` is set)."""
+
+    FLAG_NAMES = {1: "slot capacity", 2: "column capacity", 4: "device check", 8: "learned slot and arena"}
+    EXACT_RETRY = 1 | 2 | 8  # flags a learned batch recovers from by the exact form
 
     def __init__(self, controls: Controls, pairs, slot_capacity: int | None = None,
-                 cols_capacity: int | None = None, tune: clb_spgemm_tuning | None = None):
+                 cols_capacity: int | None = None, tune: clb_spgemm_tuning | None = None, sizer=None,
+                 margin_log2: float | None = None, slack: float | None = None, arena_capacity: int | None = None):
+        from .sizing import DEFAULT_MARGIN_LOG2, DEFAULT_SLACK
         self.controls = controls
         self.pairs = list(pairs)
         self.count, self._A, self._B, _ = _arrays(self.pairs)
         if self.count == 0:
             raise ClBoolException(12, "CapturedBatch needs at least one pair")
-        rows, slots = batched_plan(controls, self.pairs)
+        self.sizer = sizer
+        self.margin_log2 = float(DEFAULT_MARGIN_LOG2 if margin_log2 is None else margin_log2)
+        self.slack = float(DEFAULT_SLACK if slack is None else slack)
+        rows, slots = batched_plan(controls, self.pairs, sizer, self.margin_log2, self.slack, tune)
         self.slot_capacity = int(slots if slot_capacity is None else slot_capacity)
-        self.cols_capacity = int(slots if cols_capacity is None else cols_capacity)
+        self.arena_capacity = 0
+        if sizer is not None:
+            self.arena_capacity = int(max(self.slot_capacity // 4, 1 << 20) if arena_capacity is None
+                                      else arena_capacity)
+        self.cols_capacity = int(self.slot_capacity + self.arena_capacity if cols_capacity is None
+                                 else cols_capacity)
         self.rows_capacity = rows
         self.tune = tune
+        self.fell_back = False
         self.rpt = DeviceBuffer.empty(controls, rows + 1, np.uint64)
         self.rows = DeviceBuffer.empty(controls, max(rows, 1), np.uint32)
         self.cols = DeviceBuffer.empty(controls, max(self.cols_capacity, 1), np.uint32)
@@ -160,15 +210,38 @@ class CapturedBatch:
         self.flags = DeviceBuffer.empty(controls, 1, np.uint32)
 
     def enqueue(self) -> None:
-        check(lib.clb_dcsr_spgemm_batched_capture(
-            self.controls.handle, self.count, self._A, self._B, C.byref(self.tune) if self.tune else None,
-            self.slot_capacity, C.c_void_p(self.rpt.ptr), C.c_void_p(self.rows.ptr), C.c_void_p(self.cols.ptr),
-            self.cols_capacity, C.c_void_p(self.res.ptr), C.c_void_p(self.flags.ptr)), "batched_capture")
+        tune = C.byref(self.tune) if self.tune else None
+        out = (C.c_void_p(self.rpt.ptr), C.c_void_p(self.rows.ptr), C.c_void_p(self.cols.ptr), self.cols_capacity,
+               C.c_void_p(self.res.ptr), C.c_void_p(self.flags.ptr))
+        if self.sizer is None:
+            check(lib.clb_dcsr_spgemm_batched_capture(self.controls.handle, self.count, self._A, self._B, tune,
+                                                      self.slot_capacity, *out), "batched_capture")
+        else:
+            check(lib.clb_dcsr_spgemm_batched_capture_learned(
+                self.controls.handle, self.count, self._A, self._B, self.sizer.handle, self.margin_log2, self.slack,
+                tune, self.slot_capacity, self.arena_capacity, *out), "batched_capture_learned")
+
+    def flags_now(self) -> int:
+        """The flag word of the last enqueued call (synchronises)."""
+        self.controls.sync()
+        return int(self.flags.to_host(1)[0])
 
     def result(self):
         """[(rpt u64, rows u32, cols u32) per pair] on the host."""
-        self.controls.sync()
-        flags = int(self.flags.to_host(1)[0])
+        flags = self.flags_now()
+        self.fell_back = False
+        if flags and self.sizer is not None and not flags & ~self.EXACT_RETRY:
+            # a learned slot (and the arena) was too small for some row: the
+            # exact batched form gives the same product
+            self.fell_back = True
+            out = []
+            for c in matrix_multiplication_batched(self.controls, self.pairs):
+                if c.nnz() == 0:
+                    out.append((np.zeros(1, np.uint64), np.zeros(0, np.uint32), np.zeros(0, np.uint32)))
+                    continue
+                out.append((c.rpt_gpu().to_host(c.nzr() + 1).astype(np.uint64), c.rows_gpu().to_host(c.nzr()),
+                            c.cols_gpu().to_host(c.nnz())))
+            return out
         if flags:
             what = ", ".join(v for k, v in self.FLAG_NAMES.items() if flags & k)
             raise ClBoolException(5, f"captured batch incomplete ({what} exceeded or failed)")

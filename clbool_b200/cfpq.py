@@ -7,11 +7,15 @@ of dcsr::matrix_multiplication and the additions).
 
 Two equivalent iteration methods:
   "batched": the k products C_t L_i as ONE batched call
-             (dcsr.matrix_multiplication_batched), then the union folded
-             with the CSR addition (csr::matrix_addition);
+             (dcsr.matrix_multiplication_batched, or the learned-sized
+             dcsr.matrix_multiplication_batched_learned when a sizer is
+             given), then the union C_t v P_1 v ... v P_k as a tree of
+             batched CSR additions (csr::matrix_addition over all pairs of a
+             level in one call: two calls for k = 3);
   "fused":   C_{t+1} = C_t M with M = I v L_1 v ... v L_k built once (the
              boolean semiring distributes: C v C L_1 v ... = C (I v L_1 v ...)),
-             i.e. one product per iteration and no union pass.
+             i.e. one product per iteration (learned-sized when a sizer is
+             given) and no union pass.
 On random graphs the closure tends to the
 dense n x n matrix, so the loop is bounded: it stops at a fixpoint, after
 `max_iters` iterations, or before an iteration whose products would exceed
@@ -24,17 +28,23 @@ import time
 
 import numpy as np
 
-from .batched import matrix_multiplication_batched, matrix_multiplication_tuned
+from .batched import matrix_multiplication_batched, matrix_multiplication_batched_learned, matrix_multiplication_tuned
 from .core import Controls, matrix_dcsr, matrix_dcsr_cpu
-from .ops import csr_matrix_addition, csr_to_dcsr, dcsr_to_csr, matrix_dcsr_from_cpu, workload
+from .ops import csr_matrix_addition_batched, csr_to_dcsr, dcsr_to_csr, matrix_dcsr_from_cpu, workload
 
 
 def union(controls: Controls, mats: list[matrix_dcsr]) -> matrix_dcsr:
-    """Boolean sum of DCSR matrices of one shape (CSR addition, folded)."""
-    acc = dcsr_to_csr(controls, mats[0])
-    for m in mats[1:]:
-        acc = csr_matrix_addition(controls, None, acc, dcsr_to_csr(controls, m))
-    return csr_to_dcsr(controls, acc)
+    """Boolean sum of DCSR matrices of one shape: every operand converted to
+    CSR once, then a tree of batched CSR additions (each level's pairs in
+    one call), converted back to DCSR."""
+    level = [dcsr_to_csr(controls, m) for m in mats]
+    while len(level) > 1:
+        pairs = [(level[i], level[i + 1]) for i in range(0, len(level) - 1, 2)]
+        nxt = csr_matrix_addition_batched(controls, pairs)
+        if len(level) % 2:
+            nxt.append(level[-1])
+        level = nxt
+    return csr_to_dcsr(controls, level[0])
 
 
 def identity(controls: Controls, n: int) -> matrix_dcsr:
@@ -43,9 +53,11 @@ def identity(controls: Controls, n: int) -> matrix_dcsr:
 
 
 def closure(controls: Controls, labels: list[matrix_dcsr], start: matrix_dcsr | None = None, max_iters: int = 64,
-            max_products: int | None = None, tune=None, method: str = "fused"):
+            max_products: int | None = None, tune=None, method: str = "fused", sizer=None):
     """(C, history): the bounded fixpoint and one dict per iteration
-    (iteration, nnz, products, ms, stop reason on the last)."""
+    (iteration, nnz, products, ms, stop reason on the last).  `sizer`
+    (sizing.RowSizer, optional): the products run in the learned-sized
+    single pass; the result does not depend on it."""
     if not labels:
         raise ValueError("closure needs at least one label matrix")
     if method not in ("fused", "batched"):
@@ -62,9 +74,16 @@ def closure(controls: Controls, labels: list[matrix_dcsr], start: matrix_dcsr | 
             break
         t0 = time.perf_counter()
         if M is not None:
-            Cn = matrix_multiplication_tuned(controls, None, C, M, tune)
+            if sizer is not None:
+                from .sizing import matrix_multiplication_learned
+                Cn = matrix_multiplication_learned(controls, None, C, M, sizer, tune=tune)
+            else:
+                Cn = matrix_multiplication_tuned(controls, None, C, M, tune)
         else:
-            prods = matrix_multiplication_batched(controls, [(C, L) for L in labels], tune=tune)
+            if sizer is not None:
+                prods = matrix_multiplication_batched_learned(controls, [(C, L) for L in labels], sizer, tune=tune)
+            else:
+                prods = matrix_multiplication_batched(controls, [(C, L) for L in labels], tune=tune)
             Cn = union(controls, [C] + prods)
         controls.sync()
         ms = (time.perf_counter() - t0) * 1e3

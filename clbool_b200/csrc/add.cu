@@ -20,6 +20,8 @@
 // range.  C's CSR row pointer is lenA + lenB - (duplicates of the row),
 // counted with one atomic per duplicate, then scanned.
 #include <algorithm>
+#include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -525,72 +527,9 @@ int copy_u32(clb_controls *ctl, const uint32_t *src, uint64_t n, uint32_t **dst)
     return CLB_SUCCESS;
 }
 
-}  // namespace
 
-}  // namespace clb
-
-using namespace clb;
-
-extern "C" {
-
-int clb_coo_add(clb_controls *ctl, const clb_coo *a_, const clb_coo *b_, clb_coo *out) {
-    if (!ctl || !a_ || !b_ || !out) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
-    const clb_coo a = *a_, b = *b_;
-    CLB_RETURN_IF(shape_check(a.nrows, a.ncols, b.nrows, b.ncols));
-    DeviceGuard g(ctl);
-    clb_coo c{};
-    c.nrows = a.nrows;
-    c.ncols = a.ncols;
-    if (a.nnz == 0 && b.nnz == 0) {
-        *out = c;
-        return CLB_SUCCESS;
-    }
-    if (a.nnz == 0 || b.nnz == 0) {  // copy of the filled operand (coo_matrix_addition.cpp:48-64)
-        const clb_coo &f = a.nnz ? a : b;
-        CLB_RETURN_IF(copy_u32(ctl, f.rows, f.nnz, &c.rows));
-        CLB_RETURN_IF(copy_u32(ctl, f.cols, f.nnz, &c.cols));
-        c.nnz = f.nnz;
-        CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
-        *out = c;
-        return CLB_SUCCESS;
-    }
-    ProfScope ps(ctl, "coo_add");
-    const CooSide A{a.rows, a.cols, a.nnz}, B{b.rows, b.cols, b.nnz};
-    const CsrSide none{nullptr, nullptr, 0};
-    const uint64_t total = a.nnz + b.nnz, ntiles = (total + MP_TILE - 1) / MP_TILE;
-    if (ntiles >= (1ull << 31)) return fail(CLB_NOT_SUPPORTED, "addition too large");
-    Temp<uint64_t> split, toff, tot;
-    Temp<uint32_t> tcnt;
-    CLB_RETURN_IF(split.alloc(ctl, ntiles + 1));
-    CLB_RETURN_IF(tcnt.alloc(ctl, ntiles));
-    CLB_RETURN_IF(toff.alloc(ctl, ntiles));
-    CLB_RETURN_IF(tot.alloc(ctl, 1));
-    coo_split_kernel<<<grid_for(ctl, ntiles + 1), 256, 0, ctl->stream>>>(A, B, ntiles, split.ptr);
-    merge_tile_kernel<false, 0><<<(unsigned)ntiles, MP_NT, 0, ctl->stream>>>(A, B, none, none, 0, split.ptr, nullptr,
-                                                                             tcnt.ptr, nullptr, nullptr, nullptr, nullptr);
-    CLB_CHECK_LAUNCH();
-    CLB_RETURN_IF(scan_u32_to_u64(ctl, tcnt.ptr, toff.ptr, ntiles, tot.ptr));
-    uint64_t nnz = 0;
-    CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &nnz, 1));
-    Temp<uint32_t> rows, cols;
-    CLB_RETURN_IF(rows.alloc(ctl, nnz));
-    CLB_RETURN_IF(cols.alloc(ctl, nnz));
-    merge_tile_kernel<false, 1><<<(unsigned)ntiles, MP_NT, 0, ctl->stream>>>(A, B, none, none, 0, split.ptr, nullptr,
-                                                                             nullptr, toff.ptr, nullptr, rows.ptr, cols.ptr);
-    CLB_CHECK_LAUNCH();
-    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
-    c.nnz = nnz;
-    c.rows = rows.release_ownership();
-    c.cols = cols.release_ownership();
-    *out = c;
-    return CLB_SUCCESS;
-}
-
-int clb_csr_add(clb_controls *ctl, const clb_csr *a_, const clb_csr *b_, clb_csr *out) {
-    if (!ctl || !a_ || !b_ || !out) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
-    const clb_csr a = *a_, b = *b_;
-    CLB_RETURN_IF(shape_check(a.nrows, a.ncols, b.nrows, b.ncols));
-    DeviceGuard g(ctl);
+// C = A v B (CSR, same shape checked by the caller, ctl's device current).
+int csr_add_impl(clb_controls *ctl, const clb_csr &a, const clb_csr &b, clb_csr *out) {
     clb_csr c{};
     c.nrows = a.nrows;
     c.ncols = a.ncols;
@@ -697,6 +636,261 @@ int clb_csr_add(clb_controls *ctl, const clb_csr *a_, const clb_csr *b_, clb_csr
     c.rpt = rpt.release_ownership();
     c.cols = cols.release_ownership();
     *out = c;
+    return CLB_SUCCESS;
+}
+
+// ------------------------------------------------------ batched addition --
+// Many independent additions C_k = A_k v B_k in one set of launches: the
+// pairs' rows are stacked (row pointers shifted by the entries before the
+// pair, columns copied unshifted: a row of the stack only ever meets the
+// other operand's row of the same pair), one addition runs over the stack,
+// and its rows are cut back into the pairs' results.
+struct AddDesc {
+    const uint64_t *arpt, *brpt;
+    const uint32_t *acols, *bcols;
+    uint64_t nrows, anz, bnz;
+    uint64_t row_off, aoff, boff;  // position in the stack
+};
+
+constexpr int ST_NT = 256;
+
+__global__ void __launch_bounds__(ST_NT) add_stack_kernel(const AddDesc *__restrict__ d, uint64_t *__restrict__ arpt,
+                                                          uint32_t *__restrict__ acols, uint64_t *__restrict__ brpt,
+                                                          uint32_t *__restrict__ bcols, uint64_t rows, uint64_t anz,
+                                                          uint64_t bnz) {
+    const AddDesc p = d[blockIdx.y];
+    const uint64_t stride = (uint64_t)gridDim.x * ST_NT;
+    const uint64_t t0 = (uint64_t)blockIdx.x * ST_NT + threadIdx.x;
+    const uint64_t a0 = p.arpt[0], b0 = p.brpt[0];
+    for (uint64_t r = t0; r < p.nrows; r += stride) {
+        arpt[p.row_off + r] = p.arpt[r] - a0 + p.aoff;
+        brpt[p.row_off + r] = p.brpt[r] - b0 + p.boff;
+    }
+    for (uint64_t j = t0; j < p.anz; j += stride) acols[p.aoff + j] = p.acols[a0 + j];
+    for (uint64_t j = t0; j < p.bnz; j += stride) bcols[p.boff + j] = p.bcols[b0 + j];
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        arpt[rows] = anz;
+        brpt[rows] = bnz;
+    }
+}
+
+struct AddOut {
+    uint64_t *rpt;
+    uint32_t *cols;
+    uint64_t nrows, row_off, c0, nnz;
+};
+
+// bounds[k] = C'.rpt[row_off of pair k] (k = count: the total).
+__global__ void add_bounds_kernel(const uint64_t *__restrict__ crpt, const uint64_t *__restrict__ row_off,
+                                  uint32_t count, uint64_t *__restrict__ bounds) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= count; k += gridDim.x * blockDim.x)
+        bounds[k] = crpt[row_off[k]];
+}
+
+__global__ void __launch_bounds__(ST_NT) add_split_kernel(const AddOut *__restrict__ d, const uint64_t *__restrict__ crpt,
+                                                          const uint32_t *__restrict__ ccols) {
+    const AddOut o = d[blockIdx.y];
+    if (!o.nnz) return;  // an empty sum has no arrays (its descriptor holds null pointers)
+    const uint64_t stride = (uint64_t)gridDim.x * ST_NT;
+    const uint64_t t0 = (uint64_t)blockIdx.x * ST_NT + threadIdx.x;
+    for (uint64_t r = t0; r <= o.nrows; r += stride) o.rpt[r] = crpt[o.row_off + r] - o.c0;
+    for (uint64_t j = t0; j < o.nnz; j += stride) o.cols[j] = ccols[o.c0 + j];
+}
+
+unsigned stack_blocks(uint64_t largest) {
+    const uint64_t gx = (largest + 4 * ST_NT - 1) / (4 * ST_NT);
+    return (unsigned)std::min<uint64_t>(std::max<uint64_t>(gx, 1), 65535);
+}
+
+}  // namespace
+
+}  // namespace clb
+
+using namespace clb;
+
+extern "C" {
+
+int clb_coo_add(clb_controls *ctl, const clb_coo *a_, const clb_coo *b_, clb_coo *out) {
+    if (!ctl || !a_ || !b_ || !out) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    const clb_coo a = *a_, b = *b_;
+    CLB_RETURN_IF(shape_check(a.nrows, a.ncols, b.nrows, b.ncols));
+    DeviceGuard g(ctl);
+    clb_coo c{};
+    c.nrows = a.nrows;
+    c.ncols = a.ncols;
+    if (a.nnz == 0 && b.nnz == 0) {
+        *out = c;
+        return CLB_SUCCESS;
+    }
+    if (a.nnz == 0 || b.nnz == 0) {  // copy of the filled operand (coo_matrix_addition.cpp:48-64)
+        const clb_coo &f = a.nnz ? a : b;
+        CLB_RETURN_IF(copy_u32(ctl, f.rows, f.nnz, &c.rows));
+        CLB_RETURN_IF(copy_u32(ctl, f.cols, f.nnz, &c.cols));
+        c.nnz = f.nnz;
+        CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+        *out = c;
+        return CLB_SUCCESS;
+    }
+    ProfScope ps(ctl, "coo_add");
+    const CooSide A{a.rows, a.cols, a.nnz}, B{b.rows, b.cols, b.nnz};
+    const CsrSide none{nullptr, nullptr, 0};
+    const uint64_t total = a.nnz + b.nnz, ntiles = (total + MP_TILE - 1) / MP_TILE;
+    if (ntiles >= (1ull << 31)) return fail(CLB_NOT_SUPPORTED, "addition too large");
+    Temp<uint64_t> split, toff, tot;
+    Temp<uint32_t> tcnt;
+    CLB_RETURN_IF(split.alloc(ctl, ntiles + 1));
+    CLB_RETURN_IF(tcnt.alloc(ctl, ntiles));
+    CLB_RETURN_IF(toff.alloc(ctl, ntiles));
+    CLB_RETURN_IF(tot.alloc(ctl, 1));
+    coo_split_kernel<<<grid_for(ctl, ntiles + 1), 256, 0, ctl->stream>>>(A, B, ntiles, split.ptr);
+    merge_tile_kernel<false, 0><<<(unsigned)ntiles, MP_NT, 0, ctl->stream>>>(A, B, none, none, 0, split.ptr, nullptr,
+                                                                             tcnt.ptr, nullptr, nullptr, nullptr, nullptr);
+    CLB_CHECK_LAUNCH();
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, tcnt.ptr, toff.ptr, ntiles, tot.ptr));
+    uint64_t nnz = 0;
+    CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &nnz, 1));
+    Temp<uint32_t> rows, cols;
+    CLB_RETURN_IF(rows.alloc(ctl, nnz));
+    CLB_RETURN_IF(cols.alloc(ctl, nnz));
+    merge_tile_kernel<false, 1><<<(unsigned)ntiles, MP_NT, 0, ctl->stream>>>(A, B, none, none, 0, split.ptr, nullptr,
+                                                                             nullptr, toff.ptr, nullptr, rows.ptr, cols.ptr);
+    CLB_CHECK_LAUNCH();
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    c.nnz = nnz;
+    c.rows = rows.release_ownership();
+    c.cols = cols.release_ownership();
+    *out = c;
+    return CLB_SUCCESS;
+}
+
+int clb_csr_add(clb_controls *ctl, const clb_csr *a_, const clb_csr *b_, clb_csr *out) {
+    if (!ctl || !a_ || !b_ || !out) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    CLB_RETURN_IF(shape_check(a_->nrows, a_->ncols, b_->nrows, b_->ncols));
+    DeviceGuard g(ctl);
+    return csr_add_impl(ctl, *a_, *b_, out);
+}
+
+int clb_csr_add_batched(clb_controls *ctl, uint32_t count, const clb_csr *a, const clb_csr *b, clb_csr *c) {
+    if (!ctl || (count && (!a || !b || !c))) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    if (count > 65535) return fail(CLB_NOT_SUPPORTED, "at most 65535 pairs per batch");
+    std::vector<AddDesc> hd(count);
+    std::vector<uint64_t> row_off(count + 1);
+    uint64_t rows = 0, anz = 0, bnz = 0, ncols = 0, largest = 1;
+    for (uint32_t k = 0; k < count; ++k) {
+        const int rc = shape_check(a[k].nrows, a[k].ncols, b[k].nrows, b[k].ncols);
+        if (rc != CLB_SUCCESS) return fail(rc, "pair " + std::to_string(k) + ": " + clb_last_error());
+        if ((a[k].nnz && !a[k].rpt) || (b[k].nnz && !b[k].rpt)) return fail(CLB_INVALID_ARGUMENT, "NULL rpt");
+        hd[k] = AddDesc{a[k].rpt, b[k].rpt, a[k].cols, b[k].cols, 0, a[k].nnz, b[k].nnz, rows, anz, bnz};
+        row_off[k] = rows;
+        rows += a[k].nrows;
+        anz += a[k].nnz;
+        bnz += b[k].nnz;
+        ncols = std::max(ncols, a[k].ncols);
+        largest = std::max(largest, std::max(a[k].nrows + 1, std::max(a[k].nnz, b[k].nnz)));
+    }
+    row_off[count] = rows;
+    for (uint32_t k = 0; k < count; ++k) {
+        clb_csr e{};
+        e.nrows = a[k].nrows;
+        e.ncols = a[k].ncols;
+        c[k] = e;
+    }
+    if (anz + bnz == 0) return CLB_SUCCESS;
+    if (rows >= (1ull << 32)) return fail(CLB_NOT_SUPPORTED, "the stacked batch has 2^32 or more rows");
+    DeviceGuard g(ctl);
+    // an operand without entries may come without row pointers: it stacks as
+    // empty rows (its descriptor points at a zero row pointer array)
+    Temp<uint64_t> zeros;
+    uint64_t max_rows = 0;
+    for (uint32_t k = 0; k < count; ++k) max_rows = std::max(max_rows, a[k].nrows);
+    CLB_RETURN_IF(zeros.alloc(ctl, max_rows + 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(zeros.ptr, 0, (max_rows + 1) * 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    for (uint32_t k = 0; k < count; ++k) {
+        hd[k].nrows = a[k].nrows;
+        if (!a[k].nnz || !a[k].rpt) hd[k].arpt = zeros.ptr;
+        if (!b[k].nnz || !b[k].rpt) hd[k].brpt = zeros.ptr;
+    }
+    Temp<AddDesc> dd;
+    Temp<uint64_t> arpt, brpt, roff, bounds;
+    Temp<uint32_t> acols, bcols;
+    CLB_RETURN_IF(dd.alloc(ctl, count));
+    CLB_RETURN_IF(arpt.alloc(ctl, rows + 1));
+    CLB_RETURN_IF(brpt.alloc(ctl, rows + 1));
+    CLB_RETURN_IF(acols.alloc(ctl, std::max<uint64_t>(anz, 1)));
+    CLB_RETURN_IF(bcols.alloc(ctl, std::max<uint64_t>(bnz, 1)));
+    CLB_RETURN_IF(roff.alloc(ctl, count + 1));
+    CLB_RETURN_IF(bounds.alloc(ctl, count + 1));
+    CLB_TRY_CUDA(cudaMemcpyAsync(dd.ptr, hd.data(), count * sizeof(AddDesc), cudaMemcpyHostToDevice, ctl->stream),
+                 CLB_WRITE_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(roff.ptr, row_off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, ctl->stream),
+                 CLB_WRITE_BUFFER_ERROR);
+    {
+        ProfScope ps(ctl, "add_stack");
+        add_stack_kernel<<<dim3(stack_blocks(largest), count), ST_NT, 0, ctl->stream>>>(
+            dd.ptr, arpt.ptr, acols.ptr, brpt.ptr, bcols.ptr, rows, anz, bnz);
+        CLB_CHECK_LAUNCH();
+    }
+    const clb_csr As{rows, ncols, anz, arpt.ptr, anz ? acols.ptr : nullptr};
+    const clb_csr Bs{rows, ncols, bnz, brpt.ptr, bnz ? bcols.ptr : nullptr};
+    clb_csr Cs{};
+    CLB_RETURN_IF(csr_add_impl(ctl, As, Bs, &Cs));
+    // cut the stacked sum into the pairs
+    std::vector<uint64_t> hb(count + 1);
+    int rc = CLB_SUCCESS;
+    {
+        add_bounds_kernel<<<(count + 256) / 256, 256, 0, ctl->stream>>>(Cs.rpt, roff.ptr, count, bounds.ptr);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hb.data(), bounds.ptr, (count + 1) * 8, cudaMemcpyDeviceToHost,
+                                                  ctl->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctl->stream);
+        if (e != cudaSuccess) rc = fail(CLB_RUN_KERNEL_FAILURE, cudaGetErrorString(e));
+    }
+    std::vector<AddOut> ho(count);
+    std::vector<clb_csr> outs(count);
+    uint64_t omax = 1;
+    for (uint32_t k = 0; k < count && rc == CLB_SUCCESS; ++k) {
+        clb_csr o{};
+        o.nrows = a[k].nrows;
+        o.ncols = a[k].ncols;
+        const uint64_t nnz = hb[k + 1] - hb[k];
+        AddOut d{nullptr, nullptr, 0, row_off[k], hb[k], 0};
+        if (nnz) {
+            Temp<uint64_t> p;
+            Temp<uint32_t> cc;
+            rc = p.alloc(ctl, o.nrows + 1);
+            if (rc == CLB_SUCCESS) rc = cc.alloc(ctl, nnz);
+            if (rc != CLB_SUCCESS) break;
+            d.rpt = p.ptr;
+            d.cols = cc.ptr;
+            d.nrows = o.nrows;
+            d.nnz = nnz;
+            o.nnz = nnz;
+            o.rpt = p.release_ownership();
+            o.cols = cc.release_ownership();
+            omax = std::max(omax, std::max(o.nrows + 1, nnz));
+        }
+        ho[k] = d;
+        outs[k] = o;
+    }
+    Temp<AddOut> dout;
+    if (rc == CLB_SUCCESS) rc = dout.alloc(ctl, count);
+    if (rc == CLB_SUCCESS) {
+        cudaError_t e = cudaMemcpyAsync(dout.ptr, ho.data(), count * sizeof(AddOut), cudaMemcpyHostToDevice,
+                                        ctl->stream);
+        if (e == cudaSuccess) {
+            ProfScope ps(ctl, "add_split");
+            add_split_kernel<<<dim3(stack_blocks(omax), count), ST_NT, 0, ctl->stream>>>(dout.ptr, Cs.rpt, Cs.cols);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctl->stream);
+        if (e != cudaSuccess) rc = fail(CLB_RUN_KERNEL_FAILURE, cudaGetErrorString(e));
+    }
+    clb_csr_release(ctl, &Cs);
+    if (rc != CLB_SUCCESS) {
+        for (auto &o : outs) clb_csr_release(ctl, &o);
+        return rc;
+    }
+    for (uint32_t k = 0; k < count; ++k) c[k] = outs[k];
     return CLB_SUCCESS;
 }
 

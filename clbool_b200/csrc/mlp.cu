@@ -225,10 +225,25 @@ __device__ __forceinline__ void write_features(float *__restrict__ feat, uint32_
     if (work) work[row] = s;
 }
 
+// Row position and density features of A row `row`: relative to A itself,
+// or, in a stacked batch (br.row_pair non-null), to the row's own pair.
+__device__ __forceinline__ void row_context(const AView &a, uint64_t row, uint64_t a_nrows, float density_term,
+                                            const BatchRows &br, float &rowpos, float &dens) {
+    if (br.row_pair) {
+        const PairFeat p = br.pairs[br.row_pair[row]];
+        rowpos = p.nrows ? (float)((double)(a.rows[row] - p.row0) / (double)p.nrows) : 0.0f;
+        dens = p.density;
+    } else {
+        rowpos = a_nrows ? (float)((double)a.rows[row] / (double)a_nrows) : 0.0f;
+        dens = density_term;
+    }
+}
+
 // A group of 8 lanes per A row; rows over FT_LONG entries are listed for
 // features_long_kernel (hub rows would keep 8 lanes busy long after the rest).
 __global__ void __launch_bounds__(FT_NT) features_kernel(AView a, BRows b, uint64_t a_nrows, float density_term,
-                                                         float *__restrict__ feat, uint32_t *__restrict__ work,
+                                                         BatchRows br, float *__restrict__ feat,
+                                                         uint32_t *__restrict__ work,
                                                          uint32_t *__restrict__ long_rows,
                                                          uint32_t *__restrict__ n_long) {
     const uint32_t gl = threadIdx.x & (FT_GROUP - 1);
@@ -254,15 +269,17 @@ __global__ void __launch_bounds__(FT_NT) features_kernel(AView a, BRows b, uint6
             mx = max(mx, __shfl_xor_sync(gmask, mx, d));
             mn = min(mn, __shfl_xor_sync(gmask, mn, d));
         }
-        if (gl == 0)
-            write_features(feat, work, row, je - ja, s, mx, mn,
-                           a_nrows ? (float)((double)a.rows[row] / (double)a_nrows) : 0.0f, density_term);
+        if (gl == 0) {
+            float rowpos, dens;
+            row_context(a, row, a_nrows, density_term, br, rowpos, dens);
+            write_features(feat, work, row, je - ja, s, mx, mn, rowpos, dens);
+        }
     }
 }
 
 // The listed long rows, one CTA per row.
 __global__ void __launch_bounds__(FT_NT) features_long_kernel(AView a, BRows b, uint64_t a_nrows, float density_term,
-                                                              const uint32_t *__restrict__ long_rows,
+                                                              BatchRows br, const uint32_t *__restrict__ long_rows,
                                                               const uint32_t *__restrict__ n_long,
                                                               float *__restrict__ feat, uint32_t *__restrict__ work) {
     __shared__ uint32_t red[3][FT_NT / 32];
@@ -297,8 +314,9 @@ __global__ void __launch_bounds__(FT_NT) features_long_kernel(AView a, BRows b, 
                 mx = max(mx, red[1][w]);
                 mn = min(mn, red[2][w]);
             }
-            write_features(feat, work, row, je - ja, s, mx, mn,
-                           a_nrows ? (float)((double)a.rows[row] / (double)a_nrows) : 0.0f, density_term);
+            float rowpos, dens;
+            row_context(a, row, a_nrows, density_term, br, rowpos, dens);
+            write_features(feat, work, row, je - ja, s, mx, mn, rowpos, dens);
         }
         __syncthreads();
     }
@@ -308,11 +326,13 @@ __global__ void __launch_bounds__(FT_NT) features_long_kernel(AView a, BRows b, 
 // the bitmap rows (more than `exact_below` products); the lighter rows get
 // their exact bound min(P, ncols): they hold a small share of the products,
 // and the ESC accumulators that serve them need no capacity check.
+// row_ncols (may be null): per row, the columns of its product (a stacked
+// batch of pairs).
 __global__ void capacity_kernel(const float *__restrict__ pred, const uint32_t *__restrict__ work, uint64_t n,
-                                uint64_t ncols, float margin_log2, float slack, uint32_t exact_below,
-                                uint32_t *__restrict__ cap) {
+                                uint64_t ncols, const uint32_t *__restrict__ row_ncols, float margin_log2, float slack,
+                                uint32_t exact_below, uint32_t *__restrict__ cap) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t ub = min((uint64_t)work[i], ncols);
+        const uint64_t ub = min((uint64_t)work[i], row_ncols ? (uint64_t)row_ncols[i] : ncols);
         if (work[i] <= exact_below) {
             cap[i] = (uint32_t)ub;
             continue;
@@ -331,10 +351,6 @@ unsigned grid_for(const clb_controls *ctl, uint64_t n, int nt = 256, int per_sm 
     return (unsigned)(g > c ? c : (g ? g : 1));
 }
 
-float density_term(const clb_dcsr &B) {
-    if (B.nnz == 0) return 0.f;
-    return (float)(std::log2((double)B.nrows * (double)B.ncols / (double)B.nnz)) * FEAT_SCALE;
-}
 
 // splitmix64: deterministic initialisation of the weights from a seed.
 uint64_t splitmix(uint64_t &s) {
@@ -345,23 +361,83 @@ uint64_t splitmix(uint64_t &s) {
 }
 
 int features_launch(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
-                    float *feat, uint32_t *work) {
+                    float *feat, uint32_t *work, const BatchRows *batch = nullptr) {
+    const BatchRows br = batch ? *batch : BatchRows{};
     Temp<uint32_t> long_rows, n_long;
     CLB_RETURN_IF(n_long.alloc(ctl, 1));
     CLB_RETURN_IF(long_rows.alloc(ctl, A.nzr ? A.nzr : 1));
     CLB_TRY_CUDA(cudaMemsetAsync(n_long.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
     ProfScope ps(ctl, "features");
-    const float dt = density_term(B);
-    features_kernel<<<grid_for(ctl, A.nzr * FT_GROUP), FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, feat, work,
+    const float dt = learned_density_feature(B);
+    features_kernel<<<grid_for(ctl, A.nzr * FT_GROUP), FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, br, feat, work,
                                                                               long_rows.ptr, n_long.ptr);
-    features_long_kernel<<<ctl->sm_count * 4, FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, long_rows.ptr, n_long.ptr,
-                                                                       feat, work);
+    features_long_kernel<<<ctl->sm_count * 4, FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, br, long_rows.ptr,
+                                                                       n_long.ptr, feat, work);
     ctl->launches += 2;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
 }
 
 }  // namespace
+
+float learned_density_feature(const clb_dcsr &B) {
+    if (B.nnz == 0) return 0.f;
+    return (float)(std::log2((double)B.nrows * (double)B.ncols / (double)B.nnz)) * FEAT_SCALE;
+}
+
+int learned_caps(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
+                 const clb_sizer *sizer, float margin_log2, float slack, const Tuning &t, const BatchRows *batch,
+                 uint32_t *work, uint32_t *cap) {
+    const uint64_t n = A.nzr;
+    Temp<float> feat, pred;
+    CLB_RETURN_IF(feat.alloc(ctl, n * F));
+    CLB_RETURN_IF(pred.alloc(ctl, n));
+    CLB_RETURN_IF(features_launch(ctl, A, B, a, b, feat.ptr, work, batch));
+    ProfScope ps(ctl, "predict");
+    predict_kernel<<<grid_for(ctl, n, MLP_NT, 4), MLP_NT, 0, ctl->stream>>>(sizer->params, feat.ptr, n, pred.ptr);
+    capacity_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(pred.ptr, work, n, B.ncols, t.row_ncols, margin_log2,
+                                                              slack, t.bitmap_min, cap);
+    ctl->launches += 2;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
+int spgemm_learned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const clb_sizer *sizer,
+                   float margin_log2, float slack, const Tuning &t, const BatchRows *batch, clb_dcsr *c,
+                   clb_spgemm_stats *stats) {
+    clb_spgemm_stats st{};
+    ctl->launches = 0;
+    if (A.nnz == 0 || B.nnz == 0 || A.nzr == 0 || B.nzr == 0) {
+        clb_dcsr C{};
+        C.nrows = A.nrows;
+        C.ncols = B.ncols;
+        *c = C;
+        if (stats) *stats = st;
+        return CLB_SUCCESS;
+    }
+    CLB_RETURN_IF(clear_status(ctl));
+    const uint64_t n = A.nzr;
+    const AView a{A.rpt, A.rows, A.cols, A.nzr};
+    BRows b;
+    Temp<uint64_t> dense, tot, wsum;
+    Temp<uint32_t> work, cap;
+    CLB_RETURN_IF(prepare_b(ctl, B, dense, b));
+    CLB_RETURN_IF(work.alloc(ctl, n));
+    CLB_RETURN_IF(cap.alloc(ctl, n));
+    CLB_RETURN_IF(tot.alloc(ctl, 1));
+    CLB_RETURN_IF(learned_caps(ctl, A, B, a, b, sizer, margin_log2, slack, t, batch, work.ptr, cap.ptr));
+    // products: the single-pass driver reports them; sum the workload here
+    CLB_RETURN_IF(wsum.alloc(ctl, n));
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, work.ptr, wsum.ptr, n, tot.ptr));
+    uint64_t products = 0;
+    CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &products, 1));
+    // ESC accumulators for the rows up to ESC_MAX_PRODUCTS products, learned
+    // capacities and the spill arena (1/16 of the slots) for the bitmap rows
+    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st, 16, t);
+    st.kernel_launches = ctl->launches;
+    if (stats) *stats = st;
+    return rc;
+}
 
 }  // namespace clb
 
@@ -596,54 +672,9 @@ int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a_, const clb_dcs
                             clb_spgemm_stats *stats) {
     if (!ctl || !a_ || !b_ || !c || !sizer) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
     CLB_RETURN_IF(check_tuning(tuning));
-    const Tuning t = to_tuning(tuning);
-    const clb_dcsr A = *a_, B = *b_;
-    CLB_RETURN_IF(validate_spgemm(A, B));
+    CLB_RETURN_IF(validate_spgemm(*a_, *b_));
     DeviceGuard g(ctl);
-    clb_spgemm_stats st{};
-    ctl->launches = 0;
-    if (A.nnz == 0 || B.nnz == 0 || A.nzr == 0 || B.nzr == 0) {
-        clb_dcsr C{};
-        C.nrows = A.nrows;
-        C.ncols = B.ncols;
-        *c = C;
-        if (stats) *stats = st;
-        return CLB_SUCCESS;
-    }
-    CLB_RETURN_IF(clear_status(ctl));
-    const uint64_t n = A.nzr;
-    const AView a{A.rpt, A.rows, A.cols, A.nzr};
-    BRows b;
-    Temp<uint64_t> dense, tot;
-    Temp<uint32_t> work, cap;
-    Temp<float> feat, pred;
-    CLB_RETURN_IF(prepare_b(ctl, B, dense, b));
-    CLB_RETURN_IF(work.alloc(ctl, n));
-    CLB_RETURN_IF(cap.alloc(ctl, n));
-    CLB_RETURN_IF(feat.alloc(ctl, n * F));
-    CLB_RETURN_IF(pred.alloc(ctl, n));
-    CLB_RETURN_IF(tot.alloc(ctl, 1));
-    CLB_RETURN_IF(features_launch(ctl, A, B, a, b, feat.ptr, work.ptr));
-    {
-        ProfScope ps(ctl, "predict");
-        predict_kernel<<<grid_for(ctl, n, MLP_NT, 4), MLP_NT, 0, ctl->stream>>>(sizer->params, feat.ptr, n, pred.ptr);
-        capacity_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(pred.ptr, work.ptr, n, B.ncols, margin_log2, slack,
-                                                                  t.bitmap_min, cap.ptr);
-        ctl->launches += 2;
-        CLB_CHECK_LAUNCH();
-    }
-    // products: the single-pass driver reports them; sum the workload here
-    Temp<uint64_t> wsum;
-    CLB_RETURN_IF(wsum.alloc(ctl, n));
-    CLB_RETURN_IF(scan_u32_to_u64(ctl, work.ptr, wsum.ptr, n, tot.ptr));
-    uint64_t products = 0;
-    CLB_RETURN_IF(read_scalars(ctl, tot.ptr, &products, 1));
-    // ESC accumulators for the rows up to ESC_MAX_PRODUCTS products, learned
-    // capacities and the spill arena (1/16 of the slots) for the bitmap rows
-    int rc = spgemm_single_pass(ctl, A, B, a, b, work.ptr, cap.ptr, true, products, c, &st, 16, t);
-    st.kernel_launches = ctl->launches;
-    if (stats) *stats = st;
-    return rc;
+    return spgemm_learned(ctl, *a_, *b_, sizer, margin_log2, slack, to_tuning(tuning), nullptr, c, stats);
 }
 
 }  // extern "C"

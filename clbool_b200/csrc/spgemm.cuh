@@ -43,10 +43,47 @@ int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AVie
 int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                        const uint32_t *work, uint32_t *cap, bool esc, uint64_t products, clb_dcsr *out,
                        clb_spgemm_stats *st, uint64_t arena_div, const Tuning &t = Tuning());
+// Per-row pair context of a stacked batch (the learned form's row features
+// are relative to each row's own pair): row_pair[i] = pair of stacked row i,
+// pairs[k] = that pair's first row id in the stack, its rows and the density
+// feature of its right operand.
+struct PairFeat {
+    uint32_t row0;
+    uint32_t nrows;
+    float density;
+    uint32_t pad;
+};
+struct BatchRows {
+    const uint32_t *row_pair = nullptr;
+    const PairFeat *pairs = nullptr;
+};
+// log2(B.nrows * B.ncols / nnz(B)) / 16: the density feature of a right operand.
+float learned_density_feature(const clb_dcsr &B);
+// Learned capacities (mlp.cu): work[i] = products of A row i and cap[i] =
+// its slot (predicted for rows over t.bitmap_min products, exact below;
+// never above min(work, the row's columns)); batch = per-row pair context
+// of a stacked batch, or null.
+int learned_caps(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
+                 const clb_sizer *sizer, float margin_log2, float slack, const Tuning &t, const BatchRows *batch,
+                 uint32_t *work, uint32_t *cap);
+// The learned single pass: learned capacities, one numeric pass with the
+// spill arena, exact fallback of the rows that outgrew both, compaction.
+int spgemm_learned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const clb_sizer *sizer,
+                   float margin_log2, float slack, const Tuning &t, const BatchRows *batch, clb_dcsr *c,
+                   clb_spgemm_stats *st);
+// Learned sizing of the host-sync-free form: capacities from the predictor
+// and a spill arena of arena_capacity entries for the rows that outgrow them.
+struct CaptureLearned {
+    const clb_sizer *sizer;
+    float margin_log2, slack;
+    BatchRows batch;
+    uint64_t arena_capacity;
+};
 // Flags of the host-sync-free form (bits of its device flag word).
 constexpr uint32_t CAPTURE_SLOTS_FULL = 1u;    // slot capacity too small: rows left empty
 constexpr uint32_t CAPTURE_COLS_FULL = 2u;     // column capacity too small: rows not written
 constexpr uint32_t CAPTURE_DEVICE_CHECK = 4u;  // an accumulator's device check failed
+constexpr uint32_t CAPTURE_ROW_OVERFLOW = 8u;  // a row outgrew its learned slot and the arena: left empty
 // The ESC single pass with every size from the caller and no host read:
 // slots (slot_capacity entries) and the stream-ordered temporaries are
 // allocated on ctl's stream, C goes to the caller's arrays (rpt: A.nzr + 1,
@@ -56,7 +93,7 @@ constexpr uint32_t CAPTURE_DEVICE_CHECK = 4u;  // an accumulator's device check 
 int spgemm_esc_capture(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const Tuning &t,
                        uint64_t slot_capacity, const uint64_t *first, const uint32_t *row_base, uint32_t count,
                        uint64_t *c_rpt, uint32_t *c_rows, uint32_t *c_cols, uint64_t cols_capacity,
-                       uint64_t *d_result, uint32_t *d_flags);
+                       uint64_t *d_result, uint32_t *d_flags, const CaptureLearned *learned = nullptr);
 // cap[i] = min(work[i], ncols): the exact upper bound of a row's count.
 int launch_upper_bound_caps(clb_controls *ctl, const uint32_t *work, uint64_t n, uint64_t ncols, uint32_t *cap);
 // Public tuning struct -> internal tuning (zero fields: defaults), and its check.

@@ -36,10 +36,12 @@ struct PairDesc {
 constexpr int CAT_NT = 256;
 
 // Stacks the pairs' matrices: blockIdx.y = pair.
-// row_ncols (may be null): per stacked row, the columns of its pair's product.
+// row_ncols (may be null): per stacked row, the columns of its pair's product;
+// row_pair (may be null): per stacked row, its pair.
 __global__ void __launch_bounds__(CAT_NT) stack_kernel(const PairDesc *__restrict__ d, uint64_t *__restrict__ rpt,
                                                        uint32_t *__restrict__ rows, uint32_t *__restrict__ cols,
-                                                       uint32_t *__restrict__ row_ncols, uint64_t total_nzr,
+                                                       uint32_t *__restrict__ row_ncols,
+                                                       uint32_t *__restrict__ row_pair, uint64_t total_nzr,
                                                        uint64_t total_nnz) {
     const PairDesc p = d[blockIdx.y];
     const uint64_t stride = (uint64_t)gridDim.x * CAT_NT;
@@ -49,6 +51,7 @@ __global__ void __launch_bounds__(CAT_NT) stack_kernel(const PairDesc *__restric
         rows[p.nzr_off + r] = p.rows[r] + p.row_add;
         rpt[p.nzr_off + r] = p.rpt[r] - base + p.nnz_off;
         if (row_ncols) row_ncols[p.nzr_off + r] = p.ncols;
+        if (row_pair) row_pair[p.nzr_off + r] = blockIdx.y;
     }
     for (uint64_t j = t0; j < p.nnz; j += stride) cols[p.nnz_off + j] = p.cols[j] + p.col_add;
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) rpt[total_nzr] = total_nnz;
@@ -143,17 +146,19 @@ int spgemm_tuned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, uint32
 constexpr uint32_t DESC_CHUNK = 24;
 struct DescChunk {
     PairDesc a[DESC_CHUNK], b[DESC_CHUNK];
+    PairFeat f[DESC_CHUNK];
 };
 
 __global__ void store_descs_kernel(DescChunk c, uint32_t k0, uint32_t n, PairDesc *__restrict__ da,
                                    PairDesc *__restrict__ db, uint64_t *__restrict__ first,
-                                   uint32_t *__restrict__ row_base) {
+                                   uint32_t *__restrict__ row_base, PairFeat *__restrict__ pf) {
     const uint32_t j = threadIdx.x;
     if (j < n) {
         da[k0 + j] = c.a[j];
         db[k0 + j] = c.b[j];
         first[k0 + j] = c.a[j].nzr_off;
         row_base[k0 + j] = c.a[j].row_add;
+        if (pf) pf[k0 + j] = c.f[j];
     }
 }
 
@@ -202,63 +207,11 @@ int pair_descs(uint32_t count, const clb_dcsr *a, const clb_dcsr *b, std::vector
     return CLB_SUCCESS;
 }
 
-}  // namespace
-
-Tuning to_tuning(const clb_spgemm_tuning *t) {
-    Tuning r;
-    if (!t) return r;
-    if (t->warp_max) r.warp_max = t->warp_max;
-    if (t->bitmap_min) r.bitmap_min = t->bitmap_min;
-    if (t->bitmap_threads) r.bitmap_threads = t->bitmap_threads;
-    if (t->small_lanes) r.small_lanes = t->small_lanes;
-    if (t->wide_rows) r.wide_cluster = t->wide_rows == 1;
-    return r;
-}
-
-int check_tuning(const clb_spgemm_tuning *t) {
-    if (!t) return CLB_SUCCESS;
-    if (t->form > 1) return fail(CLB_INVALID_VALUE, "tuning.form must be 0 (two-pass) or 1 (single pass)");
-    if (t->warp_max && t->warp_max != 32 && t->warp_max != 64 && t->warp_max != 128 && t->warp_max != 256)
-        return fail(CLB_INVALID_VALUE, "tuning.warp_max must be 32, 64, 128 or 256");
-    if (t->bitmap_min && (t->bitmap_min < 256 || t->bitmap_min > ESC_MAX_PRODUCTS))
-        return fail(CLB_INVALID_VALUE, "tuning.bitmap_min must be in [256, 4096]");
-    if (t->bitmap_threads && t->bitmap_threads != 256 && t->bitmap_threads != 512 && t->bitmap_threads != 1024)
-        return fail(CLB_INVALID_VALUE, "tuning.bitmap_threads must be 256, 512 or 1024");
-    if (t->small_lanes && t->small_lanes != 8 && t->small_lanes != 16 && t->small_lanes != 32)
-        return fail(CLB_INVALID_VALUE, "tuning.small_lanes must be 8, 16 or 32");
-    if (t->wide_rows > 2) return fail(CLB_INVALID_VALUE, "tuning.wide_rows must be 1 (cluster) or 2 (chunks)");
-    return CLB_SUCCESS;
-}
-
-}  // namespace clb
-
-using namespace clb;
-
-extern "C" {
-
-void clb_spgemm_tuning_default(clb_spgemm_tuning *t) {
-    if (!t) return;
-    *t = clb_spgemm_tuning{};
-    const Tuning d;
-    t->form = 0;
-    t->warp_max = d.warp_max;
-    t->bitmap_min = d.bitmap_min;
-    t->bitmap_threads = d.bitmap_threads;
-    t->small_lanes = d.small_lanes;
-    t->wide_rows = d.wide_cluster ? 1 : 2;
-}
-
-int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_spgemm_tuning *tuning,
-                          clb_dcsr *c, clb_spgemm_stats *stats) {
-    if (!ctl || !a || !b || !c) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
-    CLB_RETURN_IF(check_tuning(tuning));
-    CLB_RETURN_IF(validate_spgemm(*a, *b));
-    DeviceGuard g(ctl);
-    return spgemm_tuned(ctl, *a, *b, tuning ? tuning->form : 0, to_tuning(tuning), c, stats);
-}
-
-int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
-                            const clb_spgemm_tuning *tuning, clb_spgemm_stats *stats) {
+// The batched product: stack, one product over the stack (exact / tuned
+// form, or the learned single pass when `sizer` is given), split.
+int batched_impl(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
+                 const clb_spgemm_tuning *tuning, const clb_sizer *sizer, float margin_log2, float slack,
+                 clb_spgemm_stats *stats) {
     if (!ctl || (count && (!a || !b || !c))) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
     if (count > 65535) return fail(CLB_NOT_SUPPORTED, "at most 65535 pairs per batch");
     CLB_RETURN_IF(check_tuning(tuning));
@@ -307,13 +260,24 @@ int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a
     // stacked operands
     Temp<PairDesc> dda, ddb;
     Temp<uint64_t> arpt, brpt, rs;
-    Temp<uint32_t> arws, acls, brws, bcls, rnc;
+    Temp<uint32_t> arws, acls, brws, bcls, rnc, rpair;
+    Temp<PairFeat> pf;
     CLB_RETURN_IF(dda.alloc(ctl, count));
     CLB_RETURN_IF(ddb.alloc(ctl, count));
     CLB_RETURN_IF(rs.alloc(ctl, count + 1));
     CLB_RETURN_IF(arpt.alloc(ctl, anzr + 1));
     CLB_RETURN_IF(arws.alloc(ctl, anzr));
     CLB_RETURN_IF(rnc.alloc(ctl, anzr));
+    if (sizer) {
+        // per-row pair context of the row features
+        std::vector<PairFeat> hf(count);
+        for (uint32_t k = 0; k < count; ++k)
+            hf[k] = PairFeat{(uint32_t)row_start[k], (uint32_t)a[k].nrows, learned_density_feature(b[k]), 0u};
+        CLB_RETURN_IF(rpair.alloc(ctl, anzr));
+        CLB_RETURN_IF(pf.alloc(ctl, count));
+        CLB_TRY_CUDA(cudaMemcpyAsync(pf.ptr, hf.data(), count * sizeof(PairFeat), cudaMemcpyHostToDevice, ctl->stream),
+                     CLB_WRITE_BUFFER_ERROR);
+    }
     CLB_RETURN_IF(acls.alloc(ctl, annz));
     CLB_RETURN_IF(brpt.alloc(ctl, bnzr + 1));
     CLB_RETURN_IF(brws.alloc(ctl, bnzr));
@@ -327,9 +291,9 @@ int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a
     {
         ProfScope ps(ctl, "batch_stack");
         stack_kernel<<<dim3(stack_grid_x(ctl, amax, count), count), CAT_NT, 0, ctl->stream>>>(
-            dda.ptr, arpt.ptr, arws.ptr, acls.ptr, rnc.ptr, anzr, annz);
+            dda.ptr, arpt.ptr, arws.ptr, acls.ptr, rnc.ptr, rpair.ptr, anzr, annz);
         stack_kernel<<<dim3(stack_grid_x(ctl, bmax, count), count), CAT_NT, 0, ctl->stream>>>(
-            ddb.ptr, brpt.ptr, brws.ptr, bcls.ptr, nullptr, bnzr, bnnz);
+            ddb.ptr, brpt.ptr, brws.ptr, bcls.ptr, nullptr, nullptr, bnzr, bnnz);
         CLB_CHECK_LAUNCH();
     }
     const clb_dcsr As{arows, brows, annz, anzr, arpt.ptr, arws.ptr, acls.ptr};
@@ -337,7 +301,12 @@ int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a
     CLB_RETURN_IF(validate_spgemm(As, Bs));
     clb_dcsr Cs{};
     t.row_ncols = rnc.ptr;  // each pair's rows use a bitmap as wide as its own product
-    CLB_RETURN_IF(spgemm_tuned(ctl, As, Bs, form, t, &Cs, &st));
+    if (sizer) {
+        const BatchRows br{rpair.ptr, pf.ptr};
+        CLB_RETURN_IF(spgemm_learned(ctl, As, Bs, sizer, margin_log2, slack, t, &br, &Cs, &st));
+    } else {
+        CLB_RETURN_IF(spgemm_tuned(ctl, As, Bs, form, t, &Cs, &st));
+    }
     const uint32_t inner_launches = st.kernel_launches;
     if (Cs.nnz == 0) {
         st.kernel_launches = inner_launches + 2;
@@ -409,6 +378,167 @@ int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a
     return CLB_SUCCESS;
 }
 
+// The pairs stacked block-diagonally on the device, with the pair
+// descriptors passed as kernel parameters (no host memory is read when the
+// launches are replayed from a CUDA graph).  pair_ctx: also the per-row pair
+// context of the learned row features.
+struct Stack {
+    Temp<PairDesc> dda, ddb;
+    Temp<uint64_t> first, arpt, brpt;
+    Temp<uint32_t> rbase, arws, acls, brws, bcls, rnc, rpair;
+    Temp<PairFeat> pf;
+    clb_dcsr As{}, Bs{};
+};
+
+int build_stack(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                const std::vector<PairDesc> &da, const std::vector<PairDesc> &db, uint64_t arows, uint64_t brows,
+                uint64_t anzr, uint64_t annz, uint64_t bnzr, uint64_t bnnz, uint64_t bcols, uint64_t amax,
+                uint64_t bmax, bool pair_ctx, Stack &st) {
+    CLB_RETURN_IF(st.dda.alloc(ctl, count));
+    CLB_RETURN_IF(st.ddb.alloc(ctl, count));
+    CLB_RETURN_IF(st.first.alloc(ctl, count));
+    CLB_RETURN_IF(st.rbase.alloc(ctl, count));
+    CLB_RETURN_IF(st.arpt.alloc(ctl, anzr + 1));
+    CLB_RETURN_IF(st.arws.alloc(ctl, anzr));
+    CLB_RETURN_IF(st.rnc.alloc(ctl, anzr));
+    CLB_RETURN_IF(st.acls.alloc(ctl, annz));
+    CLB_RETURN_IF(st.brpt.alloc(ctl, bnzr + 1));
+    CLB_RETURN_IF(st.brws.alloc(ctl, bnzr));
+    CLB_RETURN_IF(st.bcls.alloc(ctl, bnnz));
+    if (pair_ctx) {
+        CLB_RETURN_IF(st.rpair.alloc(ctl, anzr));
+        CLB_RETURN_IF(st.pf.alloc(ctl, count));
+    }
+    for (uint32_t k0 = 0; k0 < count; k0 += DESC_CHUNK) {
+        DescChunk ch{};
+        const uint32_t nk = std::min<uint32_t>(DESC_CHUNK, count - k0);
+        for (uint32_t j = 0; j < nk; ++j) {
+            ch.a[j] = da[k0 + j];
+            ch.b[j] = db[k0 + j];
+            ch.f[j] = PairFeat{da[k0 + j].row_add, (uint32_t)a[k0 + j].nrows, learned_density_feature(b[k0 + j]), 0u};
+        }
+        store_descs_kernel<<<1, DESC_CHUNK, 0, ctl->stream>>>(ch, k0, nk, st.dda.ptr, st.ddb.ptr, st.first.ptr,
+                                                              st.rbase.ptr, st.pf.ptr);
+        ctl->launches += 1;
+    }
+    CLB_CHECK_LAUNCH();
+    {
+        ProfScope ps(ctl, "batch_stack");
+        stack_kernel<<<dim3(stack_grid_x(ctl, amax, count), count), CAT_NT, 0, ctl->stream>>>(
+            st.dda.ptr, st.arpt.ptr, st.arws.ptr, st.acls.ptr, st.rnc.ptr, st.rpair.ptr, anzr, annz);
+        stack_kernel<<<dim3(stack_grid_x(ctl, bmax, count), count), CAT_NT, 0, ctl->stream>>>(
+            st.ddb.ptr, st.brpt.ptr, st.brws.ptr, st.bcls.ptr, nullptr, nullptr, bnzr, bnnz);
+        ctl->launches += 2;
+        CLB_CHECK_LAUNCH();
+    }
+    st.As = clb_dcsr{arows, brows, annz, anzr, st.arpt.ptr, st.arws.ptr, st.acls.ptr};
+    st.Bs = clb_dcsr{brows, bcols, bnnz, bnzr, st.brpt.ptr, st.brws.ptr, st.bcls.ptr};
+    return validate_spgemm(st.As, st.Bs);
+}
+
+// The host-sync-free batched product (upper-bound slots, or learned slots
+// and a spill arena when `sizer` is given).
+int capture_impl(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                 const clb_spgemm_tuning *tuning, const clb_sizer *sizer, float margin_log2, float slack,
+                 uint64_t slot_capacity, uint64_t arena_capacity, uint64_t *c_rpt, uint32_t *c_rows,
+                 uint32_t *c_cols, uint64_t cols_capacity, uint64_t *result, uint32_t *flags) {
+    if (!ctl || (count && (!a || !b)) || !result || !flags) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    if (count == 0) return fail(CLB_INVALID_ARGUMENT, "empty batch");
+    if (count > 65535) return fail(CLB_NOT_SUPPORTED, "at most 65535 pairs per batch");
+    CLB_RETURN_IF(check_tuning(tuning));
+    std::vector<PairDesc> da, db;
+    uint64_t arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax;
+    CLB_RETURN_IF(pair_descs(count, a, b, da, db, arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax));
+    if (!c_rpt || (anzr && !c_rows) || (cols_capacity && !c_cols))
+        return fail(CLB_INVALID_ARGUMENT, "NULL output array");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaMemsetAsync(flags, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(result, 0, (2 + 2 * ((uint64_t)count + 1)) * 8, ctl->stream),
+                 CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemsetAsync(c_rpt, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    if (annz == 0) return CLB_SUCCESS;
+    CLB_RETURN_IF(clear_status(ctl));
+    ctl->launches = 0;
+    Tuning t = to_tuning(tuning);
+    Stack stk;
+    CLB_RETURN_IF(build_stack(ctl, count, a, b, da, db, arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax,
+                              sizer != nullptr, stk));
+    t.row_ncols = stk.rnc.ptr;
+    if (!sizer)
+        return spgemm_esc_capture(ctl, stk.As, stk.Bs, t, slot_capacity, stk.first.ptr, stk.rbase.ptr, count, c_rpt,
+                                  c_rows, c_cols, cols_capacity, result, flags);
+    const CaptureLearned lc{sizer, margin_log2, slack, BatchRows{stk.rpair.ptr, stk.pf.ptr}, arena_capacity};
+    return spgemm_esc_capture(ctl, stk.As, stk.Bs, t, slot_capacity, stk.first.ptr, stk.rbase.ptr, count, c_rpt,
+                              c_rows, c_cols, cols_capacity, result, flags, &lc);
+}
+
+}  // namespace
+
+Tuning to_tuning(const clb_spgemm_tuning *t) {
+    Tuning r;
+    if (!t) return r;
+    if (t->warp_max) r.warp_max = t->warp_max;
+    if (t->bitmap_min) r.bitmap_min = t->bitmap_min;
+    if (t->bitmap_threads) r.bitmap_threads = t->bitmap_threads;
+    if (t->small_lanes) r.small_lanes = t->small_lanes;
+    if (t->wide_rows) r.wide_cluster = t->wide_rows == 1;
+    return r;
+}
+
+int check_tuning(const clb_spgemm_tuning *t) {
+    if (!t) return CLB_SUCCESS;
+    if (t->form > 1) return fail(CLB_INVALID_VALUE, "tuning.form must be 0 (two-pass) or 1 (single pass)");
+    if (t->warp_max && t->warp_max != 32 && t->warp_max != 64 && t->warp_max != 128 && t->warp_max != 256)
+        return fail(CLB_INVALID_VALUE, "tuning.warp_max must be 32, 64, 128 or 256");
+    if (t->bitmap_min && (t->bitmap_min < 256 || t->bitmap_min > ESC_MAX_PRODUCTS))
+        return fail(CLB_INVALID_VALUE, "tuning.bitmap_min must be in [256, 4096]");
+    if (t->bitmap_threads && t->bitmap_threads != 256 && t->bitmap_threads != 512 && t->bitmap_threads != 1024)
+        return fail(CLB_INVALID_VALUE, "tuning.bitmap_threads must be 256, 512 or 1024");
+    if (t->small_lanes && t->small_lanes != 8 && t->small_lanes != 16 && t->small_lanes != 32)
+        return fail(CLB_INVALID_VALUE, "tuning.small_lanes must be 8, 16 or 32");
+    if (t->wide_rows > 2) return fail(CLB_INVALID_VALUE, "tuning.wide_rows must be 1 (cluster) or 2 (chunks)");
+    return CLB_SUCCESS;
+}
+
+}  // namespace clb
+
+using namespace clb;
+
+extern "C" {
+
+void clb_spgemm_tuning_default(clb_spgemm_tuning *t) {
+    if (!t) return;
+    *t = clb_spgemm_tuning{};
+    const Tuning d;
+    t->form = 0;
+    t->warp_max = d.warp_max;
+    t->bitmap_min = d.bitmap_min;
+    t->bitmap_threads = d.bitmap_threads;
+    t->small_lanes = d.small_lanes;
+    t->wide_rows = d.wide_cluster ? 1 : 2;
+}
+
+int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const clb_dcsr *b, const clb_spgemm_tuning *tuning,
+                          clb_dcsr *c, clb_spgemm_stats *stats) {
+    if (!ctl || !a || !b || !c) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    CLB_RETURN_IF(check_tuning(tuning));
+    CLB_RETURN_IF(validate_spgemm(*a, *b));
+    DeviceGuard g(ctl);
+    return spgemm_tuned(ctl, *a, *b, tuning ? tuning->form : 0, to_tuning(tuning), c, stats);
+}
+
+int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
+                            const clb_spgemm_tuning *tuning, clb_spgemm_stats *stats) {
+    return batched_impl(ctl, count, a, b, c, tuning, nullptr, 0.f, 0.f, stats);
+}
+
+int clb_dcsr_spgemm_batched_learned(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                                    clb_dcsr *c, const clb_sizer *sizer, float margin_log2, float slack,
+                                    const clb_spgemm_tuning *tuning, clb_spgemm_stats *stats) {
+    if (!sizer) return fail(CLB_INVALID_ARGUMENT, "NULL sizer");
+    return batched_impl(ctl, count, a, b, c, tuning, sizer, margin_log2, slack, stats);
+}
+
 int clb_spgemm_batched_plan(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                             uint64_t *rows_need, uint64_t *slots_need) {
     if (!ctl || (count && (!a || !b)) || !rows_need || !slots_need) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
@@ -444,64 +574,57 @@ int clb_dcsr_spgemm_batched_capture(clb_controls *ctl, uint32_t count, const clb
                                     const clb_spgemm_tuning *tuning, uint64_t slot_capacity, uint64_t *c_rpt,
                                     uint32_t *c_rows, uint32_t *c_cols, uint64_t cols_capacity, uint64_t *result,
                                     uint32_t *flags) {
-    if (!ctl || (count && (!a || !b)) || !result || !flags) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
-    if (count == 0) return fail(CLB_INVALID_ARGUMENT, "empty batch");
+    return capture_impl(ctl, count, a, b, tuning, nullptr, 0.f, 0.f, slot_capacity, 0, c_rpt, c_rows, c_cols,
+                        cols_capacity, result, flags);
+}
+
+int clb_dcsr_spgemm_batched_capture_learned(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                                            const clb_sizer *sizer, float margin_log2, float slack,
+                                            const clb_spgemm_tuning *tuning, uint64_t slot_capacity,
+                                            uint64_t arena_capacity, uint64_t *c_rpt, uint32_t *c_rows,
+                                            uint32_t *c_cols, uint64_t cols_capacity, uint64_t *result,
+                                            uint32_t *flags) {
+    if (!sizer) return fail(CLB_INVALID_ARGUMENT, "NULL sizer");
+    return capture_impl(ctl, count, a, b, tuning, sizer, margin_log2, slack, slot_capacity, arena_capacity, c_rpt,
+                        c_rows, c_cols, cols_capacity, result, flags);
+}
+
+int clb_spgemm_batched_plan_learned(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
+                                    const clb_sizer *sizer, float margin_log2, float slack,
+                                    const clb_spgemm_tuning *tuning, uint64_t *rows_need, uint64_t *slots_need) {
+    if (!ctl || (count && (!a || !b)) || !sizer || !rows_need || !slots_need)
+        return fail(CLB_INVALID_ARGUMENT, "NULL argument");
     if (count > 65535) return fail(CLB_NOT_SUPPORTED, "at most 65535 pairs per batch");
     CLB_RETURN_IF(check_tuning(tuning));
     std::vector<PairDesc> da, db;
     uint64_t arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax;
     CLB_RETURN_IF(pair_descs(count, a, b, da, db, arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax));
-    if (!c_rpt || (anzr && !c_rows) || (cols_capacity && !c_cols))
-        return fail(CLB_INVALID_ARGUMENT, "NULL output array");
-    DeviceGuard g(ctl);
-    CLB_TRY_CUDA(cudaMemsetAsync(flags, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
-    CLB_TRY_CUDA(cudaMemsetAsync(result, 0, (2 + 2 * ((uint64_t)count + 1)) * 8, ctl->stream),
-                 CLB_RUN_KERNEL_FAILURE);
-    CLB_TRY_CUDA(cudaMemsetAsync(c_rpt, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    *rows_need = anzr;
+    *slots_need = 0;
     if (annz == 0) return CLB_SUCCESS;
-    CLB_RETURN_IF(clear_status(ctl));
-    ctl->launches = 0;
+    DeviceGuard g(ctl);
+    Stack stk;
+    CLB_RETURN_IF(build_stack(ctl, count, a, b, da, db, arows, brows, anzr, annz, bnzr, bnnz, bcols, amax, bmax,
+                              true, stk));
     Tuning t = to_tuning(tuning);
-    Temp<PairDesc> dda, ddb;
-    Temp<uint64_t> first, arpt, brpt;
-    Temp<uint32_t> rbase, arws, acls, brws, bcls, rnc;
-    CLB_RETURN_IF(dda.alloc(ctl, count));
-    CLB_RETURN_IF(ddb.alloc(ctl, count));
-    CLB_RETURN_IF(first.alloc(ctl, count));
-    CLB_RETURN_IF(rbase.alloc(ctl, count));
-    CLB_RETURN_IF(arpt.alloc(ctl, anzr + 1));
-    CLB_RETURN_IF(arws.alloc(ctl, anzr));
-    CLB_RETURN_IF(rnc.alloc(ctl, anzr));
-    CLB_RETURN_IF(acls.alloc(ctl, annz));
-    CLB_RETURN_IF(brpt.alloc(ctl, bnzr + 1));
-    CLB_RETURN_IF(brws.alloc(ctl, bnzr));
-    CLB_RETURN_IF(bcls.alloc(ctl, bnnz));
-    for (uint32_t k0 = 0; k0 < count; k0 += DESC_CHUNK) {
-        DescChunk ch{};
-        const uint32_t nk = std::min<uint32_t>(DESC_CHUNK, count - k0);
-        for (uint32_t j = 0; j < nk; ++j) {
-            ch.a[j] = da[k0 + j];
-            ch.b[j] = db[k0 + j];
-        }
-        store_descs_kernel<<<1, DESC_CHUNK, 0, ctl->stream>>>(ch, k0, nk, dda.ptr, ddb.ptr, first.ptr, rbase.ptr);
-        ctl->launches += 1;
-    }
+    t.row_ncols = stk.rnc.ptr;
+    const AView av{stk.As.rpt, stk.As.rows, stk.As.cols, stk.As.nzr};
+    BRows bv;
+    Temp<uint64_t> dense, need;
+    Temp<uint32_t> work, cap;
+    CLB_RETURN_IF(prepare_b(ctl, stk.Bs, dense, bv));
+    CLB_RETURN_IF(work.alloc(ctl, anzr));
+    CLB_RETURN_IF(cap.alloc(ctl, anzr));
+    CLB_RETURN_IF(need.alloc(ctl, 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(need.ptr, 0, 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    const BatchRows br{stk.rpair.ptr, stk.pf.ptr};
+    CLB_RETURN_IF(learned_caps(ctl, stk.As, stk.Bs, av, bv, sizer, margin_log2, slack, t, &br, work.ptr, cap.ptr));
+    // the slots the capture form gives these capacities (16-byte groups)
+    slot_need_kernel<<<std::max<unsigned>(1, std::min<uint64_t>((anzr + 255) / 256, ctl->sm_count * 8)), 256, 0,
+                       ctl->stream>>>(cap.ptr, anzr, ~0ull, (unsigned long long *)need.ptr);
     CLB_CHECK_LAUNCH();
-    {
-        ProfScope ps(ctl, "batch_stack");
-        stack_kernel<<<dim3(stack_grid_x(ctl, amax, count), count), CAT_NT, 0, ctl->stream>>>(
-            dda.ptr, arpt.ptr, arws.ptr, acls.ptr, rnc.ptr, anzr, annz);
-        stack_kernel<<<dim3(stack_grid_x(ctl, bmax, count), count), CAT_NT, 0, ctl->stream>>>(
-            ddb.ptr, brpt.ptr, brws.ptr, bcls.ptr, nullptr, bnzr, bnnz);
-        ctl->launches += 2;
-        CLB_CHECK_LAUNCH();
-    }
-    const clb_dcsr As{arows, brows, annz, anzr, arpt.ptr, arws.ptr, acls.ptr};
-    const clb_dcsr Bs{brows, bcols, bnnz, bnzr, brpt.ptr, brws.ptr, bcls.ptr};
-    CLB_RETURN_IF(validate_spgemm(As, Bs));
-    t.row_ncols = rnc.ptr;
-    return spgemm_esc_capture(ctl, As, Bs, t, slot_capacity, first.ptr, rbase.ptr, count, c_rpt, c_rows, c_cols,
-                              cols_capacity, result, flags);
+    CLB_RETURN_IF(read_scalars(ctl, need.ptr, slots_need, 1));
+    return CLB_SUCCESS;
 }
 
 int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,

@@ -526,10 +526,11 @@ __global__ void fit_slots_kernel(const uint64_t *__restrict__ slot_off, const ui
     if (__any_sync(0xFFFFFFFFu, cut) && lane_id() == 0) atomicOr(flags, CAPTURE_SLOTS_FULL);
 }
 
-// Overflowed rows (only rows cut by fit_slots_kernel can overflow upper-bound
-// slots) keep no columns.
+// Overflowed rows keep no columns and raise `bit` in the flag word.  With
+// upper-bound slots only rows cut by fit_slots_kernel can overflow; with
+// learned slots also a row that outgrew its slot when the arena was full.
 __global__ void drop_overflow_kernel(const uint32_t *__restrict__ ovf, uint64_t n, uint32_t *__restrict__ row_nnz,
-                                     uint32_t *__restrict__ flags) {
+                                     uint32_t *__restrict__ flags, uint32_t bit) {
     bool any = false;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         if (ovf[i]) {
@@ -537,7 +538,7 @@ __global__ void drop_overflow_kernel(const uint32_t *__restrict__ ovf, uint64_t 
             any = true;
         }
     }
-    if (__any_sync(0xFFFFFFFFu, any) && lane_id() == 0) atomicOr(flags, CAPTURE_SLOTS_FULL);
+    if (__any_sync(0xFFFFFFFFu, any) && lane_id() == 0) atomicOr(flags, bit);
 }
 
 // C.rpt / C.rows with sizes read on the device (nzr = *d_nzr, nnz = *d_nnz):
@@ -577,11 +578,14 @@ __global__ void capture_bounds_kernel(const uint32_t *__restrict__ pos, const ui
     }
 }
 
-// Compaction into the caller's column buffer; rows past its capacity are
-// not written and flag the call.
+// Compaction into the caller's column buffer (from the row's slot, or from
+// the spill arena for spilled rows: spill[i] != ~0); rows past its capacity
+// are not written and flag the call.
 __global__ void compact_capture_kernel(const uint32_t *__restrict__ row_nnz, const uint64_t *__restrict__ slot_off,
-                                       const uint64_t *__restrict__ off, const uint32_t *__restrict__ pre, uint64_t n,
-                                       uint64_t cols_cap, uint32_t *__restrict__ ccols, uint32_t *__restrict__ flags) {
+                                       const uint64_t *__restrict__ off, const uint32_t *__restrict__ pre,
+                                       const uint64_t *__restrict__ spill, const uint32_t *__restrict__ arena,
+                                       uint64_t n, uint64_t cols_cap, uint32_t *__restrict__ ccols,
+                                       uint32_t *__restrict__ flags) {
     const uint32_t lane = lane_id();
     const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
     for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); i < n; i += nw) {
@@ -591,7 +595,8 @@ __global__ void compact_capture_kernel(const uint32_t *__restrict__ row_nnz, con
             if (lane == 0) atomicOr(flags, CAPTURE_COLS_FULL);
             continue;
         }
-        warp_copy_aligned_src(pre + slot_off[i], ccols + off[i], len);
+        const uint64_t sp = spill ? spill[i] : ~0ull;
+        warp_copy_aligned_src(sp != ~0ull ? arena + sp : pre + slot_off[i], ccols + off[i], len);
     }
 }
 
@@ -605,7 +610,7 @@ __global__ void capture_status_kernel(const uint32_t *__restrict__ status, uint3
 int spgemm_esc_capture(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const Tuning &t,
                        uint64_t slot_capacity, const uint64_t *first, const uint32_t *row_base, uint32_t count,
                        uint64_t *c_rpt, uint32_t *c_rows, uint32_t *c_cols, uint64_t cols_capacity,
-                       uint64_t *d_result, uint32_t *d_flags) {
+                       uint64_t *d_result, uint32_t *d_flags, const CaptureLearned *learned) {
     const uint64_t n = A.nzr;
     const AView a{A.rpt, A.rows, A.cols, A.nzr};
     BRows b;
@@ -628,10 +633,17 @@ int spgemm_esc_capture(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     CLB_TRY_CUDA(cudaMemsetAsync(scal.ptr, 0, 8 * sizeof(uint64_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     CLB_TRY_CUDA(cudaMemsetAsync(row_nnz.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
     CLB_TRY_CUDA(cudaMemsetAsync(ovf.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
-    CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, scal.ptr + 6));
-    upper_bound_cap_rows_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(work.ptr, n, B.ncols, t.row_ncols, cap.ptr);
-    ctl->launches += 1;
-    CLB_CHECK_LAUNCH();
+    if (learned) {
+        // learned slots for the rows over t.bitmap_min products, exact below
+        CLB_RETURN_IF(learned_caps(ctl, A, B, a, b, learned->sizer, learned->margin_log2, learned->slack, t,
+                                   &learned->batch, work.ptr, cap.ptr));
+    } else {
+        CLB_RETURN_IF(launch_workload(ctl, a, b, work.ptr, scal.ptr + 6));
+        upper_bound_cap_rows_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(work.ptr, n, B.ncols, t.row_ncols,
+                                                                               cap.ptr);
+        ctl->launches += 1;
+        CLB_CHECK_LAUNCH();
+    }
     CLB_RETURN_IF(launch_binning(ctl, work.ptr, work.ptr, n, B.ncols, info.ptr, list.ptr, flags.ptr, t));
     CLB_RETURN_IF(scan_u32_inplace(ctl, flags.ptr, n, scal.ptr + 0));  // C row positions, nzr
     slot_sizes_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(cap.ptr, n, capp.ptr,
@@ -645,10 +657,24 @@ int spgemm_esc_capture(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     RowOut num{row_nnz.ptr, slot_off.ptr, cap.ptr, ovf.ptr, pre.ptr, ctl->d_status};
     num.row_ncols = t.row_ncols;
     num.row_products = work.ptr;
+    // learned slots: a bitmap row over its slot reserves its exact count in
+    // the caller-sized spill arena (the cursor is cleared with scal)
+    Temp<uint64_t> spill;
+    Temp<uint32_t> arena;
+    if (learned) {
+        CLB_RETURN_IF(spill.alloc(ctl, n));
+        CLB_RETURN_IF(arena.alloc(ctl, learned->arena_capacity + 4));
+        CLB_TRY_CUDA(cudaMemsetAsync(spill.ptr, 0xFF, n * 8, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+        num.spill = spill.ptr;
+        num.arena = arena.ptr;
+        num.arena_cursor = (unsigned long long *)(scal.ptr + 3);
+        num.arena_cap = learned->arena_capacity;
+    }
     // every bin is launched (no host read of the bin sizes); empty ones exit at once
     CLB_RETURN_IF(launch_esc_accumulators(ctl, bl, a, b, num, work.ptr, n, nullptr));
     CLB_RETURN_IF(launch_accumulators_subset(ctl, bl, a, b, num, B.ncols, n, /*hash_bins=*/false, t, nullptr));
-    drop_overflow_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, n, row_nnz.ptr, d_flags);
+    drop_overflow_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(ovf.ptr, n, row_nnz.ptr, d_flags,
+                                                                    learned ? CAPTURE_ROW_OVERFLOW : CAPTURE_SLOTS_FULL);
     ctl->launches += 1;
     CLB_CHECK_LAUNCH();
     CLB_RETURN_IF(scan_u32_to_u64(ctl, row_nnz.ptr, off.ptr, n, scal.ptr + 5));  // C row offsets, nnz
@@ -658,7 +684,7 @@ int spgemm_esc_capture(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     capture_bounds_kernel<<<(count + 256) / 256, 256, 0, ctl->stream>>>(flags.ptr, off.ptr, n, first, count,
                                                                         scal.ptr + 0, scal.ptr + 5, d_result + 2);
     compact_capture_kernel<<<grid_for(ctl, n * 32, 32), 256, 0, ctl->stream>>>(
-        row_nnz.ptr, slot_off.ptr, off.ptr, pre.ptr, n, cols_capacity, c_cols, d_flags);
+        row_nnz.ptr, slot_off.ptr, off.ptr, pre.ptr, spill.ptr, arena.ptr, n, cols_capacity, c_cols, d_flags);
     capture_status_kernel<<<1, 32, 0, ctl->stream>>>(ctl->d_status, d_flags);
     ctl->launches += 4;
     CLB_CHECK_LAUNCH();

@@ -2,9 +2,10 @@
 from .ops import (kronecker_product, matrix_multiplication, matrix_multiplication_hash, reduce, submatrix, transpose,
                   workload)
 from .sizing import RowSizer, matrix_multiplication_learned, row_features, row_nnz
-from .batched import autotune, matrix_multiplication_batched, matrix_multiplication_tuned, tuning
+from .batched import (autotune, matrix_multiplication_batched, matrix_multiplication_batched_learned,
+                      matrix_multiplication_tuned, tuning)
 
 __all__ = ["matrix_multiplication_hash", "matrix_multiplication", "kronecker_product", "transpose", "workload",
            "submatrix", "reduce",
            "matrix_multiplication_learned", "RowSizer", "row_features", "row_nnz", "matrix_multiplication_batched",
-           "matrix_multiplication_tuned", "autotune", "tuning"]
+           "matrix_multiplication_batched_learned", "matrix_multiplication_tuned", "autotune", "tuning"]

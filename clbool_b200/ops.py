@@ -208,6 +208,20 @@ def csr_matrix_addition(controls: Controls, c: matrix_csr | None, a: matrix_csr,
     return res if c is None else c._assign(res)
 
 
+def csr_matrix_addition_batched(controls: Controls, pairs) -> list[matrix_csr]:
+    """[A_k + B_k for (A_k, B_k) in pairs] (CSR, boolean) in one set of
+    launches (clb_csr_add_batched)."""
+    pairs = list(pairs)
+    n = len(pairs)
+    if n == 0:
+        return []
+    A, B, out = (clb_csr * n)(), (clb_csr * n)(), (clb_csr * n)()
+    for k, (a, b) in enumerate(pairs):
+        A[k], B[k] = a.c_struct(), b.c_struct()
+    check(_require("clb_csr_add_batched")(controls.handle, n, A, B, out), "csr::matrix_addition_batched")
+    return [matrix_csr.adopt(controls, out[k]) for k in range(n)]
+
+
 def kronecker_product(controls: Controls, matrix_c: matrix_dcsr | None, matrix_a: matrix_dcsr,
                       matrix_b: matrix_dcsr) -> matrix_dcsr:
     out = clb_dcsr()

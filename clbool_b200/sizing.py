@@ -24,7 +24,10 @@ from .core import ClBoolException, Controls, DeviceBuffer, check, matrix_dcsr
 
 NUM_FEATURES = 6
 FEATURE_SCALE = 1.0 / 16.0
+# Trained on R-MAT A*A (scales 14-19); and on R-MAT plus power-law, uniform
+# and closure-step products (for workloads whose rows collide less).
 DEFAULT_CHECKPOINT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "sizer_rmat.npz")
+MIXED_CHECKPOINT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "sizer_mixed.npz")
 # Capacity = predicted size * 2^margin_log2 + slack (clamped to the exact bound).
 DEFAULT_MARGIN_LOG2 = 0.25
 DEFAULT_SLACK = 8.0

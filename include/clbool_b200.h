@@ -237,6 +237,15 @@ CLB_API int clb_coo_add(clb_controls *ctl, const clb_coo *a, const clb_coo *b, c
 
 /* csr::matrix_addition (src/csr/csr.hpp:12, csr_addition.cpp:26-168). */
 CLB_API int clb_csr_add(clb_controls *ctl, const clb_csr *a, const clb_csr *b, clb_csr *c);
+/* No counterpart in the reference, which adds one pair per call
+ * (src/csr/csr.hpp:12): c[k] = a[k] + b[k] for k < count in one set of
+ * launches.  The pairs' rows are stacked (row pointers shifted, columns
+ * copied), one csr::matrix_addition runs over the stack (merge path, or the
+ * insertion path when one side of the stack is much sparser) and its rows
+ * are cut back into the pairs.  Each c[k] owns its buffers; a pair whose
+ * shapes differ fails the call with CLB_INVALID_ARGUMENT before any device
+ * work. */
+CLB_API int clb_csr_add_batched(clb_controls *ctl, uint32_t count, const clb_csr *a, const clb_csr *b, clb_csr *c);
 
 /* dcsr::kronecker_product (src/dcsr/dcsr.hpp:38-41,
  * dcsr_kronecker_product.cpp:5-64): C row (ia, ib) = A.rows[ia]*B.nrows +
@@ -331,6 +340,18 @@ CLB_API int clb_dcsr_spgemm_tuned(clb_controls *ctl, const clb_dcsr *a, const cl
  * owns its buffers.  stats (optional) covers the whole batch. */
 CLB_API int clb_dcsr_spgemm_batched(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                     clb_dcsr *c, const clb_spgemm_tuning *tuning, clb_spgemm_stats *stats);
+/* The learned-sized batched product (no counterpart in the reference): the
+ * pairs are stacked as in clb_dcsr_spgemm_batched, and the stack is
+ * multiplied by the learned single pass of clb_dcsr_spgemm_learned: row
+ * features relative to each row's own pair (row position in the pair's A,
+ * density of the pair's B), predicted slots for the rows over
+ * tuning->bitmap_min products (exact bounds below), the spill arena for rows
+ * over their slot, and the exact two-pass form for the rows that outgrow
+ * both.  The result never depends on the predictor. */
+CLB_API int clb_dcsr_spgemm_batched_learned(clb_controls *ctl, uint32_t count, const clb_dcsr *a,
+                                            const clb_dcsr *b, clb_dcsr *c, const clb_sizer *sizer,
+                                            float margin_log2, float slack, const clb_spgemm_tuning *tuning,
+                                            clb_spgemm_stats *stats);
 /* Times the batched product under every candidate tuning (32: form x
  * bitmap_min x bitmap_threads x warp_max x small_lanes; twice that with both
  * wide_rows settings when a pair has more than 2^20 columns) on the given
@@ -382,7 +403,9 @@ CLB_API int clb_dcsr_spgemm_to_host(clb_controls *ctl, const clb_dcsr *a, const 
  *                  c_cols[j_k, j_k+1);
  *   flags          device u32, 0 when C is complete; bit 0: slot capacity
  *                  too small (rows left empty), bit 1: cols_capacity too
- *                  small (rows not written), bit 2: a device check failed.
+ *                  small (rows not written), bit 2: a device check failed,
+ *                  bit 3 (learned form only): a row outgrew its slot and
+ *                  the spill arena (left empty).
  * Returns once the work is enqueued (no synchronisation). */
 CLB_API int clb_dcsr_spgemm_batched_capture(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                             const clb_spgemm_tuning *tuning, uint64_t slot_capacity,
@@ -392,6 +415,30 @@ CLB_API int clb_dcsr_spgemm_batched_capture(clb_controls *ctl, uint32_t count, c
  * (runs the workload pass and synchronises; call it outside a capture). */
 CLB_API int clb_spgemm_batched_plan(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                     uint64_t *rows_need, uint64_t *slots_need);
+/* The host-sync-free batched product with learned slots (no counterpart in
+ * the reference): as clb_dcsr_spgemm_batched_capture, but the rows over
+ * tuning->bitmap_min products get the slots the predictor gives them (as in
+ * clb_dcsr_spgemm_batched_learned), and a row whose exact count outgrows its
+ * slot reserves it in a spill arena of arena_capacity entries (a temporary
+ * of the call) in the same pass.  A row that finds no room there is left
+ * empty and raises bit 3 of *flags (the caller then recomputes the batch by
+ * an exact form: clb_dcsr_spgemm_batched); cols_capacity must hold C, i.e.
+ * the slots plus the spilled rows (slot_capacity + arena_capacity always
+ * suffices).  The call can be recorded into a CUDA graph like the
+ * upper-bound form. */
+CLB_API int clb_dcsr_spgemm_batched_capture_learned(clb_controls *ctl, uint32_t count, const clb_dcsr *a,
+                                                    const clb_dcsr *b, const clb_sizer *sizer, float margin_log2,
+                                                    float slack, const clb_spgemm_tuning *tuning,
+                                                    uint64_t slot_capacity, uint64_t arena_capacity,
+                                                    uint64_t *c_rpt, uint32_t *c_rows, uint32_t *c_cols,
+                                                    uint64_t cols_capacity, uint64_t *result, uint32_t *flags);
+/* Sizes for clb_dcsr_spgemm_batched_capture_learned on the pairs' current
+ * contents: stored rows and the learned slots (runs the feature and
+ * prediction passes and synchronises; call it outside a capture). */
+CLB_API int clb_spgemm_batched_plan_learned(clb_controls *ctl, uint32_t count, const clb_dcsr *a,
+                                            const clb_dcsr *b, const clb_sizer *sizer, float margin_log2,
+                                            float slack, const clb_spgemm_tuning *tuning, uint64_t *rows_need,
+                                            uint64_t *slots_need);
 
 /* Products per A row (count_workload, dcsr_matrix_multiplication.cpp:388-404):
  * workload has a->nzr entries in device memory; *total = their sum. */

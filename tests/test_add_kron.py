@@ -178,15 +178,17 @@ def _labels(n, deg, count, seed):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("method", ["fused", "batched"])
-def test_closure_fixpoint_matches_oracle(controls, method):
+@pytest.mark.parametrize("method,learned", [("fused", False), ("batched", False), ("fused", True),
+                                            ("batched", True)])
+def test_closure_fixpoint_matches_oracle(controls, method, learned):
     """Three uniform label matrices (n = 2^9, average degree 0.6 so the
     closure stays sparse): every iteration's nnz and the fixpoint equal the
-    oracle's, by both iteration methods."""
-    from clbool_b200 import cfpq
+    oracle's, by both iteration methods, with and without learned sizing."""
+    from clbool_b200 import cfpq, sizing
     labels = _labels(1 << 9, 0.6, 3, seed=11)
     want, want_hist = O.closure(labels)
-    C, hist = cfpq.closure(controls, [to_device(controls, L) for L in labels], method=method)
+    sizer = sizing.RowSizer.load(controls) if learned else None
+    C, hist = cfpq.closure(controls, [to_device(controls, L) for L in labels], method=method, sizer=sizer)
     assert [h["nnz"] for h in hist] == want_hist
     assert hist[-1]["stop"] == "fixpoint"
     assert_dcsr_equal(from_device(controls, C), want, "closure")
@@ -205,3 +207,45 @@ def test_closure_bounds(controls):
     assert_dcsr_equal(from_device(controls, C), want, "closure, 2 iterations")
     C2, hist2 = cfpq.closure(controls, [to_device(controls, L) for L in labels], max_products=1)
     assert hist2[-1]["stop"] == "max_products" and len(hist2) == 1
+
+
+def _csr_of(m: O.Dcsr) -> O.Csr:
+    return O.dcsr_to_csr(m)
+
+
+def test_addition_csr_batched(controls):
+    """Many independent additions in one call (no counterpart in the
+    reference, which adds one pair per call): pairs of different shapes,
+    power-law and R-MAT operands, a much sparser side (the stack takes the
+    insertion path when most of it is), empty operands on either side, a pair
+    of two empty operands; each sum equal to the oracle's."""
+    import clbool_b200 as cb
+    from clbool_b200 import gen
+    pairs = []
+    for k, n in enumerate((700, 3000, 12000)):
+        ra, ca = gen.power_law_rows(n, n + 5, 2.1, 6.0, 512, seed=300 + 2 * k)
+        rb, cb_ = gen.power_law_rows(n, n + 5, 2.1, 6.0, 512, seed=301 + 2 * k)
+        pairs.append((O.coo_to_csr(O.Coo(n, n + 5, ra, ca)), O.coo_to_csr(O.Coo(n, n + 5, rb, cb_))))
+    r, c = gen.rmat(12, seed=9)
+    g = O.coo_to_dcsr(O.Coo(1 << 12, 1 << 12, r, c))
+    pairs.append((_csr_of(O.spgemm(g, g)), _csr_of(g)))
+    e = O.Csr(40, 50, np.zeros(41, np.uint64), np.zeros(0, np.uint32))
+    ra, ca = O.generate_coo_pairs(40 * 3, 40)
+    f = O.coo_to_csr(O.Coo(40, 50, ra, ca))
+    pairs += [(e, f), (f, e), (e, e)]
+
+    def dev(m):
+        return cb.csr_from_cpu(controls, cb.matrix_csr_cpu(m.rpt, m.cols, m.nrows, m.ncols))
+
+    for order in (pairs, pairs[::-1]):
+        got = cb.csr.matrix_addition_batched(controls, [(dev(a), dev(b)) for a, b in order])
+        for k, ((a, b), s_) in enumerate(zip(order, got)):
+            want = O.csr_add(a, b)
+            assert s_.nrows() == a.nrows and s_.ncols() == a.ncols and s_.nnz() == len(want.cols), k
+            if len(want.cols):
+                h = cb.matrix_csr_from_gpu(controls, s_)
+                assert np.array_equal(h.rpt, want.rpt) and np.array_equal(h.cols, want.cols), k
+    assert cb.csr.matrix_addition_batched(controls, []) == []
+    with pytest.raises(cb.ClBoolException) as ex:
+        cb.csr.matrix_addition_batched(controls, [(dev(pairs[0][0]), dev(pairs[0][1])), (dev(f), dev(pairs[0][0]))])
+    assert ex.value.status_name == "CLBOOL_INVALID_ARGUMENT"

@@ -1,14 +1,19 @@
 """The headline workload at its full size: R-MAT scale 20 (edge factor 16,
 a/b/c/d = .57/.19/.19/.05, seed 1), C = A*A -- 2.09e10 products and 9.7e9
-output columns, beyond what the oracle computes in a test.  The forms are
-checked through properties that hold at any size:
+output columns, beyond what the oracle computes in a test -- and its second
+operation, the CSR addition C + A.  The forms are checked through
+properties that hold at any size:
   * the learned single pass, the ESC single pass and the exact two-pass form
     (dcsr::matrix_multiplication_hash, src/dcsr/dcsr.hpp:32-36) give
     bit-identical C, compared on the device;
   * C's row lengths equal the symbolic pass's counts (clb_dcsr_row_nnz);
   * every row of C is strictly increasing (sorted, no duplicates);
-  * 256 seeded rows of A against the full right operand equal the oracle's
-    rows of the product.
+  * 640 seeded rows of A against the full right operand equal the oracle's
+    rows of the product: 512 drawn in proportion to their products (the
+    bitmap rows carry 98.7% of them) and 128 uniformly;
+  * C + A (csr::matrix_addition, src/csr/csr_addition.cpp:26-168): every
+    row strictly increasing, nnz(C + A) >= nnz(C), and the same 640 rows
+    equal the oracle's union of the rows of C and A.
 Device memory: C is 39 GB; the peak (two-pass C held while the ESC form
 runs with its upper-bound slots) is about 160 GB of the B200's 180 GB."""
 import ctypes
@@ -17,34 +22,9 @@ import numpy as np
 import pytest
 
 import oracle as O
+from util import assert_rows_match, rows_strictly_increasing, same_on_device, sub_rows, weighted_pick
 
 SCALE = 20
-CHUNK = 1 << 28  # elements per device comparison
-
-
-class _Cai:
-    """A device array seen by torch without a copy (__cuda_array_interface__)."""
-
-    def __init__(self, ptr: int, n: int, dtype):
-        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": np.dtype(dtype).str,
-                                         "data": (int(ptr), False), "version": 3}
-
-
-def _view(buf, n, dtype):
-    """Signed view (torch compares signed integers; u32 columns < 2^31 and u64
-    offsets < 2^63 keep their order, and equality is bitwise either way)."""
-    import torch
-    signed = {np.dtype(np.uint32): np.int32, np.dtype(np.uint64): np.int64}[np.dtype(dtype)]
-    return torch.as_tensor(_Cai(buf.ptr, n, signed), device="cuda")
-
-
-def _same_on_device(x, y, what):
-    assert (x.nnz(), x.nzr()) == (y.nnz(), y.nzr()), what
-    for get, n, dt in ((lambda m: m.rpt_gpu(), x.nzr() + 1, np.uint64), (lambda m: m.rows_gpu(), x.nzr(), np.uint32),
-                       (lambda m: m.cols_gpu(), x.nnz(), np.uint32)):
-        a, b = _view(get(x), n, dt), _view(get(y), n, dt)
-        for s in range(0, n, CHUNK):
-            assert bool((a[s:s + CHUNK] == b[s:s + CHUNK]).all()), f"{what}: differs in [{s}, {s + CHUNK})"
 
 
 @pytest.fixture(scope="module")
@@ -55,10 +35,18 @@ def rmat20():
     return O.coo_to_dcsr(O.Coo(n, n, r, c))
 
 
-@pytest.mark.gpu
-def test_rmat20_forms_identical_and_sound(controls, rmat20):
-    import torch
+@pytest.fixture(scope="module")
+def sample20(rmat20):
+    """640 stored rows of A (512 by products, 128 uniform) and the oracle's
+    rows of A*A for them."""
+    a = rmat20
+    pick = weighted_pick(O.workload(a, a), 512, seed=11, uniform=128)
+    sa = sub_rows(a, pick)
+    return sa, O.spgemm(sa, a)
 
+
+@pytest.mark.gpu
+def test_rmat20_forms_identical_and_sound(controls, rmat20, sample20):
     import clbool_b200 as cb
     from clbool_b200 import sizing
     from util import to_device
@@ -72,11 +60,11 @@ def test_rmat20_forms_identical_and_sound(controls, rmat20):
     sizer = sizing.RowSizer.load(controls)
     C1 = sizing.matrix_multiplication_learned(controls, None, A, A, sizer)
     controls.sync()
-    _same_on_device(C1, C2, "learned vs two-pass")
+    same_on_device(C1, C2, "learned vs two-pass")
     del C1
     C3 = cb.dcsr.matrix_multiplication(controls, None, A, A)
     controls.sync()
-    _same_on_device(C3, C2, "ESC vs two-pass")
+    same_on_device(C3, C2, "ESC vs two-pass")
     del C3
 
     # row lengths = the symbolic counts
@@ -89,27 +77,38 @@ def test_rmat20_forms_identical_and_sound(controls, rmat20):
     lens[pos] = np.diff(rpt)
     assert np.array_equal(lens, sym)
 
-    # strictly increasing inside every row: a non-increase may only sit at a row start
-    cols = _view(C2.cols_gpu(), C2.nnz(), np.uint32)
-    starts = torch.as_tensor(rpt[1:-1], device="cuda")
-    for s in range(0, C2.nnz() - 1, CHUNK):
-        e = min(s + CHUNK + 1, C2.nnz())
-        bad = torch.nonzero(cols[s + 1:e] <= cols[s:e - 1]).flatten() + (s + 1)
-        assert bool(torch.isin(bad, starts).all()), "a row of C is not strictly increasing"
+    rows_strictly_increasing(C2, rpt, "C = A*A")
+    # the sampled rows against the oracle (heavy rows weighted in)
+    _, want = sample20
+    assert_rows_match(controls, C2, want, "C = A*A")
 
-    # 256 seeded rows against the oracle
-    rng = np.random.default_rng(11)
-    pick = np.sort(rng.choice(len(a.rows), 256, replace=False))
-    lens_a = np.diff(a.rpt.astype(np.int64))
-    sub_rpt = np.concatenate([[0], np.cumsum(lens_a[pick])]).astype(np.uint64)
-    sub_cols = np.concatenate([a.cols[int(a.rpt[i]):int(a.rpt[i + 1])] for i in pick])
-    want = O.spgemm(O.Dcsr(a.nrows, a.ncols, sub_rpt, a.rows[pick], sub_cols), a)
-    got_rows = np.searchsorted(crows, want.rows)
-    assert np.array_equal(crows[got_rows], want.rows)
+
+@pytest.mark.gpu
+def test_rmat20_csr_addition_c_plus_a(controls, rmat20, sample20):
+    import clbool_b200 as cb
+    from clbool_b200 import sizing
+    from util import to_device
+
+    a = rmat20
+    n = a.nrows
+    A = to_device(controls, a)
+    C = sizing.matrix_multiplication_learned(controls, None, A, A, sizing.RowSizer.load(controls))
+    Cc, Ac = cb.dcsr_to_csr(controls, C), cb.dcsr_to_csr(controls, A)
+    nnz_c = C.nnz()
+    del C
+    S = cb.csr.matrix_addition(controls, None, Cc, Ac)
+    controls.sync()
+    assert S.nnz() >= nnz_c and S.nnz() <= nnz_c + len(a.cols)
+    srpt = S.rpt_gpu().to_host(n + 1).astype(np.int64)
+    rows_strictly_increasing(S, srpt, "C + A")
+
+    # sampled rows: the oracle's union of the row of A*A and the row of A
+    sa, want_c = sample20
+    want = O.csr_add(O.dcsr_to_csr(want_c), O.dcsr_to_csr(sa))
     lib = cb.lib
-    for k, g in enumerate(got_rows):
-        lo, hi = int(rpt[g]), int(rpt[g + 1])
+    for r in sa.rows:
+        lo, hi = int(srpt[r]), int(srpt[r + 1])
         seg = np.empty(hi - lo, np.uint32)
         assert lib.clb_memcpy_d2h(controls.handle, seg.ctypes.data_as(ctypes.c_void_p),
-                                  ctypes.c_void_p(C2.cols_gpu().ptr + 4 * lo), 4 * (hi - lo)) == 0
-        assert np.array_equal(seg, want.cols[int(want.rpt[k]):int(want.rpt[k + 1])]), f"row {want.rows[k]}"
+                                  ctypes.c_void_p(S.cols_gpu().ptr + 4 * lo), 4 * (hi - lo)) == 0
+        assert np.array_equal(seg, want.cols[int(want.rpt[r]):int(want.rpt[r + 1])]), f"C + A row {r}"
