@@ -3,14 +3,17 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--scale 20] [--form two_pass|learned]
 
-One step = one dcsr::matrix_multiplication_hash of the synthetic R-MAT
-scale-20 graph by itself (2^20 vertices, edge factor 16, a/b/c/d =
-.57/.19/.19/.05, duplicates removed, self-loops kept), producing C on the GPU.
-`value` is products/s with A resident in HBM; `e2e` is the same metric
-through the public API with host buffers (pinned H2D of A, D2H of all of C
-inside the timed region).  With N > 1 ranks (torchrun) every rank computes
-the C rows of its share of A's rows (balanced by products) against its own
-copy of A; no collective touches the data path.
+One step = one product C = A*A of the synthetic R-MAT scale-20 graph by
+itself (2^20 vertices, edge factor 16, a/b/c/d = .57/.19/.19/.05,
+duplicates removed, self-loops kept) by the learned-sized single pass
+(default; the exact two-pass dcsr::matrix_multiplication_hash is timed beside
+it), producing C on the GPU.  `value` is products/s with A resident in HBM;
+`e2e` is the same metric through the public API with host buffers (pinned
+H2D of A, D2H of all of C inside the timed region).  With N > 1 ranks
+(torchrun) rank 0 generates A and broadcasts it into every rank's HBM with
+NCCL (clbool_b200.sharded), and every rank computes the C rows of its share
+of A's rows (balanced by products) against its own copy; no collective
+touches the timed data path.
 
 `--impl reference` times the reference's own CPU implementation
 (coo_utils::matrix_multiplication_cpu, compiled from the reference sources
@@ -129,17 +132,6 @@ def rmat_config(scale: int, nnz_a: int, products: int, world: int, row_fraction:
             "nnz_A": nnz_a, "products": products, "parallelism": f"rows{world}"}
 
 
-def shard_rows(rpt_work: np.ndarray, world: int, rank: int) -> tuple[int, int]:
-    """Contiguous block of A's stored rows with about 1/world of the products."""
-    if world == 1:
-        return 0, rpt_work.size
-    cum = np.cumsum(rpt_work, dtype=np.float64)
-    tot = cum[-1] if cum.size else 0.0
-    lo = 0 if rank == 0 else int(np.searchsorted(cum, tot * rank / world, side="left")) + 1
-    hi = rpt_work.size if rank == world - 1 else int(np.searchsorted(cum, tot * (rank + 1) / world, side="left")) + 1
-    return min(lo, rpt_work.size), min(hi, rpt_work.size)
-
-
 def bin_of(p: np.ndarray, bound: np.ndarray) -> np.ndarray:
     """The accumulator bin of every row under the default tuning (mirrors
     bin_of in spgemm_kernels.cuh)."""
@@ -180,12 +172,13 @@ def algorithmic_bytes(kernel: str, a_len: np.ndarray, work: np.ndarray, c_len: n
 
 
 # --------------------------------------------------------------- our arm --
-def make_mxm(form: str, ctl, cb, sizer_path: str):
+def make_mxm(form: str, ctl, cb, sizer_path: str, tune=None):
     """The public call one step makes: (A, B, stats) -> C."""
     if form == "learned":
         from clbool_b200 import sizing
         sizer = sizing.RowSizer.load(ctl, sizer_path)
-        return lambda A, B, stats=None: sizing.matrix_multiplication_learned(ctl, None, A, B, sizer, stats=stats)
+        return lambda A, B, stats=None: sizing.matrix_multiplication_learned(ctl, None, A, B, sizer, stats=stats,
+                                                                             tune=tune)
     if form == "esc":
         return lambda A, B, stats=None: cb.dcsr.matrix_multiplication(ctl, None, A, B, stats=stats)
     return lambda A, B, stats=None: cb.dcsr.matrix_multiplication_hash(ctl, None, A, B, stats=stats)
@@ -257,11 +250,21 @@ def learned_bounds(ctl, cb, A, B, sizer_path: str, work: np.ndarray, ncols: int)
 
 def run_ours(args, rank: int, world: int, dist) -> dict | None:
     import clbool_b200 as cb
+    from clbool_b200 import sharded
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     ctl = cb.create_controls(0, dev)
-    n, rpt, rows, cols = rmat_a(args.scale)
+    n = 1 << args.scale
+    # rank 0 generates A; every other rank receives it by an NCCL broadcast
+    # into its own HBM (A is both operands: B = A)
+    A0 = None
+    if rank == 0:
+        _, rpt, rows, cols = rmat_a(args.scale)
+        A0 = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(rpt, rows, cols), n)
+    A_full = sharded.broadcast_dcsr(ctl, A0, 0) if world > 1 else A0
+    if rank != 0:
+        h = cb.matrix_dcsr_from_gpu(ctl, A_full)  # host copy: row sampling and the end-to-end leg
+        rpt, rows, cols = h.rpt.astype(np.uint64), h.rows, h.cols
     nnz_a = cols.size
-    A_full = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(rpt, rows, cols), n)
     work_buf, total_products = cb.dcsr.workload(ctl, A_full, A_full)
     work = work_buf.to_host(rows.size).astype(np.int64)
     # left operand: A itself, or (for profiling) a seeded sample of its rows
@@ -270,7 +273,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         pick = _row_sample(rows.size, args.row_fraction, seed=3)
         lrpt, lrows, lcols = _sub_dcsr(rpt, rows, cols, pick)
         work = work[pick]
-    lo, hi = shard_rows(work, world, rank)
+    lo, hi = sharded.partition(work, world)[rank]
     srpt = (lrpt[lo:hi + 1] - lrpt[lo]).astype(np.uint64)
     srows, scols = lrows[lo:hi], lcols[int(lrpt[lo]):int(lrpt[hi])]
     A = cb.matrix_dcsr_from_cpu(ctl, cb.matrix_dcsr_cpu(srpt, srows, scols), n) if hi > lo else \
@@ -368,7 +371,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         line["form_stats"] = {k: st.get(k) for k in ("capacity", "fallback_rows", "spilled_rows", "nzr", "nnz")}
     if compare is not None:
         line["compare"] = compare
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(n, rpt, rows, cols, work)
     return line
 
@@ -624,8 +627,11 @@ def run_batch(args) -> dict:
     st_l = {}
 
     def learned():
-        outs = cb.dcsr.matrix_multiplication_batched_learned(ctl, pairs, sizer, stats=st_l)
+        outs = cb.dcsr.matrix_multiplication_batched_learned(ctl, pairs, sizer, tune=best, stats=st_l)
         del outs
+
+    # the exact two-pass form under the autotuned accumulator settings
+    two_pass_best = cb.dcsr.tuning("two_pass", best.warp_max, best.bitmap_min, best.bitmap_threads, best.small_lanes)
 
     for _ in range(args.warmup):
         batched(best)()
@@ -634,6 +640,7 @@ def run_batch(args) -> dict:
     ms_best = _event_ms(stream, batched(best), args.steps)
     ms_default = _event_ms(stream, batched(default), args.steps)
     ms_learned = _event_ms(stream, learned, args.steps)
+    ms_two_pass_best = _event_ms(stream, batched(two_pass_best), args.steps)
     ms_seq = _event_ms(stream, sequential, max(1, args.steps // 2))
     batched(best)()
     # the host-sync-free batched form recorded once into a CUDA graph, replayed
@@ -674,7 +681,10 @@ def run_batch(args) -> dict:
             "autotuned": best.as_dict(), "default_ms": ms_default, "sequential_ms": ms_seq,
             "batched_over_sequential": ms_seq / ms_best,
             "learned_batched": {"ms": ms_learned, "products_per_s": products / (ms_learned / 1e3),
-                                "over_two_pass_batched": ms_default / ms_learned,
+                                "over_two_pass_batched_default": ms_default / ms_learned,
+                                "two_pass_batched_same_tuning_ms": ms_two_pass_best,
+                                "over_two_pass_batched_same_tuning": ms_two_pass_best / ms_learned,
+                                "tuning": best.as_dict(),
                                 "capacity": st_l.get("capacity"), "spilled_rows": st_l.get("spilled_rows"),
                                 "fallback_rows": st_l.get("fallback_rows"),
                                 "graph_replay_ms": ms_graph_l, "graph_slot_capacity": capl.slot_capacity,
@@ -982,8 +992,8 @@ def run_rmat21(args) -> dict:
     sizer = sizing.RowSizer.load(ctl, args.sizer)
     blocks = max(1, args.blocks)
     tot = {"products": 0, "nnz": 0, "capacity": 0, "spilled_rows": 0, "fallback_rows": 0, "ms": 0.0}
-    for k in range(blocks):
-        lo, hi = shard_rows(work, blocks, k)
+    from clbool_b200 import sharded
+    for k, (lo, hi) in enumerate(sharded.partition(work, blocks)):
         if hi <= lo:
             continue
         srpt = (rpt[lo:hi + 1] - rpt[lo]).astype(np.uint64)

@@ -141,6 +141,7 @@ _SIGS = {
     "clb_dcsr_spgemm_to_host": (C.c_int, [vp, P(clb_dcsr), P(clb_dcsr), vp, C.c_float, C.c_float,
                                           P(clb_spgemm_tuning), C.c_uint32, vp, vp, vp, C.c_uint64, C.c_uint64,
                                           P(C.c_uint64), P(C.c_uint64), P(clb_spgemm_stats)]),
+    "clb_dcsr_row_block": (C.c_int, [vp, P(clb_dcsr), C.c_uint64, C.c_uint64, P(clb_dcsr)]),
     "clb_graph_begin": (C.c_int, [vp]),
     "clb_graph_end": (C.c_int, [vp, P(vp)]),
     "clb_graph_launch": (C.c_int, [vp, vp]),

@@ -72,6 +72,49 @@ using namespace clb;
 
 extern "C" {
 
+int clb_dcsr_row_block(clb_controls *ctl, const clb_dcsr *a_, uint64_t lo, uint64_t hi, clb_dcsr *out) {
+    if (!ctl || !a_ || !out) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    const clb_dcsr A = *a_;
+    if (lo > hi || hi > A.nzr) return fail(CLB_INVALID_ARGUMENT, "row range [" + std::to_string(lo) + ", " +
+                                                                   std::to_string(hi) + ") outside the stored rows");
+    clb_dcsr C{};
+    C.nrows = A.nrows;
+    C.ncols = A.ncols;
+    if (hi == lo || A.nnz == 0) {
+        *out = C;
+        return CLB_SUCCESS;
+    }
+    DeviceGuard g(ctl);
+    uint64_t j[2];
+    CLB_TRY_CUDA(cudaMemcpyAsync(&j[0], A.rpt + lo, 8, cudaMemcpyDeviceToHost, ctl->stream), CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(&j[1], A.rpt + hi, 8, cudaMemcpyDeviceToHost, ctl->stream), CLB_READ_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    if (j[1] == j[0]) {
+        *out = C;
+        return CLB_SUCCESS;
+    }
+    const uint64_t n = hi - lo, nnz = j[1] - j[0];
+    Temp<uint64_t> rpt;
+    Temp<uint32_t> rows, cols;
+    CLB_RETURN_IF(rpt.alloc(ctl, n + 1));
+    CLB_RETURN_IF(rows.alloc(ctl, n));
+    CLB_RETURN_IF(cols.alloc(ctl, nnz));
+    rebase_rpt_kernel<<<grid_of(ctl, n + 1), 256, 0, ctl->stream>>>(A.rpt, lo, n, rpt.ptr);
+    CLB_CHECK_LAUNCH();
+    CLB_TRY_CUDA(cudaMemcpyAsync(rows.ptr, A.rows + lo, n * 4, cudaMemcpyDeviceToDevice, ctl->stream),
+                 CLB_COPY_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemcpyAsync(cols.ptr, A.cols + j[0], nnz * 4, cudaMemcpyDeviceToDevice, ctl->stream),
+                 CLB_COPY_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    C.nnz = nnz;
+    C.nzr = n;
+    C.rpt = rpt.release_ownership();
+    C.rows = rows.release_ownership();
+    C.cols = cols.release_ownership();
+    *out = C;
+    return CLB_SUCCESS;
+}
+
 int clb_dcsr_spgemm_to_host(clb_controls *ctl, const clb_dcsr *a_, const clb_dcsr *b_, const clb_sizer *sizer,
                             float margin_log2, float slack, const clb_spgemm_tuning *tuning, uint32_t blocks,
                             uint64_t *h_rpt, uint32_t *h_rows, uint32_t *h_cols, uint64_t rows_capacity,

@@ -381,6 +381,14 @@ CLB_API int clb_dcsr_spgemm_to_host(clb_controls *ctl, const clb_dcsr *a, const 
                                     uint64_t rows_capacity, uint64_t cols_capacity, uint64_t *nzr, uint64_t *nnz,
                                     clb_spgemm_stats *stats);
 
+/* No counterpart in the reference (a single-device library,
+ * src/core/controls.hpp:12-28): the stored rows [lo, hi) of A as a DCSR of
+ * A's shape that owns copies of them (row ids kept, row pointers rebased to
+ * 0) -- one rank's share of A when A's rows are split over GPUs.  An empty
+ * range gives an empty matrix; a range past nzr(A) is rejected with
+ * CLB_INVALID_ARGUMENT. */
+CLB_API int clb_dcsr_row_block(clb_controls *ctl, const clb_dcsr *a, uint64_t lo, uint64_t hi, clb_dcsr *out);
+
 /* Host-sync-free batched product (no counterpart in the reference): the
  * pairs are stacked as in clb_dcsr_spgemm_batched and multiplied by the
  * single-pass form into upper-bound slots, but every size comes from the
