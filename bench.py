@@ -833,13 +833,16 @@ def run_cfpq(args) -> dict:
     C2, _ = cfpq.closure(ctl, labels, max_iters=2)
     M = cfpq.union(ctl, [cfpq.identity(ctl, n)] + labels)
     best, _ = cb.dcsr.autotune(ctl, [(C2, M)])
+    best_b, _ = cb.dcsr.autotune(ctl, [(C2, L) for L in labels])  # the batched iteration's three products
     del C2
     from clbool_b200 import sizing
     sizer_path = args.sizer_mixed if os.path.exists(args.sizer_mixed) else args.sizer
     sizer = sizing.RowSizer.load(ctl, sizer_path)
     out["sizer"] = os.path.basename(sizer_path)
     for method, tune, sz in (("fused", None, None), ("fused_autotuned", best, None), ("fused_learned", None, sizer),
-                             ("batched", None, None), ("batched_learned", None, sizer)):
+                             ("fused_learned_autotuned", best, sizer), ("batched", None, None),
+                             ("batched_autotuned", best_b, None), ("batched_learned", None, sizer),
+                             ("batched_learned_autotuned", best_b, sizer)):
         m = "batched" if method.startswith("batched") else "fused"
         cfpq.closure(ctl, labels, max_iters=2, method=m, tune=tune, sizer=sz)  # warm-up
         torch.cuda.synchronize()

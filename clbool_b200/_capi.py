@@ -127,6 +127,8 @@ _SIGS = {
     "clb_dcsr_spgemm_batched_learned": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_dcsr), vp,
                                                   C.c_float, C.c_float, P(clb_spgemm_tuning),
                                                   P(clb_spgemm_stats)]),
+    "clb_dcsr_union": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_spgemm_tuning), P(clb_dcsr),
+                                 P(clb_spgemm_stats)]),
     "clb_spgemm_autotune": (C.c_int, [vp, C.c_uint32, P(clb_dcsr), P(clb_dcsr), P(clb_spgemm_tuning),
                                       P(clb_spgemm_tuning), P(C.c_double), C.c_uint32, P(C.c_uint32)]),
     # host-sync-free batched product and CUDA graphs

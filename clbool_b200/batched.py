@@ -103,6 +103,26 @@ def matrix_multiplication_batched_learned(controls: Controls, pairs, sizer, marg
     return [matrix_dcsr.adopt(controls, out[k]) for k in range(n)]
 
 
+def matrix_union(controls: Controls, mats, tune: clb_spgemm_tuning | None = None,
+                 stats: dict | None = None) -> matrix_dcsr:
+    """mats[0] v mats[1] v ... (boolean sum of DCSR matrices of one shape) in
+    one pass: a product with the matrices stacked row-wise, whose rows merge
+    the matrices' rows (clb_dcsr_union)."""
+    mats = list(mats)
+    n = len(mats)
+    if n == 0:
+        raise ClBoolException(12, "union of no matrices")
+    M = (clb_dcsr * n)()
+    for k, m in enumerate(mats):
+        M[k] = m.c_struct()
+    out, st = clb_dcsr(), clb_spgemm_stats()
+    check(lib.clb_dcsr_union(controls.handle, n, M, C.byref(tune) if tune else None, C.byref(out), C.byref(st)),
+          "matrix_union")
+    if stats is not None:
+        stats.update(st.as_dict())
+    return matrix_dcsr.adopt(controls, out)
+
+
 def autotune(controls: Controls, pairs, max_tried: int = 64):
     """(best tuning, [(tuning dict, ms), ...]) over the library's candidate tunings."""
     n, A, B, _keep = _arrays(list(pairs))

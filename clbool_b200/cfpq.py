@@ -9,9 +9,8 @@ Two equivalent iteration methods:
   "batched": the k products C_t L_i as ONE batched call
              (dcsr.matrix_multiplication_batched, or the learned-sized
              dcsr.matrix_multiplication_batched_learned when a sizer is
-             given), then the union C_t v P_1 v ... v P_k as a tree of
-             batched CSR additions (csr::matrix_addition over all pairs of a
-             level in one call: two calls for k = 3);
+             given), then the union C_t v P_1 v ... v P_k in one pass
+             (batched.matrix_union);
   "fused":   C_{t+1} = C_t M with M = I v L_1 v ... v L_k built once (the
              boolean semiring distributes: C v C L_1 v ... = C (I v L_1 v ...)),
              i.e. one product per iteration (learned-sized when a sizer is
@@ -28,23 +27,17 @@ import time
 
 import numpy as np
 
-from .batched import matrix_multiplication_batched, matrix_multiplication_batched_learned, matrix_multiplication_tuned
+from .batched import (matrix_multiplication_batched, matrix_multiplication_batched_learned,
+                      matrix_multiplication_tuned, matrix_union)
 from .core import Controls, matrix_dcsr, matrix_dcsr_cpu
-from .ops import csr_matrix_addition_batched, csr_to_dcsr, dcsr_to_csr, matrix_dcsr_from_cpu, workload
+from .ops import matrix_dcsr_from_cpu, workload
 
 
-def union(controls: Controls, mats: list[matrix_dcsr]) -> matrix_dcsr:
-    """Boolean sum of DCSR matrices of one shape: every operand converted to
-    CSR once, then a tree of batched CSR additions (each level's pairs in
-    one call), converted back to DCSR."""
-    level = [dcsr_to_csr(controls, m) for m in mats]
-    while len(level) > 1:
-        pairs = [(level[i], level[i + 1]) for i in range(0, len(level) - 1, 2)]
-        nxt = csr_matrix_addition_batched(controls, pairs)
-        if len(level) % 2:
-            nxt.append(level[-1])
-        level = nxt
-    return csr_to_dcsr(controls, level[0])
+def union(controls: Controls, mats: list[matrix_dcsr], tune=None) -> matrix_dcsr:
+    """Boolean sum of DCSR matrices of one shape in one pass
+    (batched.matrix_union: the SpGEMM accumulators merge every output row's
+    rows of the operands)."""
+    return matrix_union(controls, mats, tune)
 
 
 def identity(controls: Controls, n: int) -> matrix_dcsr:
@@ -84,7 +77,7 @@ def closure(controls: Controls, labels: list[matrix_dcsr], start: matrix_dcsr | 
                 prods = matrix_multiplication_batched_learned(controls, [(C, L) for L in labels], sizer, tune=tune)
             else:
                 prods = matrix_multiplication_batched(controls, [(C, L) for L in labels], tune=tune)
-            Cn = union(controls, [C] + prods)
+            Cn = union(controls, [C] + prods, tune)
         controls.sync()
         ms = (time.perf_counter() - t0) * 1e3
         history.append({"iteration": it, "nnz": Cn.nnz(), "products": int(products), "ms": ms})

@@ -97,6 +97,25 @@ __global__ void __launch_bounds__(MLP_NT) predict_kernel(const float *__restrict
     }
 }
 
+// The prediction of the listed rows only: out[list[k]] for k < *count.
+__global__ void __launch_bounds__(MLP_NT) predict_rows_kernel(const float *__restrict__ params,
+                                                              const float *__restrict__ feat,
+                                                              const uint32_t *__restrict__ list,
+                                                              const uint32_t *__restrict__ count,
+                                                              float *__restrict__ out) {
+    __shared__ SmemWeights s;
+    const uint32_t n = *count;
+    if ((uint64_t)blockIdx.x * MLP_NT >= n) return;  // block-uniform: no row for this block
+    stage_weights(params, s);
+    for (uint32_t k = blockIdx.x * MLP_NT + threadIdx.x; k < n; k += gridDim.x * MLP_NT) {
+        const uint64_t r = list[k];
+        float x[F];
+#pragma unroll
+        for (int f = 0; f < F; ++f) x[f] = feat[r * F + f];
+        out[r] = forward_row(s, x, nullptr, nullptr);
+    }
+}
+
 // Training forward + output gradient: stores h1, h2 and dy = 2 (y - t) / n.
 __global__ void __launch_bounds__(MLP_NT) train_forward_kernel(const float *__restrict__ params,
                                                                const float *__restrict__ feat,
@@ -211,9 +230,23 @@ __global__ void adam_kernel(float *__restrict__ params, float *__restrict__ m, f
 constexpr int FT_NT = 256, FT_GROUP = 8;
 constexpr uint32_t FT_LONG = 256;  // rows with more A entries: one CTA each
 
+// Rows to size by prediction (RowSel::above > 0): only rows with more than
+// `above` products get their features written, and are listed in list[0,
+// *count) for the prediction; the others only get their products.
+struct RowSel {
+    uint32_t above = 0;
+    uint32_t *list = nullptr;
+    uint32_t *count = nullptr;
+};
+
 __device__ __forceinline__ void write_features(float *__restrict__ feat, uint32_t *__restrict__ work, uint64_t row,
                                                uint64_t len, uint32_t s, uint32_t mx, uint32_t mn, float rowpos,
-                                               float density_term) {
+                                               float density_term, const RowSel &sel) {
+    if (work) work[row] = s;
+    if (sel.above) {
+        if (s <= sel.above) return;
+        sel.list[atomicAdd(sel.count, 1u)] = (uint32_t)row;
+    }
     if (mn == 0xFFFFFFFFu) mn = 0;
     float *f = feat + row * F;
     f[0] = log2f(1.0f + (float)len) * FEAT_SCALE;
@@ -222,7 +255,6 @@ __device__ __forceinline__ void write_features(float *__restrict__ feat, uint32_
     f[3] = log2f(1.0f + (float)mn) * FEAT_SCALE;
     f[4] = rowpos;
     f[5] = density_term;
-    if (work) work[row] = s;
 }
 
 // Row position and density features of A row `row`: relative to A itself,
@@ -242,7 +274,7 @@ __device__ __forceinline__ void row_context(const AView &a, uint64_t row, uint64
 // A group of 8 lanes per A row; rows over FT_LONG entries are listed for
 // features_long_kernel (hub rows would keep 8 lanes busy long after the rest).
 __global__ void __launch_bounds__(FT_NT) features_kernel(AView a, BRows b, uint64_t a_nrows, float density_term,
-                                                         BatchRows br, float *__restrict__ feat,
+                                                         BatchRows br, RowSel sel, float *__restrict__ feat,
                                                          uint32_t *__restrict__ work,
                                                          uint32_t *__restrict__ long_rows,
                                                          uint32_t *__restrict__ n_long) {
@@ -272,14 +304,15 @@ __global__ void __launch_bounds__(FT_NT) features_kernel(AView a, BRows b, uint6
         if (gl == 0) {
             float rowpos, dens;
             row_context(a, row, a_nrows, density_term, br, rowpos, dens);
-            write_features(feat, work, row, je - ja, s, mx, mn, rowpos, dens);
+            write_features(feat, work, row, je - ja, s, mx, mn, rowpos, dens, sel);
         }
     }
 }
 
 // The listed long rows, one CTA per row.
 __global__ void __launch_bounds__(FT_NT) features_long_kernel(AView a, BRows b, uint64_t a_nrows, float density_term,
-                                                              BatchRows br, const uint32_t *__restrict__ long_rows,
+                                                              BatchRows br, RowSel sel,
+                                                              const uint32_t *__restrict__ long_rows,
                                                               const uint32_t *__restrict__ n_long,
                                                               float *__restrict__ feat, uint32_t *__restrict__ work) {
     __shared__ uint32_t red[3][FT_NT / 32];
@@ -316,7 +349,7 @@ __global__ void __launch_bounds__(FT_NT) features_long_kernel(AView a, BRows b, 
             }
             float rowpos, dens;
             row_context(a, row, a_nrows, density_term, br, rowpos, dens);
-            write_features(feat, work, row, je - ja, s, mx, mn, rowpos, dens);
+            write_features(feat, work, row, je - ja, s, mx, mn, rowpos, dens, sel);
         }
         __syncthreads();
     }
@@ -361,7 +394,7 @@ uint64_t splitmix(uint64_t &s) {
 }
 
 int features_launch(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
-                    float *feat, uint32_t *work, const BatchRows *batch = nullptr) {
+                    float *feat, uint32_t *work, const BatchRows *batch = nullptr, const RowSel &sel = RowSel{}) {
     const BatchRows br = batch ? *batch : BatchRows{};
     Temp<uint32_t> long_rows, n_long;
     CLB_RETURN_IF(n_long.alloc(ctl, 1));
@@ -369,9 +402,9 @@ int features_launch(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, con
     CLB_TRY_CUDA(cudaMemsetAsync(n_long.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
     ProfScope ps(ctl, "features");
     const float dt = learned_density_feature(B);
-    features_kernel<<<grid_for(ctl, A.nzr * FT_GROUP), FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, br, feat, work,
-                                                                              long_rows.ptr, n_long.ptr);
-    features_long_kernel<<<ctl->sm_count * 4, FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, br, long_rows.ptr,
+    features_kernel<<<grid_for(ctl, A.nzr * FT_GROUP), FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, br, sel, feat,
+                                                                              work, long_rows.ptr, n_long.ptr);
+    features_long_kernel<<<ctl->sm_count * 4, FT_NT, 0, ctl->stream>>>(a, b, A.nrows, dt, br, sel, long_rows.ptr,
                                                                        n_long.ptr, feat, work);
     ctl->launches += 2;
     CLB_CHECK_LAUNCH();
@@ -390,11 +423,22 @@ int learned_caps(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const 
                  uint32_t *work, uint32_t *cap) {
     const uint64_t n = A.nzr;
     Temp<float> feat, pred;
+    Temp<uint32_t> list, count;
     CLB_RETURN_IF(feat.alloc(ctl, n * F));
     CLB_RETURN_IF(pred.alloc(ctl, n));
-    CLB_RETURN_IF(features_launch(ctl, A, B, a, b, feat.ptr, work, batch));
+    CLB_RETURN_IF(list.alloc(ctl, n));
+    CLB_RETURN_IF(count.alloc(ctl, 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(count.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    // only the rows over t.bitmap_min products take the predicted capacity:
+    // only they get features and a prediction
+    RowSel sel;
+    sel.above = t.bitmap_min;
+    sel.list = list.ptr;
+    sel.count = count.ptr;
+    CLB_RETURN_IF(features_launch(ctl, A, B, a, b, feat.ptr, work, batch, sel));
     ProfScope ps(ctl, "predict");
-    predict_kernel<<<grid_for(ctl, n, MLP_NT, 4), MLP_NT, 0, ctl->stream>>>(sizer->params, feat.ptr, n, pred.ptr);
+    predict_rows_kernel<<<grid_for(ctl, n, MLP_NT, 4), MLP_NT, 0, ctl->stream>>>(sizer->params, feat.ptr, list.ptr,
+                                                                                count.ptr, pred.ptr);
     capacity_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(pred.ptr, work, n, B.ncols, t.row_ncols, margin_log2,
                                                               slack, t.bitmap_min, cap);
     ctl->launches += 2;

@@ -207,6 +207,51 @@ int pair_descs(uint32_t count, const clb_dcsr *a, const clb_dcsr *b, std::vector
     return CLB_SUCCESS;
 }
 
+// ------------------------------------------------------------- union ----
+// The union of k matrices of one shape is the product A_u B_u with
+// B_u = [M_0; M_1; ...; M_{k-1}] (k*nrows x ncols) and A_u (nrows x k*nrows)
+// holding, in row r, the columns j*nrows + r of the M_j that store row r:
+// row r of A_u B_u merges the k sorted rows r of the M_j and drops the
+// duplicates, i.e. the accumulators do a k-way merge in one pass.
+
+// flags[r] |= 1 << j for every stored row r of M_j (blockIdx.y = j).
+__global__ void union_mark_kernel(const PairDesc *__restrict__ d, uint32_t *__restrict__ flags) {
+    const PairDesc p = d[blockIdx.y];
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < p.nzr; k += (uint64_t)gridDim.x * blockDim.x)
+        atomicOr(flags + p.rows[k], 1u << blockIdx.y);
+}
+
+// cnt[r] = number of M_j storing row r; nonempty[r] = cnt[r] > 0.
+__global__ void union_counts_kernel(const uint32_t *__restrict__ flags, uint64_t n, uint32_t *__restrict__ cnt,
+                                    uint32_t *__restrict__ nonempty) {
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = __popc(flags[r]);
+        cnt[r] = c;
+        nonempty[r] = c ? 1u : 0u;
+    }
+}
+
+// A_u in DCSR: stored row pos[r] = r with columns j*nrows + r (j ascending).
+__global__ void union_left_kernel(const uint32_t *__restrict__ flags, const uint64_t *__restrict__ off,
+                                  const uint32_t *__restrict__ pos, uint64_t n, uint64_t nzr, uint64_t nnz,
+                                  uint64_t *__restrict__ rpt, uint32_t *__restrict__ rows,
+                                  uint32_t *__restrict__ cols) {
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t f = flags[r];
+        if (!f) continue;
+        const uint32_t p = pos[r];
+        uint64_t o = off[r];
+        rpt[p] = o;
+        rows[p] = (uint32_t)r;
+        while (f) {
+            const uint32_t j = (uint32_t)(__ffs(f) - 1);
+            cols[o++] = (uint32_t)(j * n + r);
+            f &= f - 1;
+        }
+        if (p + 1 == nzr) rpt[nzr] = nnz;
+    }
+}
+
 // The batched product: stack, one product over the stack (exact / tuned
 // form, or the learned single pass when `sizer` is given), split.
 int batched_impl(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b, clb_dcsr *c,
@@ -624,6 +669,99 @@ int clb_spgemm_batched_plan_learned(clb_controls *ctl, uint32_t count, const clb
                        ctl->stream>>>(cap.ptr, anzr, ~0ull, (unsigned long long *)need.ptr);
     CLB_CHECK_LAUNCH();
     CLB_RETURN_IF(read_scalars(ctl, need.ptr, slots_need, 1));
+    return CLB_SUCCESS;
+}
+
+int clb_dcsr_union(clb_controls *ctl, uint32_t count, const clb_dcsr *mats, const clb_spgemm_tuning *tuning,
+                   clb_dcsr *out, clb_spgemm_stats *stats) {
+    if (!ctl || !out || (count && !mats)) return fail(CLB_INVALID_ARGUMENT, "NULL argument");
+    if (count == 0) return fail(CLB_INVALID_ARGUMENT, "union of no matrices");
+    if (count > 32) return fail(CLB_NOT_SUPPORTED, "union of more than 32 matrices in one call");
+    CLB_RETURN_IF(check_tuning(tuning));
+    const uint64_t n = mats[0].nrows, ncols = mats[0].ncols;
+    for (uint32_t k = 1; k < count; ++k)
+        if (mats[k].nrows != n || mats[k].ncols != ncols)
+            return fail(CLB_INVALID_ARGUMENT, "union: matrix " + std::to_string(k) + " is " +
+                                                  std::to_string(mats[k].nrows) + " x " +
+                                                  std::to_string(mats[k].ncols) + ", matrix 0 is " +
+                                                  std::to_string(n) + " x " + std::to_string(ncols));
+    if ((uint64_t)count * n > 0xFFFFFFFFull) return fail(CLB_NOT_SUPPORTED, "union: count x nrows >= 2^32");
+    clb_spgemm_stats st{};
+    if (stats) *stats = st;
+    std::vector<PairDesc> db(count);
+    uint64_t bnzr = 0, bnnz = 0, bmax = 1;
+    for (uint32_t k = 0; k < count; ++k) {
+        const bool live = mats[k].nnz && mats[k].nzr;
+        db[k] = PairDesc{mats[k].rpt, mats[k].rows, mats[k].cols, live ? mats[k].nzr : 0, live ? mats[k].nnz : 0,
+                         bnzr, bnnz, (uint32_t)(k * n), 0u, (uint32_t)ncols};
+        if (live) {
+            bnzr += mats[k].nzr;
+            bnnz += mats[k].nnz;
+            bmax = std::max(bmax, std::max(mats[k].nnz, mats[k].nzr + 1));
+        }
+    }
+    clb_dcsr C{};
+    C.nrows = n;
+    C.ncols = ncols;
+    if (bnnz == 0) {
+        *out = C;
+        return CLB_SUCCESS;
+    }
+    DeviceGuard g(ctl);
+    Temp<PairDesc> ddb;
+    Temp<uint64_t> brpt, off, tot;
+    Temp<uint32_t> brws, bcls, flags, cnt, pos;
+    CLB_RETURN_IF(ddb.alloc(ctl, count));
+    CLB_RETURN_IF(brpt.alloc(ctl, bnzr + 1));
+    CLB_RETURN_IF(brws.alloc(ctl, bnzr));
+    CLB_RETURN_IF(bcls.alloc(ctl, bnnz));
+    CLB_RETURN_IF(flags.alloc(ctl, n));
+    CLB_RETURN_IF(cnt.alloc(ctl, n));
+    CLB_RETURN_IF(pos.alloc(ctl, n));
+    CLB_RETURN_IF(off.alloc(ctl, n));
+    CLB_RETURN_IF(tot.alloc(ctl, 2));
+    CLB_TRY_CUDA(cudaMemcpyAsync(ddb.ptr, db.data(), count * sizeof(PairDesc), cudaMemcpyHostToDevice, ctl->stream),
+                 CLB_WRITE_BUFFER_ERROR);
+    CLB_TRY_CUDA(cudaMemsetAsync(flags.ptr, 0, n * 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    {
+        ProfScope ps(ctl, "union_stack");
+        stack_kernel<<<dim3(stack_grid_x(ctl, bmax, count), count), CAT_NT, 0, ctl->stream>>>(
+            ddb.ptr, brpt.ptr, brws.ptr, bcls.ptr, nullptr, nullptr, bnzr, bnnz);
+        const uint64_t rmax = std::max<uint64_t>(1, bmax);
+        union_mark_kernel<<<dim3((unsigned)std::min<uint64_t>((rmax + 255) / 256, 4096), count), 256, 0,
+                            ctl->stream>>>(ddb.ptr, flags.ptr);
+        const unsigned g1 = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctl->sm_count * 16);
+        union_counts_kernel<<<g1, 256, 0, ctl->stream>>>(flags.ptr, n, cnt.ptr, pos.ptr);
+        CLB_CHECK_LAUNCH();
+    }
+    CLB_RETURN_IF(scan_u32_to_u64(ctl, cnt.ptr, off.ptr, n, tot.ptr + 0));  // A_u column offsets, nnz(A_u)
+    CLB_RETURN_IF(scan_u32_inplace(ctl, pos.ptr, n, tot.ptr + 1));          // A_u row positions, nzr(A_u)
+    uint64_t h[2];
+    CLB_RETURN_IF(read_scalars(ctl, tot.ptr, h, 2));
+    const uint64_t annz = h[0], anzr = h[1];
+    Temp<uint64_t> arpt;
+    Temp<uint32_t> arws, acls;
+    CLB_RETURN_IF(arpt.alloc(ctl, anzr + 1));
+    CLB_RETURN_IF(arws.alloc(ctl, anzr));
+    CLB_RETURN_IF(acls.alloc(ctl, annz));
+    {
+        const unsigned g1 = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctl->sm_count * 16);
+        union_left_kernel<<<g1, 256, 0, ctl->stream>>>(flags.ptr, off.ptr, pos.ptr, n, anzr, annz, arpt.ptr,
+                                                      arws.ptr, acls.ptr);
+        CLB_CHECK_LAUNCH();
+    }
+    flags.reset();
+    cnt.reset();
+    pos.reset();
+    off.reset();
+    const clb_dcsr Au{n, (uint64_t)count * n, annz, anzr, arpt.ptr, arws.ptr, acls.ptr};
+    const clb_dcsr Bu{(uint64_t)count * n, ncols, bnnz, bnzr, brpt.ptr, brws.ptr, bcls.ptr};
+    CLB_RETURN_IF(validate_spgemm(Au, Bu));
+    const uint32_t launches = 5;
+    CLB_RETURN_IF(spgemm_tuned(ctl, Au, Bu, tuning ? tuning->form : 1, to_tuning(tuning), &C, &st));
+    st.kernel_launches += launches;
+    if (stats) *stats = st;
+    *out = C;
     return CLB_SUCCESS;
 }
 

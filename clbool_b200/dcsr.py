@@ -3,9 +3,9 @@ from .ops import (kronecker_product, matrix_multiplication, matrix_multiplicatio
                   workload)
 from .sizing import RowSizer, matrix_multiplication_learned, row_features, row_nnz
 from .batched import (autotune, matrix_multiplication_batched, matrix_multiplication_batched_learned,
-                      matrix_multiplication_tuned, tuning)
+                      matrix_multiplication_tuned, matrix_union, tuning)
 
 __all__ = ["matrix_multiplication_hash", "matrix_multiplication", "kronecker_product", "transpose", "workload",
            "submatrix", "reduce",
            "matrix_multiplication_learned", "RowSizer", "row_features", "row_nnz", "matrix_multiplication_batched",
-           "matrix_multiplication_batched_learned", "matrix_multiplication_tuned", "autotune", "tuning"]
+           "matrix_multiplication_batched_learned", "matrix_multiplication_tuned", "matrix_union", "autotune", "tuning"]

@@ -352,6 +352,17 @@ CLB_API int clb_dcsr_spgemm_batched_learned(clb_controls *ctl, uint32_t count, c
                                             const clb_dcsr *b, clb_dcsr *c, const clb_sizer *sizer,
                                             float margin_log2, float slack, const clb_spgemm_tuning *tuning,
                                             clb_spgemm_stats *stats);
+/* No counterpart in the reference (whose additions take two operands,
+ * src/coo/coo.hpp:9-14, src/csr/csr.hpp:12): out = mats[0] v mats[1] v ...
+ * v mats[count - 1] (count <= 32 matrices of one shape, count * nrows <
+ * 2^32) in one pass.  The union is the product A_u B_u with B_u the mats
+ * stacked row-wise and A_u's row r holding column j * nrows + r for every
+ * matrix j that stores row r, so the SpGEMM accumulators merge the (at most
+ * count) sorted rows r and drop duplicates.  tuning: the accumulator tuning
+ * of that product (NULL = the single pass into upper-bound slots); stats
+ * (optional) are the product's, products = the entries of all mats. */
+CLB_API int clb_dcsr_union(clb_controls *ctl, uint32_t count, const clb_dcsr *mats,
+                           const clb_spgemm_tuning *tuning, clb_dcsr *out, clb_spgemm_stats *stats);
 /* Times the batched product under every candidate tuning (32: form x
  * bitmap_min x bitmap_threads x warp_max x small_lanes; twice that with both
  * wide_rows settings when a pair has more than 2^20 columns) on the given

@@ -249,3 +249,29 @@ def test_addition_csr_batched(controls):
     with pytest.raises(cb.ClBoolException) as ex:
         cb.csr.matrix_addition_batched(controls, [(dev(pairs[0][0]), dev(pairs[0][1])), (dev(f), dev(pairs[0][0]))])
     assert ex.value.status_name == "CLBOOL_INVALID_ARGUMENT"
+
+
+def test_union_matches_oracle(controls):
+    """The one-pass union of k matrices of one shape (no counterpart in the
+    reference): power-law and R-MAT pieces, an empty operand, a single
+    operand, rows that only one operand stores, duplicates across all of
+    them; equal to the oracle's union, under both accumulator forms."""
+    import clbool_b200 as cb
+    from clbool_b200 import gen
+    n = 3000
+    mats = []
+    for k in range(5):
+        r, c = gen.power_law_rows(n, n + 11, 2.1, 12.0, 2048, seed=600 + k)
+        mats.append(O.coo_to_dcsr(O.Coo(n, n + 11, r, c)))
+    r, c = gen.rmat(11, seed=3)
+    g = O.coo_to_dcsr(O.Coo(n, n + 11, r, c))
+    mats += [g, g, O.coo_to_dcsr(O.Coo(n, n + 11, np.zeros(0, np.uint32), np.zeros(0, np.uint32)))]
+    dev = [to_device(controls, m) for m in mats]
+    for sel in (list(range(len(mats))), [0], [5, 6], [7, 2], [7]):
+        want = O.union([mats[i] for i in sel])
+        for t in (None, cb.dcsr.tuning("two_pass")):
+            got = cb.dcsr.matrix_union(controls, [dev[i] for i in sel], t)
+            assert_dcsr_equal(from_device(controls, got), want, f"union {sel}")
+    with pytest.raises(cb.ClBoolException) as ex:
+        cb.dcsr.matrix_union(controls, [dev[0], to_device(controls, pairs_dcsr(100, 3))])
+    assert ex.value.status_name == "CLBOOL_INVALID_ARGUMENT"
