@@ -11,9 +11,12 @@ int prepare_b(clb_controls *ctl, const clb_dcsr &B, Temp<uint64_t> &dense, BRows
 // B's rows as word runs for the bitmap insertion: built when b has the dense
 // row map, B has at least B_WORDS_MIN_NNZ entries and (hinfo, rows per bin,
 // when given) some row is in a bitmap bin; otherwise b is left as it is.
+// products (when known, else 0): the product's total; the runs are skipped
+// when B's entries are read fewer than B_WORDS_MIN_REUSE times on average.
 constexpr uint64_t B_WORDS_MIN_NNZ = 1ull << 16;
+constexpr uint64_t B_WORDS_MIN_REUSE = 4;
 int prepare_b_words(clb_controls *ctl, const clb_dcsr &B, const uint32_t *hinfo, Temp<uint64_t> &wdense,
-                    Temp<uint2> &wpairs, BRows &b);
+                    Temp<uint2> &wpairs, BRows &b, uint64_t products = 0);
 // work[i] = products of A row i; *d_total += their sum.
 int launch_workload(clb_controls *ctl, const AView &a, const BRows &b, uint32_t *work, uint64_t *d_total);
 // Histogram + scatter of the rows into accumulator bins.  The bound of

@@ -156,10 +156,12 @@ __global__ void run_rows_kernel(const uint64_t *__restrict__ dense, uint64_t nro
 }  // namespace
 
 int prepare_b_words(clb_controls *ctl, const clb_dcsr &B, const uint32_t *hinfo, Temp<uint64_t> &wdense,
-                    Temp<uint2> &wpairs, BRows &b) {
+                    Temp<uint2> &wpairs, BRows &b, uint64_t products) {
     // the word form rides on the dense row map; it pays for its passes over B
-    // only when bitmap rows multiply a large B
+    // only when bitmap rows multiply a large B whose entries are read several
+    // times (a union's stacked operands are read once each: products = nnz(B))
     if (!b.dense || B.nzr == 0 || B.nnz < B_WORDS_MIN_NNZ) return CLB_SUCCESS;
+    if (products && products < B_WORDS_MIN_REUSE * B.nnz) return CLB_SUCCESS;
     if (hinfo && hinfo[BIN_BMP_XL] + hinfo[BIN_BMP_L] + hinfo[BIN_BMP] == 0) return CLB_SUCCESS;
     const uint64_t nnz = B.nnz;
     // runs <= entries: the pairs are sized by the entries (no host read).
@@ -258,9 +260,11 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     // rows per bin: only the bins with rows are launched, sized to them
     uint32_t hinfo[NUM_BINS];
     CLB_RETURN_IF(read_small(ctl, info.ptr, hinfo, sizeof(hinfo)));
+    uint64_t products = 0;
+    CLB_RETURN_IF(read_scalars(ctl, scal.ptr, &products, 1));
     Temp<uint64_t> wdense;
     Temp<uint2> wpairs;
-    CLB_RETURN_IF(prepare_b_words(ctl, B, hinfo, wdense, wpairs, b));
+    CLB_RETURN_IF(prepare_b_words(ctl, B, hinfo, wdense, wpairs, b, products));
 
     BinLists bl{list.ptr, info.ptr};
     RowOut sym{row_nnz.ptr, nullptr, nullptr, nullptr, nullptr, ctl->d_status};

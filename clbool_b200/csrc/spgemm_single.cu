@@ -351,7 +351,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     BRows b = b_in;
     Temp<uint64_t> wdense;
     Temp<uint2> wpairs;
-    CLB_RETURN_IF(prepare_b_words(ctl, B, hinfo, wdense, wpairs, b));
+    CLB_RETURN_IF(prepare_b_words(ctl, B, hinfo, wdense, wpairs, b, products));
     if (st) {
         for (int k = 0; k < NUM_BINS; ++k) st->rows_per_bin[k] = hinfo[k];
         st->capacity = capacity;
