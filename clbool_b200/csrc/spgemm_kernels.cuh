@@ -770,6 +770,8 @@ __device__ __forceinline__ void unit_products(const AView &a, const BRows &b, ui
 // bitmap word, built once per call), the same sweeps run over the pairs and
 // `set_word(w, m)` issues one atomic per run instead of one per entry: on
 // R-MAT scale 20 the products fall in 1.69 times fewer words than entries.
+// The runs of a unit lie in distinct words (one B row), so there the lanes
+// of an instruction take 32 consecutive runs.
 template <int NT, int ECH, class SetBit, class SetWord>
 __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b, uint32_t i, uint32_t shift,
                                                   uint32_t maxcol, SetBit &&set_bit, SetWord &&set_word,
@@ -827,20 +829,22 @@ __device__ __forceinline__ void bitmap_insert_row(const AView &a, const BRows &b
             for (uint32_t k0 = ws; k0 < vhi; k0 += 256u) {
                 const uint32_t p0 = k0 + lane * 8u;
                 if (words) {
-                    // eight pairs: four 16-byte loads (p0 is a multiple of 8,
-                    // the pair array 16-byte aligned), each only when it holds
-                    // a pair of [vlo, vhi)
-                    const uint4 *p4 = reinterpret_cast<const uint4 *>(b.wpairs + p0);
-                    uint4 t[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        t[q] = (p0 + 2u * q + 2u > vlo && p0 + 2u * q < vhi) ? __ldg(p4 + q) : make_uint4(0, 0, 0, 0);
+                    // eight pairs per lane, lanes 32 pairs apart in each of
+                    // them: a unit's runs come from one B row, so they lie in
+                    // distinct, increasing words, and the 32 atomics of one
+                    // instruction hit neighbouring words in distinct banks
+                    // (lanes 8 pairs apart put several lanes on one bank).
+                    // Each load instruction reads 32 consecutive pairs.
+                    uint2 t[8];
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
-                        const uint32_t q = p0 + (uint32_t)j;
-                        const uint32_t wd = (j & 1) ? t[j >> 1].z : t[j >> 1].x;
-                        const uint32_t mk = (j & 1) ? t[j >> 1].w : t[j >> 1].y;
-                        if (q >= vlo && q < vhi) set_word(min(wd, maxword), mk);
+                        const uint32_t q = k0 + 32u * (uint32_t)j + lane;
+                        t[j] = (q >= vlo && q < vhi) ? __ldg(b.wpairs + q) : make_uint2(0, 0);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const uint32_t q = k0 + 32u * (uint32_t)j + lane;
+                        if (q >= vlo && q < vhi) set_word(min(t[j].x, maxword), t[j].y);
                     }
                     continue;
                 }
