@@ -106,8 +106,8 @@ def multiply_block(controls: Controls, a: matrix_dcsr, b: matrix_dcsr, rank: int
     return c, (lo, hi), int(work[lo:hi].sum())
 
 
-def _device_tensor(buf: DeviceBuffer, n: int, dtype):
-    """A torch view of a device buffer (no copy), for the NCCL calls."""
+def _device_tensor(buf: DeviceBuffer, n: int, dtype, device: int):
+    """A torch view of a device buffer on `device` (no copy), for the NCCL calls."""
     import torch
 
     class _Cai:
@@ -115,15 +115,23 @@ def _device_tensor(buf: DeviceBuffer, n: int, dtype):
             self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": np.dtype(dt).str,
                                              "data": (int(ptr), False), "version": 3}
     signed = {np.dtype(np.uint32): np.int32, np.dtype(np.uint64): np.int64}[np.dtype(dtype)]
-    return torch.as_tensor(_Cai(buf.ptr, n, signed), device=f"cuda:{torch.cuda.current_device()}")
+    return torch.as_tensor(_Cai(buf.ptr, n, signed), device=f"cuda:{device}")
 
 
 def broadcast_dcsr(controls: Controls, m: matrix_dcsr | None, src: int = 0, group=None) -> matrix_dcsr:
     """`m` (given on rank `src`) in every rank's own device memory: one
-    broadcast of the sizes, then one per array.  Other ranks pass None."""
+    broadcast of the sizes, then one per array.  Other ranks pass None.
+    The broadcasts run on torch's current stream of the controls' device,
+    after the controls' stream has finished its work."""
+    import torch
+    with torch.cuda.device(controls.device):
+        return _broadcast_dcsr(controls, m, src, group)
+
+
+def _broadcast_dcsr(controls, m, src, group):
     import torch
     import torch.distributed as dist
-    dev = torch.device(f"cuda:{torch.cuda.current_device()}")
+    dev = torch.device(f"cuda:{controls.device}")
     me = dist.get_rank(group)
     head = torch.zeros(4, dtype=torch.int64, device=dev)
     if me == src:
@@ -141,7 +149,7 @@ def broadcast_dcsr(controls: Controls, m: matrix_dcsr | None, src: int = 0, grou
         cols = DeviceBuffer.empty(controls, nnz, np.uint32)
         controls.sync()
     for buf, n, dt in ((rpt, nzr + 1, np.uint64), (rows, nzr, np.uint32), (cols, nnz, np.uint32)):
-        dist.broadcast(_device_tensor(buf, n, dt), src, group=group)
+        dist.broadcast(_device_tensor(buf, n, dt, controls.device), src, group=group)
     torch.cuda.synchronize(dev)
     if me == src:
         return m
