@@ -185,7 +185,7 @@ CLB_API int clb_prefix_sum_u64(clb_controls *ctl, uint64_t *array, uint64_t n, u
  * entries in place, for callers that cannot allocate device memory when they
  * need it (for instance a runtime that has reserved all of the GPU's memory
  * for its own pool, or a hot loop that must not pay for cudaMalloc's implicit
- * synchronisation).  It allocates nothing: its scratch is a fixed 512 KiB
+ * synchronisation).  It allocates nothing: its scratch is a fixed 256 KiB
  * array inside the library, so n is limited to 2^28 entries (larger n is
  * rejected with CLB_INVALID_ARGUMENT).  It takes no controls object, launches
  * on `stream` (a cudaStream_t; NULL = legacy default stream of the current

@@ -22,7 +22,7 @@ def test_prefix_sum_vectors(controls):
         assert sha(buf.to_host(), np.uint32) == case["scan"]
 
 
-@pytest.mark.parametrize("n", [1, 2, 4095, 4096, 4097, 1_000_003])
+@pytest.mark.parametrize("n", [1, 2, 4095, 4096, 4097, 8193, 1_000_003])
 def test_prefix_sum_sizes_u64(controls, n):
     import clbool_b200 as cb
     rng = np.random.default_rng(n)
@@ -32,6 +32,32 @@ def test_prefix_sum_sizes_u64(controls, n):
     ref = np.concatenate([np.zeros(1, np.uint64), np.cumsum(v, dtype=np.uint64)[:-1]])
     assert total == int(v.sum(dtype=np.uint64))
     assert np.array_equal(buf.to_host(), ref)
+
+
+@pytest.mark.parametrize("n,offset", [(4097, 0), (8192, 0), (8193, 0), (8193, 2), (12_289, 1), (16_384, 0),
+                                      (1_000_003, 0), (1_000_003, 3), ((1 << 26) + 5, 0), ((1 << 26) + 5, 1)])
+def test_prefix_sum_u32_tiles(controls, n, offset):
+    """u32 scans in place through the C ABI around the 8192-entry tile
+    (one tile, one tile plus one entry, ragged last tiles), on arrays that do
+    not start on a 16-byte boundary (element loads instead of vectors), with
+    entries up to 2^32 - 1 (the scan wraps modulo 2^32 like the reference's
+    u32 output; the returned total is the exact 64-bit sum)."""
+    import ctypes
+
+    import clbool_b200 as cb
+    rng = np.random.default_rng(n + offset)
+    v = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+    pad = np.full(offset, 7, np.uint32)
+    buf = cb.DeviceBuffer.from_host(controls, np.concatenate([pad, v, pad]), np.uint32)
+    tot = ctypes.c_uint64()
+    rc = cb.lib.clb_prefix_sum_u32(controls.handle, ctypes.c_void_p(buf.ptr + 4 * offset), n, ctypes.byref(tot))
+    assert rc == 0, cb.lib.clb_last_error()
+    inc = np.cumsum(v, dtype=np.uint64)
+    assert tot.value == int(inc[-1])
+    got = buf.to_host()
+    assert np.array_equal(got[:offset], pad) and np.array_equal(got[offset + n:], pad)
+    want = np.concatenate([np.zeros(1, np.uint64), inc[:-1]]).astype(np.uint32)
+    assert np.array_equal(got[offset:offset + n], want)
 
 
 def test_bitonic_sort_vectors(controls):

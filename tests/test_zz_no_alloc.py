@@ -50,7 +50,7 @@ def test_noalloc_prefix_sum_rejects_sizes_past_its_scratch(controls):
     assert b"static scratch limit" in cb.lib.clb_last_error()
 
 
-@pytest.mark.parametrize("n", [0, 1, 4096, 4097])
+@pytest.mark.parametrize("n", [0, 1, 4096, 4097, 8192, 8193])
 def test_noalloc_prefix_sum_edge_sizes(controls, n):
     """No entries (only the total is written), one entry, exactly one tile
     and one past it, each compared with the regular scan and numpy."""
