@@ -118,7 +118,10 @@ __global__ void __launch_bounds__(MP_NT) merge_tile_kernel(CooSide Ac, CooSide B
                                                            const uint64_t *__restrict__ tile_off,
                                                            uint32_t *__restrict__ row_dup, uint32_t *__restrict__ out_rows,
                                                            uint32_t *__restrict__ out_cols) {
-    __shared__ uint64_t s[MP_TILE];
+    // the tile's A and B keys for the merge; then (MODE 1) its outputs,
+    // compacted at position q + q / 8 (threads stage 8 outputs each, so the
+    // skew keeps neighbouring lanes off the same banks)
+    __shared__ uint64_t s[MP_TILE + MP_TILE / 8];
     __shared__ uint32_t scratch[33];
     const uint64_t na = CSR ? As.n : Ac.n, nb = CSR ? Bs.n : Bc.n;
     const uint64_t total = na + nb;
@@ -133,8 +136,10 @@ __global__ void __launch_bounds__(MP_NT) merge_tile_kernel(CooSide Ac, CooSide B
         rlo = split_row[t];
         rhi = split_row[t + 1];
     }
+#pragma unroll 4
     for (uint32_t k = threadIdx.x; k < nta; k += MP_NT)
         s[k] = CSR ? csr_key(As, a0 + k, rlo, rhi) : coo_key(Ac, a0 + k);
+#pragma unroll 4
     for (uint32_t k = threadIdx.x; k < ntb; k += MP_NT)
         s[nta + k] = CSR ? csr_key(Bs, b0 + k, rlo, rhi) : coo_key(Bc, b0 + k);
     __syncthreads();
@@ -187,16 +192,23 @@ __global__ void __launch_bounds__(MP_NT) merge_tile_kernel(CooSide Ac, CooSide B
         if (threadIdx.x == 0) tile_cnt[t] = tot;
         return;
     }
+    // (the block scan's barriers also end every thread's merge reads of s)
     uint32_t tot;
-    uint32_t off = block_exclusive_scan<uint32_t, MP_NT>(cnt, scratch, &tot);
-    uint64_t p = tile_off[t] + off;
+    uint32_t q = block_exclusive_scan<uint32_t, MP_NT>(cnt, scratch, &tot);
 #pragma unroll
     for (int k = 0; k < MP_ITEMS; ++k) {
         if (flags & (1u << k)) {
-            if (!CSR) out_rows[p] = (uint32_t)(keys[k] >> 32);
-            out_cols[p] = (uint32_t)keys[k];
-            ++p;
+            s[q + (q >> 3)] = keys[k];
+            ++q;
         }
+    }
+    __syncthreads();
+    // coalesced copy-out of the tile's outputs
+    const uint64_t base = tile_off[t];
+    for (uint32_t i = threadIdx.x; i < tot; i += MP_NT) {
+        const uint64_t key = s[i + (i >> 3)];
+        if (!CSR) out_rows[base + i] = (uint32_t)(key >> 32);
+        out_cols[base + i] = (uint32_t)key;
     }
 }
 
