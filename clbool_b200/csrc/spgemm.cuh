@@ -37,6 +37,10 @@ int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos
 int launch_bitmap_expand(clb_controls *ctl, const uint32_t *list, const uint32_t *count, uint64_t nmax,
                          const uint64_t *slot_off, const uint32_t *slots, const uint64_t *off,
                          const uint32_t *row_ncols, uint64_t ncols, uint32_t *ccols);
+// The same by step, from the deferred rows' step records (RowOut::defer_steps).
+int launch_bitmap_expand_steps(clb_controls *ctl, const uint32_t *list, const uint32_t *count, const uint32_t *steps,
+                               const uint64_t *slot_off, const uint32_t *slots, const uint64_t *off,
+                               uint32_t *ccols);
 // Numeric accumulators without (hash_bins = false) the hash bins.
 int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
                                const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins,

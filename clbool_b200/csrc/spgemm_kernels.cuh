@@ -144,6 +144,9 @@ struct RowOut {
     uint32_t *defer = nullptr;
     uint32_t *defer_list = nullptr;
     uint32_t *defer_count = nullptr;
+    // Optional: record d (BMP_STEP_REC words) of defer_list[d] gets its
+    // non-empty steps and their output offsets (bitmap_expand_steps_kernel).
+    uint32_t *defer_steps = nullptr;
 };
 
 // ------------------------------------------------------------- warp ESC ----
@@ -625,6 +628,9 @@ constexpr uint32_t BMP_MAX_WORDS = 32768;     // 128 KB: 2^20 columns per chunk
 constexpr int BMP_U = 8;                      // B-column loads in flight per lane
 constexpr uint32_t BMP_STEP_WORDS = 128;      // emission step: 4 words per lane
 constexpr uint32_t BMP_MAX_STEPS = BMP_MAX_WORDS / BMP_STEP_WORDS;
+// A deferred row's step record: count of non-empty steps | the steps
+// (BMP_MAX_STEPS) | their first outputs and the row's total (BMP_MAX_STEPS + 1).
+constexpr uint32_t BMP_STEP_REC = 2 + 2 * BMP_MAX_STEPS;
 constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (columns)
 // Bitmaps at least this wide (2^18 columns) may be kept for bitmap_expand_kernel:
 // narrower ones cost more per row to reload than their compaction.
@@ -929,19 +935,113 @@ __device__ __forceinline__ uint32_t bitmap_list_steps(const uint4 *bm4, uint32_t
     return ctot;
 }
 
-// Emits the listed steps as sorted columns colbase + bit index to out[],
-// clearing the bitmap.  Warps take steps dynamically; for a step, lane l
-// holds words 4l..4l+3 and a warp scan of their counts places them; the
-// step's outputs are produced in windows of up to BMP_STAGE: the window's
-// outputs are split evenly over the lanes, each lane finds the word and bit
-// of its first output (shuffle search over the scan, then nth_set_bit) and
-// walks the bitmap from there into the warp's staging buffer, which the warp
-// copies out with coalesced stores.  A step with at most BMP_FEW outputs
-// skips the windows: each lane writes its own bits at its scan offset.  A
-// step with at least BMP_DENSE outputs is emitted bit-parallel instead.  Cost
-// follows the non-empty steps and the output, not the bitmap width.  The
-// caller synchronises the block after.
-__device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t nlist, const uint32_t *s_list,
+// Emits one 128-word step holding T > 0 set bits, stored at sbm in shared
+// memory, as the sorted columns cb + bit index to out[0, T); CLEAR zeroes
+// the step's words after.  Lane l holds words 4l..4l+3 and a warp scan of
+// their counts places them; the step's outputs are produced in windows of up
+// to BMP_STAGE: the window's outputs are split evenly over the lanes, each
+// lane finds the word and bit of its first output (shuffle search over the
+// scan, then nth_set_bit) and walks the bitmap from there into the warp's
+// staging buffer, which the warp copies out with coalesced stores.  A step
+// with at most BMP_FEW outputs skips the windows: each lane writes its own
+// bits at its scan offset.  A step with at least BMP_DENSE outputs is
+// emitted bit-parallel instead.
+template <bool CLEAR>
+__device__ __forceinline__ void bitmap_emit_step(uint32_t *sbm, uint32_t T, uint32_t *out, uint32_t cb0,
+                                                 uint32_t *stage) {
+    const uint32_t lane = lane_id();
+    uint4 *const sbm4 = reinterpret_cast<uint4 *>(sbm);
+    if (T >= BMP_DENSE) {
+        // dense step: bit-parallel.  Lane l tests bit l of every word (one
+        // broadcast 16-byte load per four words); a word's outputs land at
+        // consecutive addresses, one store instruction per word.
+        const uint32_t lb = 1u << lane, lt = lb - 1u;
+        const uint32_t cb = cb0 + lane;
+        uint32_t off = 0;
+#pragma unroll 4
+        for (uint32_t q = 0; q < 32; ++q) {
+            const uint4 y = sbm4[q];
+            const uint32_t c = cb + q * 128u;
+            if (y.x & lb) out[off + __popc(y.x & lt)] = c;
+            off += __popc(y.x);
+            if (y.y & lb) out[off + __popc(y.y & lt)] = c + 32u;
+            off += __popc(y.y);
+            if (y.z & lb) out[off + __popc(y.z & lt)] = c + 64u;
+            off += __popc(y.z);
+            if (y.w & lb) out[off + __popc(y.w & lt)] = c + 96u;
+            off += __popc(y.w);
+        }
+        __syncwarp();  // every lane has read the step
+        if (CLEAR) sbm4[lane] = make_uint4(0, 0, 0, 0);
+        return;
+    }
+    const uint4 x = sbm4[lane];
+    const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+    const uint32_t inc = warp_inclusive_scan(pc);
+    if (T <= BMP_FEW) {
+        // few outputs (a quarter of the steps of R-MAT rows hold <= 8):
+        // every lane writes its own bits in place, no search, no staging
+        uint32_t *o = out + inc - pc;
+        const uint32_t wb = cb0 + lane * 128u;
+        uint32_t cur = x.x, j = 0;
+        for (uint32_t t = 0; t < pc; ++t) {
+            while (!cur) {
+                ++j;
+                cur = j == 1 ? x.y : (j == 2 ? x.z : x.w);
+            }
+            o[t] = wb + j * 32u + (uint32_t)(__ffs(cur) - 1);
+            cur &= cur - 1;
+        }
+        if (CLEAR && pc) sbm4[lane] = make_uint4(0, 0, 0, 0);
+        return;
+    }
+    for (uint32_t w0 = 0; w0 < T; w0 += BMP_STAGE) {
+        const uint32_t m = min(BMP_STAGE, T - w0);
+        const uint32_t per = (m + 31) >> 5;  // outputs per lane
+        const uint32_t k = w0 + lane * per;
+        const uint32_t kend = min(k + per, w0 + m);
+        const uint32_t key = min(k, T - 1);
+        // L = first lane whose inclusive count exceeds key
+        uint32_t L = 0;
+#pragma unroll
+        for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
+            const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, L + sft - 1);
+            if (v <= key) L += sft;
+        }
+        const uint32_t exL = __shfl_sync(0xFFFFFFFFu, inc - pc, L);
+        if (k < kend) {
+            const uint4 y = sbm4[L];
+            uint32_t r = key - exL, wv = y.x, widx = L * 4u, c;
+            c = __popc(y.x);
+            if (r >= c) {
+                r -= c; wv = y.y; ++widx; c = __popc(y.y);
+                if (r >= c) {
+                    r -= c; wv = y.z; ++widx; c = __popc(y.z);
+                    if (r >= c) { r -= c; wv = y.w; ++widx; }
+                }
+            }
+            uint32_t cur = wv & (0xFFFFFFFFu << nth_set_bit(wv, r));
+            for (uint32_t kk = k; kk < kend; ++kk) {
+                while (!cur) cur = sbm[++widx];  // the step holds more outputs
+                stage[kk - w0] = cb0 + widx * 32u + (uint32_t)(__ffs(cur) - 1);
+                cur &= cur - 1;
+            }
+        }
+        __syncwarp();
+        uint32_t *const o2 = out + w0 + lane;
+#pragma unroll
+        for (uint32_t u = 0; u < BMP_STAGE / 32; ++u)
+            if (lane + 32 * u < m) o2[32 * u] = stage[lane + 32 * u];
+        __syncwarp();
+    }
+    if (CLEAR && pc) sbm4[lane] = make_uint4(0, 0, 0, 0);
+}
+
+// Emits the listed steps (bitmap_list_steps) as sorted columns colbase + bit
+// index to out[], clearing the bitmap; warps take steps dynamically
+// (bitmap_emit_step).  Cost follows the non-empty steps and the output, not
+// the bitmap width.  The caller synchronises the block after.
+__device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint32_t nlist, const uint32_t *s_list,
                                             const uint32_t *s_soff, uint32_t *s_next, uint32_t *stage, uint32_t *out,
                                             uint32_t colbase) {
     const uint32_t lane = lane_id();
@@ -952,93 +1052,8 @@ __device__ __forceinline__ void bitmap_emit(uint32_t *bm, uint4 *bm4, uint32_t n
         if (g >= nlist) break;
         const uint32_t st = s_list[g];
         const uint32_t pos = s_soff[g];
-        const uint32_t T = s_soff[g + 1] - pos;
-        const uint32_t q4 = st * 32u + lane;  // lane's uint4 of the step
-        if (T >= BMP_DENSE) {
-            // dense step: bit-parallel.  Lane l tests bit l of every word (one
-            // broadcast 16-byte load per four words); a word's outputs land at
-            // consecutive addresses, one store instruction per word.
-            const uint32_t lb = 1u << lane, lt = lb - 1u;
-            const uint4 *s4 = bm4 + st * 32u;
-            const uint32_t cb = colbase + st * (BMP_STEP_WORDS * 32u) + lane;
-            uint32_t off = pos;
-#pragma unroll 4
-            for (uint32_t q = 0; q < 32; ++q) {
-                const uint4 y = s4[q];
-                const uint32_t c = cb + q * 128u;
-                if (y.x & lb) out[off + __popc(y.x & lt)] = c;
-                off += __popc(y.x);
-                if (y.y & lb) out[off + __popc(y.y & lt)] = c + 32u;
-                off += __popc(y.y);
-                if (y.z & lb) out[off + __popc(y.z & lt)] = c + 64u;
-                off += __popc(y.z);
-                if (y.w & lb) out[off + __popc(y.w & lt)] = c + 96u;
-                off += __popc(y.w);
-            }
-            __syncwarp();  // every lane has read the step
-            bm4[q4] = make_uint4(0, 0, 0, 0);
-            continue;
-        }
-        const uint4 x = bm4[q4];
-        const uint32_t pc = __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
-        const uint32_t inc = warp_inclusive_scan(pc);
-        if (T <= BMP_FEW) {
-            // few outputs (a quarter of the steps of R-MAT rows hold <= 8):
-            // every lane writes its own bits in place, no search, no staging
-            uint32_t *o = out + pos + inc - pc;
-            const uint32_t wb = colbase + q4 * 128u;
-            uint32_t cur = x.x, j = 0;
-            for (uint32_t t = 0; t < pc; ++t) {
-                while (!cur) {
-                    ++j;
-                    cur = j == 1 ? x.y : (j == 2 ? x.z : x.w);
-                }
-                o[t] = wb + j * 32u + (uint32_t)(__ffs(cur) - 1);
-                cur &= cur - 1;
-            }
-            if (pc) bm4[q4] = make_uint4(0, 0, 0, 0);
-            continue;
-        }
-        for (uint32_t w0 = 0; w0 < T; w0 += BMP_STAGE) {
-            const uint32_t m = min(BMP_STAGE, T - w0);
-            const uint32_t per = (m + 31) >> 5;  // outputs per lane
-            const uint32_t k = w0 + lane * per;
-            const uint32_t kend = min(k + per, w0 + m);
-            const uint32_t key = min(k, T - 1);
-            // L = first lane whose inclusive count exceeds key
-            uint32_t L = 0;
-#pragma unroll
-            for (uint32_t sft = 16; sft >= 1; sft >>= 1) {
-                const uint32_t v = __shfl_sync(0xFFFFFFFFu, inc, L + sft - 1);
-                if (v <= key) L += sft;
-            }
-            const uint32_t exL = __shfl_sync(0xFFFFFFFFu, inc - pc, L);
-            if (k < kend) {
-                const uint4 y = bm4[st * 32u + L];
-                uint32_t r = key - exL, wv = y.x, widx = (st * 32u + L) * 4u, c;
-                c = __popc(y.x);
-                if (r >= c) {
-                    r -= c; wv = y.y; ++widx; c = __popc(y.y);
-                    if (r >= c) {
-                        r -= c; wv = y.z; ++widx; c = __popc(y.z);
-                        if (r >= c) { r -= c; wv = y.w; ++widx; }
-                    }
-                }
-                uint32_t cur = wv & (0xFFFFFFFFu << nth_set_bit(wv, r));
-                for (uint32_t kk = k; kk < kend; ++kk) {
-                    while (!cur) cur = bm[++widx];  // the step holds more outputs
-                    stage[kk - w0] = colbase + widx * 32u + (uint32_t)(__ffs(cur) - 1);
-                    cur &= cur - 1;
-                }
-            }
-            __syncwarp();
-            uint32_t *const o2 = out + pos + w0 + lane;
-#pragma unroll
-            for (uint32_t u = 0; u < BMP_STAGE / 32; ++u)
-                if (lane + 32 * u < m) o2[32 * u] = stage[lane + 32 * u];
-            __syncwarp();
-        }
-        if (pc) bm4[q4] = make_uint4(0, 0, 0, 0);
+        bitmap_emit_step<true>(bm + st * BMP_STEP_WORDS, s_soff[g + 1] - pos, out + pos,
+                               colbase + st * (BMP_STEP_WORDS * 32u), stage);
     }
 }
 
@@ -1152,7 +1167,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
     const BitmapSmem S(smem, W);
     uint32_t *const bm = S.bm;
     __shared__ uint32_t scratch[33];
-    __shared__ uint32_t s_slot, s_row, s_next;
+    __shared__ uint32_t s_slot, s_row, s_next, s_dslot;
     __shared__ unsigned long long s_spill;
     uint32_t beg, cnt = 0, tmp;
     bin_range(bl, bin_lo, beg, tmp);
@@ -1256,13 +1271,25 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 }
                 if (threadIdx.x == 0) {
                     o.defer[i] = 1;
-                    o.defer_list[atomicAdd(o.defer_count, 1u)] = i;
+                    const uint32_t d = atomicAdd(o.defer_count, 1u);
+                    o.defer_list[d] = i;
+                    s_dslot = d;
+                }
+                __syncthreads();
+                if (o.defer_steps) {
+                    // the step list the expansion would otherwise recount
+                    uint32_t *rec = o.defer_steps + (uint64_t)s_dslot * BMP_STEP_REC;
+                    for (uint32_t g = threadIdx.x; g <= nlist; g += BMP_NT) {
+                        if (g < nlist) rec[1 + g] = S.s_list[g];
+                        rec[1 + BMP_MAX_STEPS + g] = S.s_soff[g];
+                    }
+                    if (threadIdx.x == 0) rec[0] = nlist;
                 }
                 total += ctot;
                 __syncthreads();
                 continue;
             }
-            bitmap_emit(bm, bm4, nlist, S.s_list, S.s_soff, &s_next, stage, out, (uint32_t)c0);
+            bitmap_emit(bm, nlist, S.s_list, S.s_soff, &s_next, stage, out, (uint32_t)c0);
             total += ctot;
             __syncthreads();
         }
@@ -1309,8 +1336,60 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_expand_kernel(
         __syncthreads();
         uint32_t nlist;
         bitmap_list_steps<BMP_NT>(bm4, Wr / BMP_STEP_WORDS, S.s_list, S.s_soff, &s_next, scratch, nlist);
-        bitmap_emit(bm, bm4, nlist, S.s_list, S.s_soff, &s_next, stage, ccols + off[i], 0u);
+        bitmap_emit(bm, nlist, S.s_list, S.s_soff, &s_next, stage, ccols + off[i], 0u);
         __syncthreads();
+    }
+}
+
+// Deferred rows by warp: the numeric kernel stored each deferred row's
+// bitmap in its slot and, in record d of `steps` (row list[d]), the row's
+// non-empty steps and their output offsets.  Each warp claims rows from
+// `counter`; it holds 32 of the row's step entries at a time in registers,
+// copies each step's 512 bytes into its own shared buffer (the next step's
+// copy in flight while the current one is emitted) and emits it at its place
+// in C (bitmap_emit_step).  No block barrier and no whole-row reload, so the
+// warps of an SM work on different rows at their own pace.
+template <int NT>
+__global__ void __launch_bounds__(NT) bitmap_expand_steps_kernel(const uint32_t *__restrict__ list,
+                                                                 const uint32_t *__restrict__ count,
+                                                                 const uint32_t *__restrict__ steps,
+                                                                 const uint64_t *__restrict__ slot_off,
+                                                                 const uint32_t *__restrict__ slots,
+                                                                 const uint64_t *__restrict__ off,
+                                                                 uint32_t *__restrict__ ccols, uint32_t *counter) {
+    constexpr int NW = NT / 32;
+    __shared__ __align__(16) uint32_t s_bm[NW][BMP_STEP_WORDS];
+    __shared__ uint32_t s_stage[NW][BMP_STAGE];
+    const uint32_t lane = lane_id(), w = warp_id();
+    uint4 *const sb4 = reinterpret_cast<uint4 *>(s_bm[w]);
+    const uint32_t cnt = *count;
+    for (;;) {
+        uint32_t d = 0;
+        if (lane == 0) d = atomicAdd(counter, 1u);
+        d = __shfl_sync(0xFFFFFFFFu, d, 0);
+        if (d >= cnt) break;
+        const uint32_t *rec = steps + (uint64_t)d * BMP_STEP_REC;
+        const uint32_t nlist = rec[0];
+        const uint32_t i = list[d];
+        const uint4 *src = reinterpret_cast<const uint4 *>(slots + slot_off[i]) + lane;
+        uint32_t *const out = ccols + off[i];
+        for (uint32_t g0 = 0; g0 < nlist; g0 += 32) {
+            const uint32_t gl = g0 + lane, m = min(32u, nlist - g0);
+            const uint32_t my_st = gl < nlist ? rec[1 + gl] : 0u;
+            const uint32_t my_pos = gl < nlist ? rec[1 + BMP_MAX_STEPS + gl] : 0u;
+            const uint32_t my_end = gl < nlist ? rec[2 + BMP_MAX_STEPS + gl] : 0u;
+            uint4 nxt = src[__shfl_sync(0xFFFFFFFFu, my_st, 0) * 32u];
+            for (uint32_t k = 0; k < m; ++k) {
+                const uint32_t st = __shfl_sync(0xFFFFFFFFu, my_st, k);
+                const uint32_t pos = __shfl_sync(0xFFFFFFFFu, my_pos, k);
+                const uint32_t T = __shfl_sync(0xFFFFFFFFu, my_end, k) - pos;
+                sb4[lane] = nxt;
+                if (k + 1 < m) nxt = src[__shfl_sync(0xFFFFFFFFu, my_st, k + 1) * 32u];
+                __syncwarp();
+                bitmap_emit_step<false>(s_bm[w], T, out + pos, st * (BMP_STEP_WORDS * 32u), s_stage[w]);
+                __syncwarp();  // the buffers serve the warp's next step
+            }
+        }
     }
 }
 
@@ -1432,7 +1511,7 @@ __global__ void __launch_bounds__(1024, 1) bitmap_cluster_kernel(BinLists bl, in
             }
             out = o.arena + s_spill;
         }
-        bitmap_emit(bm, bm4, nlist, S.s_list, S.s_soff, &s_next, stage, out + before, rank << CLB_CHUNK_SHIFT);
+        bitmap_emit(bm, nlist, S.s_list, S.s_soff, &s_next, stage, out + before, rank << CLB_CHUNK_SHIFT);
         if (o.row_cap && rank == 0 && threadIdx.x == 0) o.row_nnz[i] = (uint32_t)total;
         __syncthreads();
     }

@@ -299,6 +299,22 @@ int launch_bitmap_expand(clb_controls *ctl, const uint32_t *list, const uint32_t
     return CLB_SUCCESS;
 }
 
+int launch_bitmap_expand_steps(clb_controls *ctl, const uint32_t *list, const uint32_t *count, const uint32_t *steps,
+                               const uint64_t *slot_off, const uint32_t *slots, const uint64_t *off,
+                               uint32_t *ccols) {
+    constexpr int NT = 256;
+    auto kern = bitmap_expand_steps_kernel<NT>;
+    Temp<uint32_t> ctr;
+    CLB_RETURN_IF(ctr.alloc(ctl, 1));
+    CLB_TRY_CUDA(cudaMemsetAsync(ctr.ptr, 0, sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
+    const unsigned grid = (unsigned)ctl->sm_count * (unsigned)occupancy(kern, NT, 0);
+    ProfScope ps(ctl, "bitmap_expand");
+    kern<<<grid, NT, 0, ctl->stream>>>(list, count, steps, slot_off, slots, off, ccols, ctr.ptr);
+    ctl->launches += 1;
+    CLB_CHECK_LAUNCH();
+    return CLB_SUCCESS;
+}
+
 int launch_assemble(clb_controls *ctl, const uint32_t *work, const uint32_t *pos, const uint64_t *off,
                     const uint32_t *a_rows, uint64_t n, uint64_t *c_rpt, uint32_t *c_rows, uint64_t nzr, uint64_t nnz) {
     unsigned grid = persistent_grid(ctl, 8, ceil_div_u(n, 256));

@@ -366,7 +366,7 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     // bitmap rows denser than their bitmap keep the bitmap in their slot
     // (without room for the row flags every row is emitted in place)
     const uint64_t nbmp = (uint64_t)hinfo[BIN_BMP_XL] + hinfo[BIN_BMP_L] + hinfo[BIN_BMP];
-    Temp<uint32_t> defer, dlist, dcount;
+    Temp<uint32_t> defer, dlist, dcount, dsteps;
     const bool deferring =
         nbmp && defer.try_alloc(ctl, n) && dlist.try_alloc(ctl, nbmp) && dcount.try_alloc(ctl, 1);
     if (deferring) {
@@ -375,6 +375,9 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
         num.defer = defer.ptr;
         num.defer_list = dlist.ptr;
         num.defer_count = dcount.ptr;
+        // step records for the by-step expansion (without room for them the
+        // rows are expanded a row per CTA)
+        if (dsteps.try_alloc(ctl, nbmp * BMP_STEP_REC)) num.defer_steps = dsteps.ptr;
     } else {
         defer.reset();
     }
@@ -477,7 +480,10 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) rc = fail(CLB_RUN_KERNEL_FAILURE, cudaGetErrorString(e));
         }
-        if (rc == CLB_SUCCESS && deferring)
+        if (rc == CLB_SUCCESS && deferring && dsteps.ptr)
+            rc = launch_bitmap_expand_steps(ctl, dlist.ptr, dcount.ptr, dsteps.ptr, slot_off.ptr, pre.ptr, off.ptr,
+                                            c_cols.ptr);
+        else if (rc == CLB_SUCCESS && deferring)
             rc = launch_bitmap_expand(ctl, dlist.ptr, dcount.ptr, nbmp, slot_off.ptr, pre.ptr, off.ptr, t.row_ncols,
                                       B.ncols, c_cols.ptr);
     }
