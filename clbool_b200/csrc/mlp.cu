@@ -360,10 +360,13 @@ __global__ void __launch_bounds__(FT_NT) features_long_kernel(AView a, BRows b, 
 // their exact bound min(P, ncols): they hold a small share of the products,
 // and the ESC accumulators that serve them need no capacity check.
 // row_ncols (may be null): per row, the columns of its product (a stacked
-// batch of pairs).
+// batch of pairs).  defer: a single-chunk bitmap row of at least
+// BMP_DEFER_MIN_WORDS words whose capacity reaches 1 / BMP_DEFER_DIV of its
+// bitmap's words gets at least the bitmap's words, so that it can keep its
+// bitmap in the slot.
 __global__ void capacity_kernel(const float *__restrict__ pred, const uint32_t *__restrict__ work, uint64_t n,
                                 uint64_t ncols, const uint32_t *__restrict__ row_ncols, float margin_log2, float slack,
-                                uint32_t exact_below, uint32_t *__restrict__ cap) {
+                                uint32_t exact_below, bool defer, uint32_t *__restrict__ cap) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t ub = min((uint64_t)work[i], row_ncols ? (uint64_t)row_ncols[i] : ncols);
         if (work[i] <= exact_below) {
@@ -375,6 +378,11 @@ __global__ void capacity_kernel(const float *__restrict__ pred, const uint32_t *
         uint64_t k = c <= 1.0f ? 1 : (c >= 4.0e9f ? ub : (uint64_t)ceilf(c));
         if (k > ub) k = ub;
         if (ub == 0) k = 0;
+        if (defer) {
+            const uint64_t rn = row_ncols ? (uint64_t)row_ncols[i] : ncols;
+            const uint32_t wr = bitmap_words(rn);
+            if (wr >= BMP_DEFER_MIN_WORDS && rn <= (uint64_t)wr * 32 && k * BMP_DEFER_DIV >= wr && k < wr) k = wr;
+        }
         cap[i] = (uint32_t)k;
     }
 }
@@ -420,7 +428,7 @@ float learned_density_feature(const clb_dcsr &B) {
 
 int learned_caps(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                  const clb_sizer *sizer, float margin_log2, float slack, const Tuning &t, const BatchRows *batch,
-                 uint32_t *work, uint32_t *cap) {
+                 uint32_t *work, uint32_t *cap, bool defer) {
     const uint64_t n = A.nzr;
     Temp<float> feat, pred;
     Temp<uint32_t> list, count;
@@ -440,7 +448,7 @@ int learned_caps(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const 
     predict_rows_kernel<<<grid_for(ctl, n, MLP_NT, 4), MLP_NT, 0, ctl->stream>>>(sizer->params, feat.ptr, list.ptr,
                                                                                 count.ptr, pred.ptr);
     capacity_kernel<<<grid_for(ctl, n), 256, 0, ctl->stream>>>(pred.ptr, work, n, B.ncols, t.row_ncols, margin_log2,
-                                                              slack, t.bitmap_min, cap);
+                                                              slack, t.bitmap_min, defer, cap);
     ctl->launches += 2;
     CLB_CHECK_LAUNCH();
     return CLB_SUCCESS;
@@ -469,7 +477,7 @@ int spgemm_learned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, cons
     CLB_RETURN_IF(work.alloc(ctl, n));
     CLB_RETURN_IF(cap.alloc(ctl, n));
     CLB_RETURN_IF(tot.alloc(ctl, 1));
-    CLB_RETURN_IF(learned_caps(ctl, A, B, a, b, sizer, margin_log2, slack, t, batch, work.ptr, cap.ptr));
+    CLB_RETURN_IF(learned_caps(ctl, A, B, a, b, sizer, margin_log2, slack, t, batch, work.ptr, cap.ptr, true));
     // products: the single-pass driver reports them; sum the workload here
     CLB_RETURN_IF(wsum.alloc(ctl, n));
     CLB_RETURN_IF(scan_u32_to_u64(ctl, work.ptr, wsum.ptr, n, tot.ptr));

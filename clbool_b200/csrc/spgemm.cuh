@@ -70,9 +70,11 @@ float learned_density_feature(const clb_dcsr &B);
 // its slot (predicted for rows over t.bitmap_min products, exact below;
 // never above min(work, the row's columns)); batch = per-row pair context
 // of a stacked batch, or null.
+// defer: the caller keeps the bitmaps of dense enough bitmap rows in their
+// slots (RowOut::defer), so those rows get room for their bitmap.
 int learned_caps(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
                  const clb_sizer *sizer, float margin_log2, float slack, const Tuning &t, const BatchRows *batch,
-                 uint32_t *work, uint32_t *cap);
+                 uint32_t *work, uint32_t *cap, bool defer = false);
 // The learned single pass: learned capacities, one numeric pass with the
 // spill arena, exact fallback of the rows that outgrew both, compaction.
 int spgemm_learned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const clb_sizer *sizer,

@@ -137,10 +137,12 @@ struct RowOut {
     uint64_t arena_cap = 0;                        // entries
     const uint32_t *row_ncols = nullptr;           // columns of row i's product (batched pairs), or all
     const uint32_t *row_products = nullptr;        // products of row i (picks the bitmap insertion path)
-    // Single-pass forms: bitmap rows with at least as many columns as bitmap
-    // words (bitmaps of at least BMP_DEFER_MIN_WORDS words) store the bitmap
-    // in their slot instead (defer[i] = 1, listed in defer_list[0,
-    // *defer_count)); bitmap_expand_kernel writes their columns.
+    // Single-pass forms: bitmap rows whose slot holds their bitmap (of at
+    // least BMP_DEFER_MIN_WORDS words) and whose columns reach 1 /
+    // BMP_DEFER_DIV of its words store the bitmap in their slot instead
+    // (defer[i] = 1, listed in defer_list[0, *defer_count));
+    // bitmap_expand_steps_kernel (or bitmap_expand_kernel) writes their
+    // columns.
     uint32_t *defer = nullptr;
     uint32_t *defer_list = nullptr;
     uint32_t *defer_count = nullptr;
@@ -635,6 +637,9 @@ constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (column
 // Bitmaps at least this wide (2^18 columns) may be kept for bitmap_expand_kernel:
 // narrower ones cost more per row to reload than their compaction.
 constexpr uint32_t BMP_DEFER_MIN_WORDS = 8192;
+// Rows with at least 1 / BMP_DEFER_DIV of their bitmap's words in outputs
+// are deferred when their slot holds the bitmap.
+constexpr uint32_t BMP_DEFER_DIV = 4;
 constexpr uint32_t BMP_FEW = 16;  // steps with at most this many outputs skip the balanced windows
 constexpr uint32_t BMP_DENSE = 1024;  // steps with at least this many outputs (1/4 of the bits) emit bit-parallel
 constexpr uint32_t BMP_SHORT = 64;            // products per A entry below which a row uses the per-product mapping
@@ -1259,11 +1264,12 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 in_slot = false;
                 if (threadIdx.x == 0) o.spill[i] = s_spill;
             }
-            if (!MULTI && o.defer && in_slot && ctot >= Wr && Wr >= BMP_DEFER_MIN_WORDS) {
-                // the bitmap is no larger than the row's columns: it is
-                // stored in the row's slot (16-byte aligned, >= ctot >= Wr
-                // words) and expanded straight into C once C's offsets are
-                // known, so these columns skip the slot-to-C compaction
+            if (!MULTI && o.defer && in_slot && o.row_cap && o.row_cap[i] >= Wr &&
+                (uint64_t)ctot * BMP_DEFER_DIV >= Wr && Wr >= BMP_DEFER_MIN_WORDS) {
+                // the slot holds the bitmap (16-byte aligned, >= Wr words):
+                // it is stored there and expanded straight into C once C's
+                // offsets are known, so these columns skip the slot-to-C
+                // compaction
                 uint4 *dst = reinterpret_cast<uint4 *>(out);
                 for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) {
                     dst[w4] = bm4[w4];
