@@ -844,7 +844,12 @@ def run_cfpq(args) -> dict:
                              ("batched_autotuned", best_b, None), ("batched_learned", None, sizer),
                              ("batched_learned_autotuned", best_b, sizer)):
         m = "batched" if method.startswith("batched") else "fused"
-        cfpq.closure(ctl, labels, max_iters=2, method=m, tune=tune, sizer=sz)  # warm-up
+        # warm-up: the whole bounded closure, so that the timed run's largest
+        # product (the last iteration's) is not the first of its size in the
+        # process (the first one grows the stream-ordered memory pool, which
+        # took from 0.05 to 1.5 s here)
+        del_c, _ = cfpq.closure(ctl, labels, max_iters=64, max_products=int(4e9), method=m, tune=tune, sizer=sz)
+        del del_c
         torch.cuda.synchronize()
         C, hist = cfpq.closure(ctl, labels, max_iters=64, max_products=int(4e9), method=m, tune=tune, sizer=sz)
         out[method] = {"iterations": hist, "final_nnz": C.nnz(), "stop": hist[-1].get("stop"),

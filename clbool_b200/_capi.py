@@ -69,6 +69,7 @@ _SIGS = {
     "clb_controls_get_stream": (vp, [vp]),
     "clb_controls_set_allocator": (C.c_int, [vp, vp, vp, vp]),
     "clb_controls_sync": (C.c_int, [vp]),
+    "clb_controls_trim": (C.c_int, [vp]),
     "clb_controls_device": (C.c_int, [vp]),
     "clb_device_count": (C.c_int, [P(C.c_int)]),
     "clb_device_info": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, P(C.c_int), P(C.c_uint64)]),

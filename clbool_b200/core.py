@@ -63,6 +63,11 @@ class Controls:
     def sync(self) -> None:
         check(lib.clb_controls_sync(self._h), "sync")
 
+    def trim(self) -> None:
+        """Wait for the stream, then hand the memory pool's cached, unused
+        device memory back to the driver (clb_controls_trim)."""
+        check(lib.clb_controls_trim(self._h), "trim")
+
     def set_stream(self, stream_ptr: int) -> None:
         check(lib.clb_controls_set_stream(self._h, C.c_void_p(stream_ptr or None)), "set_stream")
 

@@ -269,6 +269,16 @@ int clb_controls_sync(clb_controls *ctl) {
     return CLB_SUCCESS;
 }
 
+int clb_controls_trim(clb_controls *ctl) {
+    if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
+    DeviceGuard g(ctl);
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    cudaMemPool_t pool;
+    CLB_TRY_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctl->device), CLB_RUN_KERNEL_FAILURE);
+    CLB_TRY_CUDA(cudaMemPoolTrimTo(pool, 0), CLB_RUN_KERNEL_FAILURE);
+    return CLB_SUCCESS;
+}
+
 int clb_graph_begin(clb_controls *ctl) {
     if (!ctl) return fail(CLB_INVALID_ARGUMENT, "controls is NULL");
     DeviceGuard g(ctl);

@@ -87,6 +87,8 @@ struct Controls {
     }
     clb_controls *get() const { return handle.get(); }
     void sync() const { details::check(clb_controls_sync(get())); }
+    // hands the memory pool's cached, unused device memory back (clb_controls_trim)
+    void trim() const { details::check(clb_controls_trim(get())); }
 };
 
 inline Controls create_controls(uint32_t platform_id = 0, uint32_t device_id = 0) {

@@ -123,6 +123,13 @@ CLB_API void *clb_controls_get_stream(clb_controls *ctl);
  * reference allocates cl::Buffer objects itself). */
 CLB_API int clb_controls_set_allocator(clb_controls *ctl, clb_alloc_fn alloc, clb_free_fn release, void *ctx);
 CLB_API int clb_controls_sync(clb_controls *ctl);
+/* No counterpart in the reference.  Waits for the controls' stream, then
+ * returns the device memory that the library's stream-ordered pool keeps
+ * cached (freed buffers are kept for reuse and never handed back on their
+ * own) to the driver, for a caller that needs that memory elsewhere (another
+ * library, another process).  Buffers still in use are not touched; the next
+ * large requests grow the pool again. */
+CLB_API int clb_controls_trim(clb_controls *ctl);
 /* CUDA graphs over the controls' stream (no counterpart in the reference,
  * which enqueues OpenCL commands one by one).  clb_graph_begin starts
  * capturing the stream (thread-local mode); operations that read nothing back
