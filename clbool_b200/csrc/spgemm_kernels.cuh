@@ -634,8 +634,8 @@ constexpr uint32_t BMP_MAX_STEPS = BMP_MAX_WORDS / BMP_STEP_WORDS;
 // (BMP_MAX_STEPS) | their first outputs and the row's total (BMP_MAX_STEPS + 1).
 constexpr uint32_t BMP_STEP_REC = 2 + 2 * BMP_MAX_STEPS;
 constexpr uint32_t BMP_STAGE = 256;           // per-warp output staging (columns)
-// Bitmaps at least this wide (2^18 columns) may be kept for bitmap_expand_kernel:
-// narrower ones cost more per row to reload than their compaction.
+// Bitmaps at least this wide (2^18 columns) may be kept for the expansion
+// kernels: narrower ones cost more per row to reload than their compaction.
 constexpr uint32_t BMP_DEFER_MIN_WORDS = 8192;
 // Rows with at least 1 / BMP_DEFER_DIV of their bitmap's words in outputs
 // are deferred when their slot holds the bitmap.
@@ -1313,12 +1313,14 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
     }
 }
 
-// Deferred bitmap rows (RowOut::defer): each row's bitmap, stored in its
-// slot by bitmap_cta_kernel, is loaded back into shared memory and emitted
-// at the row's final offset in C, once the offsets are known.  One row per
-// CTA at a time, rows taken from `counter`.  (Emitting straight from the
-// bitmap in global memory, one warp per step and no block barriers, was
-// measured slower: the emission's bitmap walk waits on every load.)
+// Deferred bitmap rows (RowOut::defer) when there was no room for their
+// step records: each row's bitmap, stored in its slot by bitmap_cta_kernel,
+// is loaded back into shared memory, its steps are counted again and it is
+// emitted at the row's final offset in C, once the offsets are known.  One
+// row per CTA at a time, rows taken from `counter`.  (Emitting straight
+// from the bitmap in global memory, one warp per step and no block
+// barriers, was measured slower: the emission's bitmap walk waits on every
+// load.)  bitmap_expand_steps_kernel below is the usual form.
 template <int BMP_NT>
 __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_expand_kernel(
     const uint32_t *__restrict__ list, const uint32_t *__restrict__ count, const uint64_t *__restrict__ slot_off,

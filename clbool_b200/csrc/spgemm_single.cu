@@ -221,7 +221,7 @@ __global__ void compact_rows_kernel(const uint32_t *__restrict__ row_nnz, const 
     const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x / 32);
     for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + warp_id(); i < n; i += nw) {
         const uint32_t len = row_nnz[i];
-        if (!len || (defer && defer[i])) continue;  // deferred rows: bitmap_expand_kernel
+        if (!len || (defer && defer[i])) continue;  // deferred rows: the expansion kernels
         uint32_t *dst = ccols + off[i];
         if (ovf && ovf[i]) {
             const uint32_t *src = sub_ccols + sub_crpt[pos[i]];
