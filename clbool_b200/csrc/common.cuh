@@ -143,6 +143,14 @@ int read_scalars(clb_controls *ctl, const uint64_t *d_src, uint64_t *h_dst, int 
 // engine (clb_dcsr_spgemm_to_host copies row blocks while the next block's
 // call reads its sizes back).  Synchronises the stream.
 int read_small(clb_controls *ctl, const void *d_src, void *h_dst, size_t bytes);
+// Several such reads (each a multiple of 4 bytes, at most 512 bytes in all)
+// with one synchronisation.
+struct SmallRead {
+    const void *src;
+    void *dst;
+    size_t bytes;
+};
+int read_small_multi(clb_controls *ctl, const SmallRead *r, int n);
 // Clears, then after the call checks, the device status word.
 int clear_status(clb_controls *ctl);
 int check_status(clb_controls *ctl, const char *op);

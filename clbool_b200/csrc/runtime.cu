@@ -63,6 +63,28 @@ int read_small(clb_controls *ctl, const void *d_src, void *h_dst, size_t bytes) 
     return CLB_SUCCESS;
 }
 
+int read_small_multi(clb_controls *ctl, const SmallRead *r, int n) {
+    size_t at = 0;
+    for (int k = 0; k < n; ++k) {
+        if (r[k].bytes == 0) continue;
+        if ((r[k].bytes & 3) || at + r[k].bytes > 64 * sizeof(uint64_t))
+            return fail(CLB_INVALID_ARGUMENT, "read_small_multi: bad size");
+        stage_words_kernel<<<1, 32, 0, ctl->stream>>>(
+            static_cast<const uint32_t *>(r[k].src), (uint32_t)(r[k].bytes / 4),
+            reinterpret_cast<volatile uint32_t *>(ctl->d_h_scalars) + at / 4);
+        CLB_TRY_CUDA(cudaGetLastError(), CLB_RUN_KERNEL_FAILURE);
+        ctl->launches += 1;
+        at += r[k].bytes;
+    }
+    CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
+    at = 0;
+    for (int k = 0; k < n; ++k) {
+        memcpy(r[k].dst, reinterpret_cast<const char *>(ctl->h_scalars) + at, r[k].bytes);
+        at += r[k].bytes;
+    }
+    return CLB_SUCCESS;
+}
+
 int read_scalars(clb_controls *ctl, const uint64_t *d_src, uint64_t *h_dst, int count) {
     return read_small(ctl, d_src, h_dst, sizeof(uint64_t) * (size_t)count);
 }

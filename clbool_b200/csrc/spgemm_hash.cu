@@ -259,9 +259,9 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     CLB_TRY_CUDA(cudaMemsetAsync(row_nnz.ptr, 0, n * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     // rows per bin: only the bins with rows are launched, sized to them
     uint32_t hinfo[NUM_BINS];
-    CLB_RETURN_IF(read_small(ctl, info.ptr, hinfo, sizeof(hinfo)));
     uint64_t products = 0;
-    CLB_RETURN_IF(read_scalars(ctl, scal.ptr, &products, 1));
+    const SmallRead rd[2] = {{info.ptr, hinfo, sizeof(hinfo)}, {scal.ptr, &products, sizeof(products)}};
+    CLB_RETURN_IF(read_small_multi(ctl, rd, 2));
     Temp<uint64_t> wdense;
     Temp<uint2> wpairs;
     CLB_RETURN_IF(prepare_b_words(ctl, B, hinfo, wdense, wpairs, b, products));

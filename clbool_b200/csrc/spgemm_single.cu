@@ -343,11 +343,11 @@ int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, 
     CLB_CHECK_LAUNCH();
     CLB_RETURN_IF(scan_u32_to_u64(ctl, capp.ptr, slot_off.ptr, n, scal.ptr + 1));  // slot offsets, slots
     uint64_t h[2], capacity = 0;
-    CLB_RETURN_IF(read_scalars(ctl, scal.ptr, h, 2));
-    CLB_RETURN_IF(read_scalars(ctl, scal.ptr + 7, &capacity, 1));
-    const uint64_t nzr = h[0], slots = h[1];
     uint32_t hinfo[NUM_BINS];  // rows per bin: only bins with rows are launched
-    CLB_RETURN_IF(read_small(ctl, info.ptr, hinfo, sizeof(hinfo)));
+    const SmallRead rd[3] = {{scal.ptr, h, sizeof(h)}, {scal.ptr + 7, &capacity, sizeof(capacity)},
+                             {info.ptr, hinfo, sizeof(hinfo)}};
+    CLB_RETURN_IF(read_small_multi(ctl, rd, 3));
+    const uint64_t nzr = h[0], slots = h[1];
     BRows b = b_in;
     Temp<uint64_t> wdense;
     Temp<uint2> wpairs;
