@@ -22,6 +22,7 @@ constexpr int RS_WARPS = RS_NT / 32;
 constexpr int RS_ROUNDS = 8;                       // 32-key rounds per warp
 constexpr uint64_t RS_TILE = 32ull * RS_ROUNDS * RS_WARPS;  // 2048 keys
 constexpr int RADIX = 256;
+static_assert(RS_NT == RADIX, "the downsweep gives each thread one digit");
 
 __global__ void max_pair_kernel(const uint32_t *__restrict__ rows, const uint32_t *__restrict__ cols, uint64_t n,
                                 unsigned int *__restrict__ out) {
@@ -71,11 +72,18 @@ __global__ void __launch_bounds__(RS_NT) radix_upsweep_kernel(const uint64_t *__
 }
 
 // Stable scatter of one tile; offs = exclusive scan of counts (digit-major).
+// The tile's keys are first placed in shared memory in their sorted order
+// (digit buckets one after another), then written out by consecutive
+// threads, so the keys of one digit leave as runs of consecutive addresses
+// instead of one scattered 8-byte store per key.
 __global__ void __launch_bounds__(RS_NT) radix_downsweep_kernel(const uint64_t *__restrict__ in, uint64_t *__restrict__ out,
                                                                 uint64_t n, int shift, uint32_t ntiles,
                                                                 const uint32_t *__restrict__ offs) {
     __shared__ uint32_t whist[RS_WARPS][RADIX];
     __shared__ uint32_t goff[RADIX];
+    __shared__ uint32_t dstart[RADIX];     // first tile position of each digit
+    __shared__ uint32_t scratch[33];
+    __shared__ uint64_t skeys[RS_TILE];
     const uint32_t lane = lane_id(), w = warp_id();
     for (int d = threadIdx.x; d < RS_WARPS * RADIX; d += RS_NT) (&whist[0][0])[d] = 0;
     goff[threadIdx.x] = offs[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
@@ -101,8 +109,8 @@ __global__ void __launch_bounds__(RS_NT) radix_downsweep_kernel(const uint64_t *
         rank[r] = old + (uint32_t)__popc(peers & lt);
     }
     __syncthreads();
+    uint32_t run = 0;
     {   // per digit: exclusive prefix over warps (warp order = key order)
-        uint32_t run = 0;
 #pragma unroll
         for (int q = 0; q < RS_WARPS; ++q) {
             uint32_t c = whist[q][threadIdx.x];
@@ -110,14 +118,23 @@ __global__ void __launch_bounds__(RS_NT) radix_downsweep_kernel(const uint64_t *
             run += c;
         }
     }
+    // digit starts inside the tile (RS_NT == RADIX: thread d holds digit d)
+    uint32_t tile_keys;
+    dstart[threadIdx.x] = block_exclusive_scan<uint32_t, RS_NT>(run, scratch, &tile_keys);
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < RS_ROUNDS; ++r) {
         uint64_t i = base + (uint64_t)r * 32 + lane;
         if (i < n) {
             uint32_t digit = (uint32_t)((key[r] >> shift) & (RADIX - 1));
-            out[(uint64_t)goff[digit] + whist[w][digit] + rank[r]] = key[r];
+            skeys[dstart[digit] + whist[w][digit] + rank[r]] = key[r];
         }
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < tile_keys; t += RS_NT) {
+        const uint64_t k = skeys[t];
+        const uint32_t digit = (uint32_t)((k >> shift) & (RADIX - 1));
+        out[(uint64_t)goff[digit] + (t - dstart[digit])] = k;
     }
 }
 
