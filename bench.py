@@ -181,6 +181,9 @@ def make_mxm(form: str, ctl, cb, sizer_path: str, tune=None):
                                                                              tune=tune)
     if form == "esc":
         return lambda A, B, stats=None: cb.dcsr.matrix_multiplication(ctl, None, A, B, stats=stats)
+    if form == "two_pass_kept":
+        kept = cb.dcsr.tuning("two_pass_kept")
+        return lambda A, B, stats=None: cb.dcsr.matrix_multiplication_tuned(ctl, None, A, B, kept, stats=stats)
     return lambda A, B, stats=None: cb.dcsr.matrix_multiplication_hash(ctl, None, A, B, stats=stats)
 
 
@@ -317,6 +320,20 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                    f"{args.form}_over_two_pass": value / v2,
                    "kernels_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in
                                            sorted(run2["prof"].items(), key=lambda kv: -kv[1][1])}}
+        if args.form != "two_pass_kept":
+            # the exact two-pass form keeping its symbolic pass's bitmaps
+            mxm3 = make_mxm("two_pass_kept", ctl, cb, args.sizer)
+            for _ in range(max(1, args.warmup // 2)):
+                c = mxm3(A, A_full)
+                del c
+            ctl.sync()
+            run3 = timed_steps(ctl, mxm3, A, A_full, args.steps, l2_flush, barrier, srows, dev, False)
+            t3, _, _ = reduce_over_ranks(dist, dev, sum(run3["ev_ms"]), my_products, 0)
+            v3 = products_all / (t3 / args.steps / 1e3)
+            compare["two_pass_kept"] = {
+                "value": v3, "ms_per_step": t3 / args.steps, f"{args.form}_over_two_pass_kept": value / v3,
+                "kernels_ms_per_step": {k: round(v[1] / args.steps, 3) for k, v in
+                                        sorted(run3["prof"].items(), key=lambda kv: -kv[1][1])}}
 
     # roofline of the dominant kernel (largest device time in the timed steps)
     peak, peak_kind = peaks()
@@ -367,7 +384,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "kernel_ms_per_step_sum": sum(run["kern_ms"]) / args.steps,
         "e2e": e2e, "gpu_launches": run["launches"], "clocks": run["clocks"], "wall_s": run["wall"],
     }
-    if args.form != "two_pass":
+    if args.form in ("learned", "esc"):
         line["form_stats"] = {k: st.get(k) for k in ("capacity", "fallback_rows", "spilled_rows", "nzr", "nnz")}
     if compare is not None:
         line["compare"] = compare
@@ -403,7 +420,8 @@ def run_e2e(args, ctl, cb, n, srpt, srows, scols, A_full, products, dist, dev, m
     h_c = pinned(c_bytes)
     del c0
     sizer = sizing.RowSizer.load(ctl, args.sizer) if args.form == "learned" else None
-    tune = batched.tuning(form="single_pass") if args.form == "esc" else None
+    tune = ({"esc": batched.tuning(form="single_pass"), "two_pass_kept": batched.tuning(form="two_pass_kept")}
+            .get(args.form))
     steps = max(1, min(args.steps, 3))
     times = []
     for _ in range(steps):
@@ -1033,7 +1051,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=20)
-    ap.add_argument("--form", default=None, choices=["two_pass", "learned", "esc"],
+    ap.add_argument("--form", default=None, choices=["two_pass", "two_pass_kept", "learned", "esc"],
                     help="default: learned when the packaged predictor checkpoint exists, else two_pass")
     ap.add_argument("--sizer", default=os.path.join(ROOT, "clbool_b200", "sizer_rmat.npz"),
                     help="predictor checkpoint of the learned form")

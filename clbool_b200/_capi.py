@@ -51,7 +51,8 @@ class clb_spgemm_tuning(C.Structure):
                 ("reserved", C.c_uint32 * 2)]
 
     def as_dict(self) -> dict:
-        return {"form": "two_pass" if self.form == 0 else "single_pass", "warp_max": self.warp_max,
+        return {"form": {0: "two_pass", 1: "single_pass", 2: "two_pass_kept"}.get(self.form, self.form),
+                "warp_max": self.warp_max,
                 "bitmap_min": self.bitmap_min, "bitmap_threads": self.bitmap_threads,
                 "small_lanes": self.small_lanes, "wide_rows": {1: "cluster", 2: "chunks"}.get(self.wide_rows, "chunks")}
 

@@ -24,10 +24,13 @@ from .core import ClBoolException, Controls, DeviceBuffer, check, matrix_dcsr
 
 def tuning(form: str | int = "two_pass", warp_max: int = 0, bitmap_min: int = 0, bitmap_threads: int = 0,
            small_lanes: int = 0, wide_rows: str = "") -> clb_spgemm_tuning:
-    """A tuning; zero fields take the library defaults."""
+    """A tuning; zero fields take the library defaults.  form: "two_pass",
+    "single_pass" or "two_pass_kept" (the exact two-pass form whose symbolic
+    pass keeps the bitmap rows' bitmaps for its numeric pass)."""
     t = clb_spgemm_tuning()
     lib.clb_spgemm_tuning_default(C.byref(t))
-    t.form = {"two_pass": 0, "single_pass": 1}.get(form, form) if isinstance(form, str) else int(form)
+    t.form = ({"two_pass": 0, "single_pass": 1, "two_pass_kept": 2}.get(form, form) if isinstance(form, str)
+              else int(form))
     if warp_max:
         t.warp_max = warp_max
     if bitmap_min:

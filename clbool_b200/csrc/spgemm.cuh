@@ -44,7 +44,8 @@ int launch_bitmap_expand_steps(clb_controls *ctl, const uint32_t *list, const ui
 // Numeric accumulators without (hash_bins = false) the hash bins.
 int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
                                const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins,
-                               const Tuning &t = Tuning(), const uint32_t *bin_rows = nullptr);
+                               const Tuning &t = Tuning(), const uint32_t *bin_rows = nullptr,
+                               bool bitmap_bins = true);
 // Single-pass forms (spgemm_single.cu): capacity slots, one numeric pass,
 // exact fallback for rows that outgrew their capacity, compaction.
 int spgemm_single_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, const AView &a, const BRows &b,
@@ -108,7 +109,11 @@ int launch_upper_bound_caps(clb_controls *ctl, const uint32_t *work, uint64_t n,
 // Public tuning struct -> internal tuning (zero fields: defaults), and its check.
 Tuning to_tuning(const clb_spgemm_tuning *t);
 int check_tuning(const clb_spgemm_tuning *t);
+// keep: the symbolic pass keeps the bitmap rows' bitmaps (128 KB a row at 2^20
+// columns) for the numeric pass, which expands them instead of inserting
+// their products again; without room for them (or for rows wider than one
+// bitmap chunk, or batched rows of several widths) the plain form runs.
 int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
-                         clb_spgemm_stats *stats, const Tuning &t = Tuning());
+                         clb_spgemm_stats *stats, const Tuning &t = Tuning(), bool keep = false);
 
 }  // namespace clb

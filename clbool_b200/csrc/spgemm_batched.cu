@@ -110,7 +110,7 @@ unsigned stack_grid_x(const clb_controls *ctl, uint64_t largest, uint32_t count)
 // upper-bound slots (ESC accumulators for the rows below bitmap_min).
 int spgemm_tuned(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, uint32_t form, const Tuning &t,
                  clb_dcsr *c, clb_spgemm_stats *st) {
-    if (form == 0) return spgemm_hash_two_pass(ctl, A, B, c, st, t);
+    if (form == 0 || form == 2) return spgemm_hash_two_pass(ctl, A, B, c, st, t, form == 2);
     clb_spgemm_stats s{};
     ctl->launches = 0;
     if (A.nnz == 0 || B.nnz == 0 || A.nzr == 0 || B.nzr == 0) {
@@ -532,7 +532,9 @@ Tuning to_tuning(const clb_spgemm_tuning *t) {
 
 int check_tuning(const clb_spgemm_tuning *t) {
     if (!t) return CLB_SUCCESS;
-    if (t->form > 1) return fail(CLB_INVALID_VALUE, "tuning.form must be 0 (two-pass) or 1 (single pass)");
+    if (t->form > 2)
+        return fail(CLB_INVALID_VALUE,
+                    "tuning.form must be 0 (two-pass), 1 (single pass) or 2 (two-pass keeping its bitmaps)");
     if (t->warp_max && t->warp_max != 32 && t->warp_max != 64 && t->warp_max != 128 && t->warp_max != 256)
         return fail(CLB_INVALID_VALUE, "tuning.warp_max must be 32, 64, 128 or 256");
     if (t->bitmap_min && (t->bitmap_min < 256 || t->bitmap_min > ESC_MAX_PRODUCTS))

@@ -223,7 +223,7 @@ int validate_spgemm(const clb_dcsr &A, const clb_dcsr &B) {
 }
 
 int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
-                         clb_spgemm_stats *stats, const Tuning &t) {
+                         clb_spgemm_stats *stats, const Tuning &t, bool keep) {
     clb_dcsr C{};
     C.nrows = A.nrows;
     C.ncols = B.ncols;
@@ -270,6 +270,24 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     RowOut sym{row_nnz.ptr, nullptr, nullptr, nullptr, nullptr, ctl->d_status};
     sym.row_ncols = t.row_ncols;
     sym.row_products = work.ptr;
+    // bitmaps kept from the symbolic pass for the numeric pass's expansion
+    const uint64_t nbmp = (uint64_t)hinfo[BIN_BMP_XL] + hinfo[BIN_BMP_L] + hinfo[BIN_BMP];
+    const uint32_t kw = bitmap_words(B.ncols);
+    Temp<uint32_t> kbits, krec, klist, kcount;
+    Temp<uint64_t> koff;
+    keep = keep && nbmp && !t.row_ncols && B.ncols <= (uint64_t)kw * 32 && kbits.try_alloc(ctl, nbmp * kw) &&
+           krec.try_alloc(ctl, nbmp * BMP_STEP_REC) && klist.try_alloc(ctl, nbmp) && kcount.try_alloc(ctl, 1) &&
+           koff.try_alloc(ctl, n);
+    const uint32_t h_nbmp = (uint32_t)nbmp;  // (a pageable copy: staged before the call returns)
+    if (keep) {
+        CLB_TRY_CUDA(cudaMemcpyAsync(kcount.ptr, &h_nbmp, 4, cudaMemcpyHostToDevice, ctl->stream),
+                     CLB_RUN_KERNEL_FAILURE);
+        sym.keep = kbits.ptr;
+        sym.keep_stride = kw;
+        sym.keep_off = koff.ptr;
+        sym.defer_steps = krec.ptr;
+        sym.defer_list = klist.ptr;
+    }
     CLB_RETURN_IF(launch_accumulators(ctl, false, bl, a, b, sym, B.ncols, n, t, hinfo));
 
     CLB_RETURN_IF(scan_u32_to_u64(ctl, row_nnz.ptr, off.ptr, n, scal.ptr + 1));
@@ -299,7 +317,13 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     RowOut num{nullptr, off.ptr, nullptr, nullptr, c_cols.ptr, ctl->d_status};
     num.row_ncols = t.row_ncols;
     num.row_products = work.ptr;
-    CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t, hinfo));
+    if (keep) {
+        CLB_RETURN_IF(launch_accumulators_subset(ctl, bl, a, b, num, B.ncols, n, true, t, hinfo, false));
+        CLB_RETURN_IF(launch_bitmap_expand_steps(ctl, klist.ptr, kcount.ptr, krec.ptr, koff.ptr, kbits.ptr, off.ptr,
+                                                 c_cols.ptr));
+    } else {
+        CLB_RETURN_IF(launch_accumulators(ctl, true, bl, a, b, num, B.ncols, n, t, hinfo));
+    }
     CLB_RETURN_IF(check_status(ctl, "matrix_multiplication_hash"));
 
     C.nnz = nnz;

@@ -149,6 +149,14 @@ struct RowOut {
     // Optional: record d (BMP_STEP_REC words) of defer_list[d] gets its
     // non-empty steps and their output offsets (bitmap_expand_steps_kernel).
     uint32_t *defer_steps = nullptr;
+    // Two-pass form keeping its bitmaps (symbolic pass, single-chunk rows):
+    // the row claimed as item k of the bitmap bins stores its bitmap at
+    // keep + k * keep_stride, its step record in defer_steps, its index in
+    // defer_list[k] and the bitmap's offset in keep_off[row]; the numeric
+    // pass expands it at C's row offset instead of inserting it again.
+    uint32_t *keep = nullptr;
+    uint64_t keep_stride = 0;
+    uint64_t *keep_off = nullptr;
 };
 
 // ------------------------------------------------------------- warp ESC ----
@@ -1231,6 +1239,31 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
             }
             if (threadIdx.x == 0 && c0 == 0 && nxt < cnt)
                 asm volatile("prefetch.global.L1 [%0];" ::"l"(bl.list + beg + nxt));
+            if (!NUMERIC && !MULTI && o.keep && Wr <= o.keep_stride) {
+                // two-pass form keeping its bitmaps: count by steps, store the
+                // bitmap and its step record for the numeric pass's expansion
+                uint32_t nlist;
+                const uint32_t ctot =
+                    bitmap_list_steps<BMP_NT>(bm4, nsteps, S.s_list, S.s_soff, &s_next, scratch, nlist);
+                uint4 *dst = reinterpret_cast<uint4 *>(o.keep + (uint64_t)item * o.keep_stride);
+                for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) {
+                    dst[w4] = bm4[w4];
+                    bm4[w4] = make_uint4(0, 0, 0, 0);
+                }
+                uint32_t *rec = o.defer_steps + (uint64_t)item * BMP_STEP_REC;
+                for (uint32_t g = threadIdx.x; g <= nlist; g += BMP_NT) {
+                    if (g < nlist) rec[1 + g] = S.s_list[g];
+                    rec[1 + BMP_MAX_STEPS + g] = S.s_soff[g];
+                }
+                if (threadIdx.x == 0) {
+                    rec[0] = nlist;
+                    o.defer_list[item] = i;
+                    o.keep_off[i] = (uint64_t)item * o.keep_stride;
+                }
+                total += ctot;
+                __syncthreads();
+                continue;
+            }
             if (!NUMERIC || overflowed) {
                 total += bitmap_count_clear<BMP_NT>(bm4, Wr, scratch);
                 continue;

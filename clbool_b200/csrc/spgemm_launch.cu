@@ -204,7 +204,7 @@ int launch_bitmap(clb_controls *ctl, const BinLists &bl, const AView &a, const B
 // without rows are not launched and the grids follow the bins' sizes.
 template <bool NUM>
 int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b, const RowOut &o, uint64_t ncols,
-               uint64_t nmax, const Tuning &t, const uint32_t *hc, bool hash_bins = true) {
+               uint64_t nmax, const Tuning &t, const uint32_t *hc, bool hash_bins = true, bool bitmap_bins = true) {
     auto rows = [&](int bin) -> uint64_t { return hc ? hc[bin] : nmax; };
     // work counters of the dynamically scheduled launches
     Temp<uint32_t> ctr;
@@ -212,7 +212,7 @@ int launch_all(clb_controls *ctl, const BinLists &bl, const AView &a, const BRow
     CLB_TRY_CUDA(cudaMemsetAsync(ctr.ptr, 0, 8 * sizeof(uint32_t), ctl->stream), CLB_RUN_KERNEL_FAILURE);
     // Heavy bins first so the long rows start early.
     const uint64_t nbmp = hc ? (uint64_t)hc[BIN_BMP_XL] + hc[BIN_BMP_L] + hc[BIN_BMP] : nmax;
-    if (nbmp)
+    if (nbmp && bitmap_bins)
         CLB_RETURN_IF(launch_bitmap<NUM>(ctl, bl, a, b, o, ncols, nbmp, ctr.ptr + 0,
                                          NUM ? "bitmap_numeric" : "bitmap_symbolic", t.bitmap_threads,
                                          t.wide_cluster));
@@ -275,8 +275,8 @@ int launch_accumulators(clb_controls *ctl, bool numeric, const BinLists &bl, con
 
 int launch_accumulators_subset(clb_controls *ctl, const BinLists &bl, const AView &a, const BRows &b,
                                const RowOut &o, uint64_t ncols, uint64_t nmax, bool hash_bins, const Tuning &t,
-                               const uint32_t *hc) {
-    return launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t, hc, hash_bins);
+                               const uint32_t *hc, bool bitmap_bins) {
+    return launch_all<true>(ctl, bl, a, b, o, ncols, nmax, t, hc, hash_bins, bitmap_bins);
 }
 
 int launch_bitmap_expand(clb_controls *ctl, const uint32_t *list, const uint32_t *count, uint64_t nmax,

@@ -315,7 +315,13 @@ CLB_API int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a, const 
 /* ------------------------------------------------- tuning and batching -- */
 /* Not in the reference.  Accumulator tuning; every setting gives the same C.
  *   form            0: exact two-pass (hash form), 1: one pass into
- *                   upper-bound slots (ESC form) + compaction
+ *                   upper-bound slots (ESC form) + compaction, 2: exact
+ *                   two-pass whose symbolic pass keeps the bitmap rows'
+ *                   bitmaps (4 bytes per 32 columns per bitmap row: 128 KB
+ *                   a row at 2^20 columns) and whose numeric pass expands
+ *                   them instead of inserting their products again (falls
+ *                   back to 0 without room for them, for products wider than
+ *                   2^20 columns, and inside batches)
  *   warp_max        rows with at most this many products use the warp ESC
  *                   kernels: 32, 64, 128 or 256 (threads per row: 32)
  *   bitmap_min      rows with more products use the bitmap kernel: 256..4096

@@ -120,3 +120,29 @@ def test_refused_word_runs_fall_back_to_entries():
         del got, A, B
     finally:
         ctl.close()
+
+
+def test_refused_kept_bitmaps_fall_back_to_two_passes():
+    """The two-pass form keeping its bitmaps (tuning form 2) without room for
+    them inserts the bitmap rows' products again in its numeric pass."""
+    import clbool_b200 as cb
+    from clbool_b200 import gen
+    r, c = gen.rmat(14, seed=4)
+    n = 1 << 14
+    a = O.coo_to_dcsr(O.Coo(n, n, r, c))
+    want = O.spgemm(a, a)
+    nbmp = int((O.workload(a, a) > 4096).sum())
+    words = n // 32  # bitmap words of a 2^14-column row
+    assert nbmp >= 8
+    ctl = cb.create_controls(0, 0)
+    al = TorchAllocator(ctl.device)
+    try:
+        assert cb.lib.clb_controls_set_allocator(ctl.handle, al.alloc_cb, al.free_cb, None) == 0
+        al.refuse.add(nbmp * words * 4)
+        A = to_device(ctl, a)
+        got = cb.dcsr.matrix_multiplication_tuned(ctl, None, A, A, cb.dcsr.tuning("two_pass_kept"))
+        assert_dcsr_equal(from_device(ctl, got), want, "kept form, bitmaps refused")
+        assert al.refused == [nbmp * words * 4]
+        del got, A
+    finally:
+        ctl.close()

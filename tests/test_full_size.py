@@ -66,6 +66,10 @@ def test_rmat20_forms_identical_and_sound(controls, rmat20, sample20):
     controls.sync()
     same_on_device(C3, C2, "ESC vs two-pass")
     del C3
+    C4 = cb.dcsr.matrix_multiplication_tuned(controls, None, A, A, cb.dcsr.tuning("two_pass_kept"))
+    controls.sync()
+    same_on_device(C4, C2, "two-pass keeping its bitmaps vs two-pass")
+    del C4
 
     # row lengths = the symbolic counts
     rpt = C2.rpt_gpu().to_host(C2.nzr() + 1).astype(np.int64)
