@@ -1247,7 +1247,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                     bitmap_list_steps<BMP_NT>(bm4, nsteps, S.s_list, S.s_soff, &s_next, scratch, nlist);
                 uint4 *dst = reinterpret_cast<uint4 *>(o.keep + (uint64_t)item * o.keep_stride);
                 for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) {
-                    dst[w4] = bm4[w4];
+                    __stcs(dst + w4, bm4[w4]);  // read once, by the expansion
                     bm4[w4] = make_uint4(0, 0, 0, 0);
                 }
                 uint32_t *rec = o.defer_steps + (uint64_t)item * BMP_STEP_REC;
@@ -1305,7 +1305,7 @@ __global__ void __launch_bounds__(BMP_NT, 1024 / BMP_NT) bitmap_cta_kernel(BinLi
                 // compaction
                 uint4 *dst = reinterpret_cast<uint4 *>(out);
                 for (uint32_t w4 = threadIdx.x; w4 < Wr / 4; w4 += BMP_NT) {
-                    dst[w4] = bm4[w4];
+                    __stcs(dst + w4, bm4[w4]);  // read once, by the expansion
                     bm4[w4] = make_uint4(0, 0, 0, 0);
                 }
                 if (threadIdx.x == 0) {
@@ -1419,13 +1419,13 @@ __global__ void __launch_bounds__(NT) bitmap_expand_steps_kernel(const uint32_t 
             const uint32_t my_st = gl < nlist ? rec[1 + gl] : 0u;
             const uint32_t my_pos = gl < nlist ? rec[1 + BMP_MAX_STEPS + gl] : 0u;
             const uint32_t my_end = gl < nlist ? rec[2 + BMP_MAX_STEPS + gl] : 0u;
-            uint4 nxt = src[__shfl_sync(0xFFFFFFFFu, my_st, 0) * 32u];
+            uint4 nxt = __ldcs(src + __shfl_sync(0xFFFFFFFFu, my_st, 0) * 32u);  // bitmaps are read once
             for (uint32_t k = 0; k < m; ++k) {
                 const uint32_t st = __shfl_sync(0xFFFFFFFFu, my_st, k);
                 const uint32_t pos = __shfl_sync(0xFFFFFFFFu, my_pos, k);
                 const uint32_t T = __shfl_sync(0xFFFFFFFFu, my_end, k) - pos;
                 sb4[lane] = nxt;
-                if (k + 1 < m) nxt = src[__shfl_sync(0xFFFFFFFFu, my_st, k + 1) * 32u];
+                if (k + 1 < m) nxt = __ldcs(src + __shfl_sync(0xFFFFFFFFu, my_st, k + 1) * 32u);
                 __syncwarp();
                 bitmap_emit_step<false>(s_bm[w], T, out + pos, st * (BMP_STEP_WORDS * 32u), s_stage[w]);
                 __syncwarp();  // the buffers serve the warp's next step
