@@ -777,8 +777,13 @@ int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, co
     for (uint32_t k = 0; k < count; ++k) widest = std::max(widest, b[k].ncols);
     const std::vector<uint32_t> wides = widest > (1ull << CLB_CHUNK_SHIFT) ? std::vector<uint32_t>{2u, 1u}
                                                                             : std::vector<uint32_t>{2u};
+    // a single pair also tries the two-pass form keeping its bitmaps (form 2),
+    // which only a call outside a batch can use, and is timed that way
+    const bool single = count == 1;
+    const std::vector<uint32_t> forms =
+        single && widest <= (1ull << CLB_CHUNK_SHIFT) ? std::vector<uint32_t>{0u, 1u, 2u} : std::vector<uint32_t>{0u, 1u};
     for (uint32_t wide : wides)
-    for (uint32_t form : {0u, 1u})
+    for (uint32_t form : forms)
         for (uint32_t bmin : {4096u, 1024u})
             for (uint32_t bthr : {1024u, 256u})
                 for (uint32_t wmax : {256u, 64u})
@@ -809,7 +814,8 @@ int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, co
         // candidates within 1% of each other swap places from call to call)
         for (int rep = 0; rep < 4 && rc == CLB_SUCCESS; ++rep) {
             cudaEventRecord(e0, ctl->stream);
-            rc = clb_dcsr_spgemm_batched(ctl, count, a, b, out.data(), &t, nullptr);
+            rc = single ? clb_dcsr_spgemm_tuned(ctl, a, b, &t, out.data(), nullptr)
+                        : clb_dcsr_spgemm_batched(ctl, count, a, b, out.data(), &t, nullptr);
             cudaEventRecord(e1, ctl->stream);
             cudaEventSynchronize(e1);
             float f = 0.f;

@@ -382,7 +382,9 @@ CLB_API int clb_dcsr_union(clb_controls *ctl, uint32_t count, const clb_dcsr *ma
  * pairs and returns the
  * fastest in *best (each candidate: one warm-up call, then the best of three
  * timed calls); tried/ms (optional, max_tried entries) receive each
- * candidate and its device time in ms, *n_tried their number. */
+ * candidate and its device time in ms, *n_tried their number.  A single pair
+ * (count = 1) is timed through clb_dcsr_spgemm_tuned, with form 2 among the
+ * candidates (48 in all) when it has at most 2^20 columns. */
 CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                 clb_spgemm_tuning *best, clb_spgemm_tuning *tried, double *ms, uint32_t max_tried,
                                 uint32_t *n_tried);
