@@ -112,7 +112,7 @@ int check_tuning(const clb_spgemm_tuning *t);
 // keep: the symbolic pass keeps the bitmap rows' bitmaps (128 KB a row at 2^20
 // columns) for the numeric pass, which expands them instead of inserting
 // their products again; without room for them (or for rows wider than one
-// bitmap chunk, or batched rows of several widths) the plain form runs.
+// bitmap chunk) the plain form runs.
 int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B, clb_dcsr *out,
                          clb_spgemm_stats *stats, const Tuning &t = Tuning(), bool keep = false);
 

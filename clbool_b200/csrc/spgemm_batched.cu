@@ -777,11 +777,11 @@ int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, co
     for (uint32_t k = 0; k < count; ++k) widest = std::max(widest, b[k].ncols);
     const std::vector<uint32_t> wides = widest > (1ull << CLB_CHUNK_SHIFT) ? std::vector<uint32_t>{2u, 1u}
                                                                             : std::vector<uint32_t>{2u};
-    // a single pair also tries the two-pass form keeping its bitmaps (form 2),
-    // which only a call outside a batch can use, and is timed that way
+    // pairs within one bitmap chunk also try the two-pass form keeping its
+    // bitmaps (form 2); a single pair is timed through the plain tuned call
     const bool single = count == 1;
     const std::vector<uint32_t> forms =
-        single && widest <= (1ull << CLB_CHUNK_SHIFT) ? std::vector<uint32_t>{0u, 1u, 2u} : std::vector<uint32_t>{0u, 1u};
+        widest <= (1ull << CLB_CHUNK_SHIFT) ? std::vector<uint32_t>{0u, 1u, 2u} : std::vector<uint32_t>{0u, 1u};
     for (uint32_t wide : wides)
     for (uint32_t form : forms)
         for (uint32_t bmin : {4096u, 1024u})

@@ -275,7 +275,8 @@ int spgemm_hash_two_pass(clb_controls *ctl, const clb_dcsr &A, const clb_dcsr &B
     const uint32_t kw = bitmap_words(B.ncols);
     Temp<uint32_t> kbits, krec, klist, kcount;
     Temp<uint64_t> koff;
-    keep = keep && nbmp && !t.row_ncols && B.ncols <= (uint64_t)kw * 32 && kbits.try_alloc(ctl, nbmp * kw) &&
+    // (batched rows of narrower pairs use the first words of their stride)
+    keep = keep && nbmp && B.ncols <= (uint64_t)kw * 32 && kbits.try_alloc(ctl, nbmp * kw) &&
            krec.try_alloc(ctl, nbmp * BMP_STEP_REC) && klist.try_alloc(ctl, nbmp) && kcount.try_alloc(ctl, 1) &&
            koff.try_alloc(ctl, n);
     const uint32_t h_nbmp = (uint32_t)nbmp;  // (a pageable copy: staged before the call returns)

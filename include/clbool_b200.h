@@ -320,8 +320,8 @@ CLB_API int clb_dcsr_spgemm_learned(clb_controls *ctl, const clb_dcsr *a, const 
  *                   bitmaps (4 bytes per 32 columns per bitmap row: 128 KB
  *                   a row at 2^20 columns) and whose numeric pass expands
  *                   them instead of inserting their products again (falls
- *                   back to 0 without room for them, for products wider than
- *                   2^20 columns, and inside batches)
+ *                   back to 0 without room for them and for products wider
+ *                   than 2^20 columns)
  *   warp_max        rows with at most this many products use the warp ESC
  *                   kernels: 32, 64, 128 or 256 (threads per row: 32)
  *   bitmap_min      rows with more products use the bitmap kernel: 256..4096
@@ -382,9 +382,9 @@ CLB_API int clb_dcsr_union(clb_controls *ctl, uint32_t count, const clb_dcsr *ma
  * pairs and returns the
  * fastest in *best (each candidate: one warm-up call, then the best of three
  * timed calls); tried/ms (optional, max_tried entries) receive each
- * candidate and its device time in ms, *n_tried their number.  A single pair
- * (count = 1) is timed through clb_dcsr_spgemm_tuned, with form 2 among the
- * candidates (48 in all) when it has at most 2^20 columns. */
+ * candidate and its device time in ms, *n_tried their number.  Pairs of at
+ * most 2^20 columns also try form 2 (48 candidates); a single pair (count =
+ * 1) is timed through clb_dcsr_spgemm_tuned. */
 CLB_API int clb_spgemm_autotune(clb_controls *ctl, uint32_t count, const clb_dcsr *a, const clb_dcsr *b,
                                 clb_spgemm_tuning *best, clb_spgemm_tuning *tried, double *ms, uint32_t max_tried,
                                 uint32_t *n_tried);

@@ -50,7 +50,8 @@ def test_batch_of_power_law_pairs(controls):
 
 @pytest.mark.parametrize("form,warp_max,bitmap_min,bitmap_threads,small_lanes", [
     ("two_pass", 256, 4096, 1024, 8), ("single_pass", 256, 4096, 1024, 8), ("two_pass", 64, 256, 256, 32),
-    ("single_pass", 32, 256, 512, 16), ("two_pass", 128, 1024, 256, 16), ("single_pass", 64, 1024, 1024, 32)])
+    ("single_pass", 32, 256, 512, 16), ("two_pass", 128, 1024, 256, 16), ("single_pass", 64, 1024, 1024, 32),
+    ("two_pass_kept", 256, 256, 1024, 8), ("two_pass_kept", 64, 1024, 256, 32)])
 def test_every_tuning_gives_the_same_product(controls, form, warp_max, bitmap_min, bitmap_threads, small_lanes):
     import clbool_b200 as cb
     pairs = batch(6, seed=3) + [(pairs_dcsr(1500, 40), pairs_dcsr(1500, 40))]
@@ -113,7 +114,8 @@ def test_autotune_picks_a_tuning(controls):
     pairs = batch(8, seed=5)
     dev = [(to_device(controls, a), to_device(controls, b)) for a, b in pairs]
     best, tried = cb.dcsr.autotune(controls, dev)
-    assert len(tried) == 32
+    assert len(tried) == 48  # forms 0, 1 and 2 (pairs within one bitmap chunk)
+    assert {t["form"] for t, _ in tried} == {"two_pass", "single_pass", "two_pass_kept"}
     assert all(ms > 0 for _, ms in tried)
     fastest = min(tried, key=lambda t: t[1])
     assert fastest[0] == best.as_dict()
