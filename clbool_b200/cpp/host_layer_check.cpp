@@ -105,6 +105,15 @@ int main(int argc, char **argv) {
         matrix_dcsr C3;
         dcsr::matrix_multiplication_learned(controls, C3, A, B, sizer);
         EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, C3)) == product(pa, pb));
+        {  // the two-pass form keeping its symbolic pass's bitmaps
+            clb_spgemm_tuning kept;
+            clb_spgemm_tuning_default(&kept);
+            kept.form = 2;
+            kept.bitmap_min = 256;  // bitmap rows even in this small product
+            matrix_dcsr C4;
+            dcsr::matrix_multiplication_tuned(controls, C4, A, B, kept);
+            EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, C4)) == product(pa, pb));
+        }
         auto batch = dcsr::matrix_multiplication_batched(controls, {{A, B}, {B, A}, {A, A}});
         EXPECT(batch.size() == 3);
         EXPECT(pairs_of(matrix_dcsr_from_gpu(controls, batch[0])) == product(pa, pb));

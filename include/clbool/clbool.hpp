@@ -438,6 +438,17 @@ inline void matrix_multiplication_learned(Controls &c, matrix_dcsr &matrix_out, 
     matrix_out = matrix_dcsr::adopt(c, out);
 }
 
+// C = A*B under an accumulator tuning (form 0: exact two-pass, 1: single
+// pass into upper-bound slots, 2: exact two-pass keeping the symbolic pass's
+// bitmaps for the numeric pass); every tuning gives the same C.
+inline void matrix_multiplication_tuned(Controls &c, matrix_dcsr &matrix_out, const matrix_dcsr &a,
+                                        const matrix_dcsr &b, const clb_spgemm_tuning &tuning,
+                                        clb_spgemm_stats *stats = nullptr) {
+    clb_dcsr va = a.view(), vb = b.view(), out{};
+    details::check(clb_dcsr_spgemm_tuned(c.get(), &va, &vb, &tuning, &out, stats));
+    matrix_out = matrix_dcsr::adopt(c, out);
+}
+
 // out[k] = pairs[k].first * pairs[k].second, all pairs in one pass.
 inline std::vector<matrix_dcsr> matrix_multiplication_batched(
     Controls &c, const std::vector<std::pair<matrix_dcsr, matrix_dcsr>> &pairs,
