@@ -275,3 +275,19 @@ def test_union_matches_oracle(controls):
     with pytest.raises(cb.ClBoolException) as ex:
         cb.dcsr.matrix_union(controls, [dev[0], to_device(controls, pairs_dcsr(100, 3))])
     assert ex.value.status_name == "CLBOOL_INVALID_ARGUMENT"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["fused", "batched"])
+def test_closure_with_the_kept_two_pass_tuning(controls, method):
+    """The tuning the autotuner now often returns (the two-pass form keeping
+    its bitmaps, bitmap rows from 256 products), through both iteration
+    methods (the batched one also hands it to the one-pass union)."""
+    import clbool_b200 as cb
+    from clbool_b200 import cfpq
+    labels = _labels(1 << 10, 3, 3, seed=23)
+    want, want_hist = O.closure(labels, max_iters=2)
+    t = cb.dcsr.tuning("two_pass_kept", bitmap_min=256, bitmap_threads=256)
+    C, hist = cfpq.closure(controls, [to_device(controls, L) for L in labels], max_iters=2, method=method, tune=t)
+    assert [h["nnz"] for h in hist] == want_hist
+    assert_dcsr_equal(from_device(controls, C), want, f"closure {method}, kept two-pass tuning")
