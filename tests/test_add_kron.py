@@ -158,6 +158,27 @@ def test_kronecker_vs_oracle(controls, na, nb):
     assert dcsr_digest(from_device(controls, k)) == dcsr_digest(O.kronecker(a, b))
 
 
+def test_kronecker_row_length_sweep(controls):
+    """Every B row length from 1 to 260 against A rows of 1-5, 7, 31-33 and
+    127-129 entries: C's rows start at every 16-byte alignment, and the
+    column kernel's head, whole-group and tail entries, its step carry and
+    its short-row division all occur."""
+    import clbool_b200 as cb
+    rng = np.random.default_rng(29)
+    la = np.array([1, 2, 3, 4, 5, 7, 31, 32, 33, 127, 128, 129])
+    ra = np.repeat(np.arange(la.size, dtype=np.uint32), la)
+    ca = np.concatenate([np.sort(rng.choice(200, k, replace=False)) for k in la]).astype(np.uint32)
+    a = O.coo_to_dcsr(O.Coo(la.size, 200, ra, ca))
+    lb = np.arange(1, 261)
+    rb = np.repeat(np.arange(lb.size, dtype=np.uint32), lb)
+    cbb = np.concatenate([np.sort(rng.choice(300, k, replace=False)) for k in lb]).astype(np.uint32)
+    b = O.coo_to_dcsr(O.Coo(lb.size, 300, rb, cbb))
+    want = O.kronecker(a, b)
+    assert len(want.cols) == int(la.sum()) * int(lb.sum())
+    k = cb.dcsr.kronecker_product(controls, None, to_device(controls, a), to_device(controls, b))
+    assert_dcsr_equal(from_device(controls, k), want, "row length sweep")
+
+
 @pytest.mark.parametrize("size,k", [(0, 0), (5, 3), (95, 19), (900, 25), (9400, 60)])
 def test_transpose(controls, size, k):
     """transpose_* suites (test_operations.cpp:14-37)."""
