@@ -33,8 +33,8 @@ __device__ __forceinline__ void kron_small_divmod(uint32_t q, uint32_t l, uint32
     r = q - d * l;
 }
 
-// One C row (A's row ar[0, la) times B's row br[0, lb), more than KR_SMALL
-// entries) written by the whole warp.  B rows of at most 128 entries are
+// A's entries ar[0, la) times B's row br[0, lb) (la, lb >= 1: a C row, or a
+// chunk of one, which is a contiguous block of it) written by the whole warp.  B rows of at most 128 entries are
 // held in registers (four per lane) and each A entry's copy is written by
 // one step; longer B rows are looped over per A entry; B rows shorter than
 // 32 entries are flattened: lane l writes entries l, l + 32, ... and moves
