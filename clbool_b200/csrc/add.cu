@@ -580,15 +580,22 @@ int csr_add_impl(clb_controls *ctl, const clb_csr &a, const clb_csr &b, clb_csr 
             Temp<uint64_t> rpt, tot;
             CLB_RETURN_IF(rpt.alloc(ctl, a.nrows + 1));
             CLB_RETURN_IF(tot.alloc(ctl, 1));
-            const unsigned gw = (unsigned)std::min<uint64_t>((a.nrows + 7) / 8, (uint64_t)ctl->sm_count * 8);
+            // grid-stride kernels: no more blocks than the SMs hold at once
+            static const int w0_per_sm = blocks_per_sm(csr_insert_kernel<0>, 256);
+            static const int w1_per_sm = blocks_per_sm(csr_insert_kernel<1>, 256);
+            static const int l0_per_sm = blocks_per_sm(csr_insert_long_kernel<0>, 256);
+            static const int l1_per_sm = blocks_per_sm(csr_insert_long_kernel<1>, 256);
+            const uint64_t warps_rows = (a.nrows + 7) / 8;
+            const unsigned gw0 = persistent_grid(ctl, w0_per_sm, warps_rows);
+            const unsigned gw1 = persistent_grid(ctl, w1_per_sm, warps_rows);
             Temp<uint32_t> lrows, nlong;
             CLB_RETURN_IF(lrows.alloc(ctl, a.nrows));
             CLB_RETURN_IF(nlong.alloc(ctl, 1));
             CLB_TRY_CUDA(cudaMemsetAsync(nlong.ptr, 0, 4, ctl->stream), CLB_RUN_KERNEL_FAILURE);
-            csr_insert_kernel<0><<<gw, 256, 0, ctl->stream>>>(A, B, a.nrows, rpt.ptr, nullptr, nullptr, lrows.ptr,
-                                                              nlong.ptr);
-            csr_insert_long_kernel<0><<<ctl->sm_count * 6, 256, 0, ctl->stream>>>(A, B, lrows.ptr, nlong.ptr, rpt.ptr,
-                                                                                 nullptr, nullptr);
+            csr_insert_kernel<0><<<gw0, 256, 0, ctl->stream>>>(A, B, a.nrows, rpt.ptr, nullptr, nullptr, lrows.ptr,
+                                                               nlong.ptr);
+            csr_insert_long_kernel<0><<<ctl->sm_count * l0_per_sm, 256, 0, ctl->stream>>>(
+                A, B, lrows.ptr, nlong.ptr, rpt.ptr, nullptr, nullptr);
             CLB_CHECK_LAUNCH();
             CLB_RETURN_IF(scan_u64_inplace(ctl, rpt.ptr, a.nrows, tot.ptr));
             uint64_t nnz = 0;
@@ -597,10 +604,10 @@ int csr_add_impl(clb_controls *ctl, const clb_csr &a, const clb_csr &b, clb_csr 
                          CLB_COPY_BUFFER_ERROR);
             Temp<uint32_t> cols;
             CLB_RETURN_IF(cols.alloc(ctl, nnz));
-            csr_insert_kernel<1><<<gw, 256, 0, ctl->stream>>>(A, B, a.nrows, nullptr, rpt.ptr, cols.ptr, nullptr,
-                                                              nullptr);
-            csr_insert_long_kernel<1><<<ctl->sm_count * 6, 256, 0, ctl->stream>>>(A, B, lrows.ptr, nlong.ptr, nullptr,
-                                                                                 rpt.ptr, cols.ptr);
+            csr_insert_kernel<1><<<gw1, 256, 0, ctl->stream>>>(A, B, a.nrows, nullptr, rpt.ptr, cols.ptr, nullptr,
+                                                               nullptr);
+            csr_insert_long_kernel<1><<<ctl->sm_count * l1_per_sm, 256, 0, ctl->stream>>>(
+                A, B, lrows.ptr, nlong.ptr, nullptr, rpt.ptr, cols.ptr);
             CLB_CHECK_LAUNCH();
             CLB_TRY_CUDA(cudaStreamSynchronize(ctl->stream), CLB_EVENT_WAITING_ERROR);
             c.nnz = nnz;

@@ -165,6 +165,21 @@ inline unsigned persistent_grid(const clb_controls *ctl, int per_sm, uint64_t it
 
 inline unsigned ceil_div_u(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
+// Blocks of `kernel` (`threads` per block, `smem` dynamic bytes) that one SM
+// holds at once, 1 if the query fails.  A kernel whose blocks loop over
+// their work with a grid stride gets at most this many blocks per SM: a
+// block past it would start only after an earlier block had finished all
+// of its work, and would then run its whole share at lower occupancy.
+template <class K>
+inline int blocks_per_sm(K kernel, int threads, size_t smem = 0) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        n = 1;
+    }
+    return n > 0 ? n : 1;
+}
+
 // ------------------------------------------------------ device primitives --
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned warp_id() { return threadIdx.x >> 5; }
